@@ -1,0 +1,298 @@
+"""ctypes mirror of include/mrt.h and a thin Python handle over libmrt.so.
+
+The library is the product; this module only declares the C structs and
+function signatures so that tests, the benchmark and Python users can call the
+C-ABI directly. There is no Python fallback: if libmrt.so is missing or cannot
+be loaded, every entry point raises.
+
+Struct layouts follow include/mrt.h field for field (ctypes applies the same
+natural alignment as the C compiler on x86-64).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "libmrt.so"
+MINIRT_LIB_PATH = HERE / "libmrt_minirt.so"
+
+MRT_ABI_VERSION = 1
+
+MRT_OK = 0
+STATUS_NAMES = {
+    0: "MRT_OK", -1: "MRT_ERR_INVALID", -2: "MRT_ERR_CUDA", -3: "MRT_ERR_OOM",
+    -4: "MRT_ERR_QUEUE_OVERFLOW", -5: "MRT_ERR_BUDGET", -6: "MRT_ERR_ABORTED",
+    -7: "MRT_ERR_NO_DEVICE", -8: "MRT_ERR_STACK",
+}
+
+FORM_MEGAKERNEL, FORM_WAVEFRONT, FORM_AUTO = 0, 1, 2
+JITTER_SHARED, JITTER_PIXEL = 0, 1
+LIGHT_POINT, LIGHT_DIRECTIONAL = 0, 1
+
+u8x3 = C.c_uint8 * 3
+f64x3 = C.c_double * 3
+f32x3 = C.c_float * 3
+
+
+class Material(C.Structure):
+    _fields_ = [("color", u8x3), ("emission_color", u8x3), ("pad_", C.c_uint8 * 2),
+                ("metallic", C.c_double), ("roughness", C.c_double), ("ior", C.c_double),
+                ("transmission", C.c_double), ("ao", C.c_double),
+                ("emission_strength", C.c_double), ("scale", C.c_double)]
+
+
+class Sphere(C.Structure):
+    _fields_ = [("center", f64x3), ("radius", C.c_double), ("material", C.c_int32),
+                ("color", u8x3), ("pad_", C.c_uint8)]
+
+
+class Plane(C.Structure):
+    _fields_ = [("point", f64x3), ("normal", f64x3), ("material", C.c_int32),
+                ("color", u8x3), ("pad_", C.c_uint8)]
+
+
+class Mesh(C.Structure):
+    _fields_ = [("n_vertices", C.c_uint32), ("n_triangles", C.c_uint32),
+                ("positions", C.POINTER(C.c_double)), ("normals", C.POINTER(C.c_double)),
+                ("uvs", C.POINTER(C.c_double)), ("indices", C.POINTER(C.c_uint32)),
+                ("tri_material", C.POINTER(C.c_int32)), ("material", C.c_int32),
+                ("color", u8x3), ("pad_", C.c_uint8)]
+
+
+class Light(C.Structure):
+    _fields_ = [("type", C.c_int32), ("shadow_sample", C.c_int32), ("position", f64x3),
+                ("brightness", C.c_double), ("radius", C.c_float), ("color", u8x3),
+                ("pad_", C.c_uint8)]
+
+
+class Camera(C.Structure):
+    _fields_ = [("position", f64x3), ("orientation", f64x3), ("focus_dist", C.c_double),
+                ("defocus_angle", C.c_double), ("fov", C.c_uint8), ("pad_", C.c_uint8 * 7)]
+
+
+class Ambient(C.Structure):
+    _fields_ = [("ratio", C.c_double), ("hdr_rgbe", C.POINTER(C.c_uint8)),
+                ("hdr_width", C.c_int32), ("hdr_height", C.c_int32),
+                ("hdr_exposure", C.c_float), ("hdr_gamma", C.c_float),
+                ("color", u8x3), ("pad_", C.c_uint8 * 5)]
+
+
+class Caustic(C.Structure):
+    _fields_ = [("enable", C.c_int32), ("passes", C.c_int32),
+                ("photons_per_light", C.c_uint64), ("radius", C.c_double),
+                ("norm_factor", C.c_double), ("shrink", C.c_double),
+                ("knn", C.c_int32), ("mode", C.c_int32)]
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [("abi_version", C.c_uint32), ("render_width", C.c_int32),
+                ("render_height", C.c_int32), ("max_bounces", C.c_int32),
+                ("triangle_one_sided", C.c_int32), ("pad_", C.c_int32),
+                ("ior_all", C.c_double), ("camera", Camera), ("ambient", Ambient),
+                ("caustic", Caustic),
+                ("materials", C.POINTER(Material)), ("n_materials", C.c_int32),
+                ("n_spheres", C.c_int32), ("spheres", C.POINTER(Sphere)),
+                ("planes", C.POINTER(Plane)), ("n_planes", C.c_int32),
+                ("n_meshes", C.c_int32), ("meshes", C.POINTER(Mesh)),
+                ("lights", C.POINTER(Light)), ("n_lights", C.c_int32),
+                ("pad2_", C.c_int32)]
+
+
+class RenderParams(C.Structure):
+    _fields_ = [("spp", C.c_int32), ("sample_base", C.c_int32), ("seed", C.c_uint64),
+                ("max_bounces", C.c_int32), ("form", C.c_int32), ("jitter", C.c_int32),
+                ("render_mode", C.c_int32), ("block_size", C.c_int32),
+                ("queue_capacity", C.c_int32), ("sort_threshold", C.c_int32),
+                ("use_graph", C.c_int32), ("offset", C.POINTER(C.c_double))]
+
+
+class RenderStats(C.Structure):
+    _fields_ = [("ms", C.c_double), ("paths", C.c_uint64), ("segments", C.c_uint64),
+                ("shadow_rays", C.c_uint64), ("kernel_launches", C.c_uint32),
+                ("status", C.c_int32)]
+
+
+class Ray(C.Structure):
+    _fields_ = [("orig", f64x3), ("dir", f64x3)]
+
+
+class Hit(C.Structure):
+    _fields_ = [("prim", C.c_int32), ("front_face", C.c_int32), ("t", C.c_float),
+                ("u", C.c_float), ("v", C.c_float), ("normal", f32x3), ("point", f32x3),
+                ("visits", C.c_int32)]
+
+
+HIT_DTYPE = np.dtype([("prim", "<i4"), ("front_face", "<i4"), ("t", "<f4"), ("u", "<f4"),
+                      ("v", "<f4"), ("normal", "<f4", 3), ("point", "<f4", 3),
+                      ("visits", "<i4")])
+assert HIT_DTYPE.itemsize == C.sizeof(Hit)
+
+_P = C.c_void_p
+
+SIGNATURES = {
+    "mrt_last_error": (C.c_char_p, []),
+    "mrt_version": (C.c_int, []),
+    "mrt_device_count": (C.c_int, []),
+    "mrt_create": (_P, [C.c_int, C.c_int, C.c_int]),
+    "mrt_destroy": (None, [_P]),
+    "mrt_scene_build": (C.c_int, [_P, C.POINTER(SceneDesc)]),
+    "mrt_set_camera": (C.c_int, [_P, C.POINTER(Camera), C.c_double, C.c_double]),
+    "mrt_render": (C.c_int, [_P, C.POINTER(RenderParams), C.POINTER(RenderStats)]),
+    "mrt_clear": (C.c_int, [_P]),
+    "mrt_read_accum": (C.c_int, [_P, _P, C.POINTER(C.c_int32)]),
+    "mrt_accumulate_double": (C.c_int, [_P, _P]),
+    "mrt_read_depth": (C.c_int, [_P, _P]),
+    "mrt_trace_first_hit": (C.c_int, [_P, _P, C.c_int64, _P]),
+    "mrt_read_env_tables": (C.c_int, [_P, _P, _P, _P]),
+    "mrt_photon_count": (C.c_int64, [_P]),
+    "mrt_read_photons": (C.c_int, [_P, _P, _P, C.c_int64]),
+    "mrt_set_photons": (C.c_int, [_P, _P, _P, C.c_int64]),
+    "mrt_caustic_query": (C.c_int, [_P, _P, C.c_int64, C.c_int32, _P]),
+}
+
+
+class MRTError(RuntimeError):
+    pass
+
+
+_lib = None
+
+
+def load(path: str | os.PathLike | None = None) -> C.CDLL:
+    """Load libmrt.so (built in-tree by build.py). Raises if it is missing."""
+    global _lib
+    if _lib is not None and path is None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise MRTError(f"{p} not built: run `python 42-minirt_b200/build.py` "
+                       "(or __graft_entry__.build())")
+    lib = C.CDLL(str(p), mode=C.RTLD_GLOBAL)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if path is None:
+        _lib = lib
+    return lib
+
+
+def check(rc: int, what: str) -> None:
+    if rc != MRT_OK:
+        msg = load().mrt_last_error()
+        raise MRTError(f"{what} failed: {STATUS_NAMES.get(rc, rc)}: "
+                       f"{msg.decode() if msg else ''}")
+
+
+def _ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class Context:
+    """One device context (mrt_ctx): scene + accumulator on one GPU."""
+
+    def __init__(self, width: int, height: int, device: int = 0):
+        self.lib = load()
+        self.width, self.height = int(width), int(height)
+        self.h = self.lib.mrt_create(int(device), self.width, self.height)
+        if not self.h:
+            raise MRTError(f"mrt_create failed: {self.lib.mrt_last_error().decode()}")
+        self._keep = None
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.mrt_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def build(self, scene) -> None:
+        desc = scene.desc() if hasattr(scene, "desc") else scene
+        self._keep = scene
+        check(self.lib.mrt_scene_build(self.h, C.byref(desc)), "mrt_scene_build")
+
+    def set_camera(self, cam: Camera, ior_all: float, ratio: float) -> None:
+        check(self.lib.mrt_set_camera(self.h, C.byref(cam), ior_all, ratio), "mrt_set_camera")
+
+    def render(self, spp: int, seed: int = 1, sample_base: int = 0, form: int = FORM_MEGAKERNEL,
+               jitter: int = JITTER_SHARED, max_bounces: int = 0, render_mode: int = 0,
+               block_size: int = 0, queue_capacity: int = 0, sort_threshold: int = 0,
+               use_graph: int = 0, offset=None) -> RenderStats:
+        p = RenderParams(spp=spp, sample_base=sample_base, seed=seed, max_bounces=max_bounces,
+                         form=form, jitter=jitter, render_mode=render_mode,
+                         block_size=block_size, queue_capacity=queue_capacity,
+                         sort_threshold=sort_threshold, use_graph=use_graph)
+        off = None
+        if offset is not None:
+            off = (C.c_double * 2)(float(offset[0]), float(offset[1]))
+            p.offset = C.cast(off, C.POINTER(C.c_double))
+        st = RenderStats()
+        check(self.lib.mrt_render(self.h, C.byref(p), C.byref(st)), "mrt_render")
+        return st
+
+    def clear(self) -> None:
+        check(self.lib.mrt_clear(self.h), "mrt_clear")
+
+    def read_accum(self) -> tuple[np.ndarray, int]:
+        out = np.zeros((self.height, self.width, 3), np.float32)
+        spp = C.c_int32(0)
+        check(self.lib.mrt_read_accum(self.h, _ptr(out), C.byref(spp)), "mrt_read_accum")
+        return out, spp.value
+
+    def accumulate_double(self, buf: np.ndarray) -> None:
+        assert buf.dtype == np.float64 and buf.size == self.width * self.height * 3
+        check(self.lib.mrt_accumulate_double(self.h, _ptr(buf)), "mrt_accumulate_double")
+
+    def read_depth(self) -> np.ndarray:
+        out = np.zeros((self.height, self.width), np.int32)
+        check(self.lib.mrt_read_depth(self.h, _ptr(out)), "mrt_read_depth")
+        return out
+
+    def first_hit(self, orig: np.ndarray, dirs: np.ndarray) -> np.ndarray:
+        rays = np.ascontiguousarray(np.concatenate([orig, dirs], axis=1), np.float64)
+        hits = np.zeros(len(rays), HIT_DTYPE)
+        check(self.lib.mrt_trace_first_hit(self.h, _ptr(rays), len(rays), _ptr(hits)),
+              "mrt_trace_first_hit")
+        return hits
+
+    def env_tables(self, w: int, h: int):
+        pdf = np.zeros(w * h, np.float32)
+        cm = np.zeros(h, np.float32)
+        cc = np.zeros(w * h, np.float32)
+        check(self.lib.mrt_read_env_tables(self.h, _ptr(pdf), _ptr(cm), _ptr(cc)),
+              "mrt_read_env_tables")
+        return pdf, cm, cc
+
+    def photon_count(self) -> int:
+        n = self.lib.mrt_photon_count(self.h)
+        if n < 0:
+            check(int(n), "mrt_photon_count")
+        return int(n)
+
+    def photons(self):
+        n = self.photon_count()
+        pos = np.zeros((n, 4), np.float32)
+        pw = np.zeros((n, 4), np.float32)
+        check(self.lib.mrt_read_photons(self.h, _ptr(pos), _ptr(pw), n), "mrt_read_photons")
+        return pos[:, :3], pw[:, :3]
+
+    def set_photons(self, pos: np.ndarray, power: np.ndarray) -> None:
+        pos = np.ascontiguousarray(pos, np.float64)
+        power = np.ascontiguousarray(power, np.float64)
+        check(self.lib.mrt_set_photons(self.h, _ptr(pos), _ptr(power), len(pos)),
+              "mrt_set_photons")
+
+    def caustic_query(self, pts: np.ndarray, k: int = 15) -> np.ndarray:
+        pts = np.ascontiguousarray(pts, np.float64)
+        out = np.zeros((len(pts), 3), np.float64)
+        check(self.lib.mrt_caustic_query(self.h, _ptr(pts), len(pts), k, _ptr(out)),
+              "mrt_caustic_query")
+        return out

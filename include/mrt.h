@@ -1,0 +1,319 @@
+/*
+ * mrt.h — C-ABI of the B200 path-tracing library (libmrt.so).
+ *
+ * This is the boundary that replaces miniRT's OpenGL compute path
+ * (the src/gpu C files and the src/shaders GLSL tree) and its serial CPU sample loop
+ * (src/ray_tracing/calc_sample.c). Everything crossing it is a plain C type:
+ * pointers, sizes and fixed-layout structs; no CUDA or PyTorch type appears.
+ *
+ * Two layers use it:
+ *  - the reference-named entry points (init_shader, convert_scene_build,
+ *    convert_scene, compute_frame_gpu, clean_shaders, clean_scene,
+ *    calc_one_sample) in libmrt_minirt.so, compiled against miniRT's own
+ *    headers; they walk t_scene and call the functions below;
+ *  - any other host (tests, benchmarks, ctypes) that describes a scene with
+ *    the flat structs below.
+ *
+ * Scene values keep the reference's types and units (doubles for geometry,
+ * 8-bit t_color colours, RGBE sky texels) so that the reference and this
+ * library read identical numbers; the library repacks them to float32
+ * device layouts itself.
+ *
+ * Error convention (reference: int 0 / -1 plus an "[Error]" line on stderr):
+ * every int-returning call returns MRT_OK (0) or a negative mrt_status and
+ * stores a message retrievable with mrt_last_error() (thread-local).
+ * Threading: one context per host thread; calls on a context are serialised
+ * by the caller (the reference calls its GPU path from the mlx loop thread
+ * only, main_shader_utils.c:20-38).
+ */
+#ifndef MRT_H
+# define MRT_H
+
+# include <stddef.h>
+# include <stdint.h>
+
+# ifdef __cplusplus
+extern "C" {
+# endif
+
+# define MRT_ABI_VERSION 1
+
+typedef enum mrt_status
+{
+	MRT_OK = 0,
+	MRT_ERR_INVALID = -1,        /* bad argument or malformed scene */
+	MRT_ERR_CUDA = -2,           /* CUDA runtime error */
+	MRT_ERR_OOM = -3,            /* device or host allocation failed */
+	MRT_ERR_QUEUE_OVERFLOW = -4, /* a wavefront queue overflowed (device status word) */
+	MRT_ERR_BUDGET = -5,         /* a bounded device loop ran out of iterations */
+	MRT_ERR_ABORTED = -6,        /* host watchdog raised the abort flag */
+	MRT_ERR_NO_DEVICE = -7,      /* no CUDA device / extension not loadable */
+	MRT_ERR_STACK = -8           /* traversal stack overflow (restart also failed) */
+}	mrt_status;
+
+/* ------------------------------------------------------------------ scene */
+
+/* t_mat (scene_structs.h:84-106), untextured fields. Colours are the 8-bit
+ * values the reference stores; emission_color is emission_color_tmp, which
+ * set_values_mat turns into emission_color = c / 255 (set_dependant_values_objs2.c:34). */
+typedef struct mrt_material
+{
+	uint8_t	color[3];
+	uint8_t	emission_color[3];
+	uint8_t	pad_[2];
+	double	metallic;          /* clamped to [0,1] like set_values_mat */
+	double	roughness;         /* clamped to [0,1] */
+	double	ior;               /* <= 0 means "diffuse only" (dielectric.c:42) */
+	double	transmission;
+	double	ao;                /* ambient occlusion factor, default 1 */
+	double	emission_strength;
+	double	scale;             /* uv scale, default 1 */
+}	mrt_material;
+
+/* t_sphere (scene_structs.h:167-175); material < 0 means no material
+ * (the object's own colour is used, like "sp ... 255,0,0"). */
+typedef struct mrt_sphere
+{
+	double	center[3];
+	double	radius;
+	int32_t	material;
+	uint8_t	color[3];
+	uint8_t	pad_;
+}	mrt_sphere;
+
+/* t_plane (scene_structs.h:177-183); normal must be unit length. */
+typedef struct mrt_plane
+{
+	double	point[3];
+	double	normal[3];
+	int32_t	material;
+	uint8_t	color[3];
+	uint8_t	pad_;
+}	mrt_plane;
+
+/* Triangle mesh (t_custom_object + t_triangle/t_vertex, scene_structs.h:208-252).
+ * Indexed: positions/normals per vertex, 3 indices per triangle. indices may
+ * be NULL (triangle t uses vertices 3t..3t+2). uvs may be NULL (all zero).
+ * tri_material may be NULL (every triangle uses `material`). Positions must
+ * be the final world-space values (the reference re-transforms custom
+ * objects in ft_update_obj_position; the miniRT adapter reads the vertices
+ * after that step). */
+typedef struct mrt_mesh
+{
+	uint32_t		n_vertices;
+	uint32_t		n_triangles;
+	const double	*positions;     /* 3 * n_vertices */
+	const double	*normals;       /* 3 * n_vertices */
+	const double	*uvs;           /* 2 * n_vertices or NULL */
+	const uint32_t	*indices;       /* 3 * n_triangles or NULL */
+	const int32_t	*tri_material;  /* n_triangles or NULL */
+	int32_t			material;
+	uint8_t			color[3];
+	uint8_t			pad_;
+}	mrt_mesh;
+
+typedef enum mrt_light_type
+{
+	MRT_LIGHT_POINT = 0,       /* t_light (scene_structs.h:137-145) */
+	MRT_LIGHT_DIRECTIONAL = 1  /* t_dlight (scene_structs.h:147-152) */
+}	mrt_light_type;
+
+typedef struct mrt_light
+{
+	int32_t	type;
+	int32_t	shadow_sample;     /* soft-shadow samples (default 5 when radius given) */
+	double	position[3];       /* point: position; directional: orientation (unit) */
+	double	brightness;
+	float	radius;            /* point light radius (0 = hard shadow) */
+	uint8_t	color[3];
+	uint8_t	pad_;
+}	mrt_light;
+
+/* t_camera (scene_structs.h:128-135). fov is the HORIZONTAL field of view in
+ * integer degrees, as in the reference (viewport.c:57). */
+typedef struct mrt_camera
+{
+	double	position[3];
+	double	orientation[3];
+	double	focus_dist;        /* 0 -> 1, as the reference UI does */
+	double	defocus_angle;
+	uint8_t	fov;
+	uint8_t	pad_[7];
+}	mrt_camera;
+
+/* t_amb_light (scene_structs.h:108-126) with an optional Radiance RGBE sky
+ * (t_hdr, hdr_parsing.h:18-35). hdr_rgbe == NULL means a uniform sky of
+ * colour color * ratio / 255. */
+typedef struct mrt_ambient
+{
+	double			ratio;
+	const uint8_t	*hdr_rgbe;     /* 4 * hdr_width * hdr_height (r,g,b,e) */
+	int32_t			hdr_width;
+	int32_t			hdr_height;
+	float			hdr_exposure;
+	float			hdr_gamma;     /* 1 = linear */
+	uint8_t			color[3];
+	uint8_t			pad_[5];
+}	mrt_ambient;
+
+/* --caustic=N;radius;norm (option_caustic.c:63) plus the progressive
+ * extension (fixed radius, shrinking by `shrink` per pass). */
+typedef struct mrt_caustic
+{
+	int32_t		enable;
+	int32_t		passes;          /* 1 = the reference's single kNN pass */
+	uint64_t	photons_per_light;
+	double		radius;          /* compared against r^2 (get_caustic.c:45) */
+	double		norm_factor;
+	double		shrink;          /* progressive mode radius factor per pass */
+	int32_t		knn;             /* k nearest (reference: 15, material_default.c:81) */
+	int32_t		mode;            /* 0 = kNN parity mode, 1 = fixed-radius progressive */
+}	mrt_caustic;
+
+typedef struct mrt_scene_desc
+{
+	uint32_t			abi_version;    /* MRT_ABI_VERSION */
+	int32_t				render_width;
+	int32_t				render_height;
+	int32_t				max_bounces;
+	int32_t				triangle_one_sided;
+	int32_t				pad_;
+	double				ior_all;        /* scene ior, default 1 (parse_scene.c:122) */
+	mrt_camera			camera;
+	mrt_ambient			ambient;
+	mrt_caustic			caustic;
+	const mrt_material	*materials;
+	int32_t				n_materials;
+	int32_t				n_spheres;
+	const mrt_sphere	*spheres;
+	const mrt_plane		*planes;
+	int32_t				n_planes;
+	int32_t				n_meshes;
+	const mrt_mesh		*meshes;
+	const mrt_light		*lights;
+	int32_t				n_lights;
+	int32_t				pad2_;
+}	mrt_scene_desc;
+
+/* ------------------------------------------------------------- rendering */
+
+typedef enum mrt_form
+{
+	MRT_FORM_MEGAKERNEL = 0,   /* one thread = one path, all bounces */
+	MRT_FORM_WAVEFRONT = 1,    /* per-bounce queues, material-sorted shading */
+	MRT_FORM_AUTO = 2          /* autotuned choice for this scene */
+}	mrt_form;
+
+typedef enum mrt_jitter
+{
+	MRT_JITTER_SHARED = 0,     /* one sub-pixel offset per sample for all pixels (render.c:33) */
+	MRT_JITTER_PIXEL = 1       /* independent offset per pixel and sample */
+}	mrt_jitter;
+
+typedef struct mrt_render_params
+{
+	int32_t		spp;            /* samples per pixel this call */
+	int32_t		sample_base;    /* index of the first sample (RNG counter) */
+	uint64_t	seed;
+	int32_t		max_bounces;    /* <= 0: the scene's value */
+	int32_t		form;           /* mrt_form */
+	int32_t		jitter;         /* mrt_jitter */
+	int32_t		render_mode;    /* 0 path trace, 1 BVH heat map, 2 normals (minirt->render_mode) */
+	int32_t		block_size;     /* 0 = tuned default */
+	int32_t		queue_capacity; /* wavefront paths in flight, 0 = tuned default */
+	int32_t		sort_threshold; /* wavefront: sort shading queue above this many paths */
+	int32_t		use_graph;      /* capture the spp loop in a CUDA graph */
+	const double *offset;       /* optional explicit shared jitter (x,y) for spp == 1 */
+}	mrt_render_params;
+
+typedef struct mrt_render_stats
+{
+	double		ms;             /* device time of the call (CUDA events) */
+	uint64_t	paths;          /* camera paths traced */
+	uint64_t	segments;       /* extension rays traced */
+	uint64_t	shadow_rays;    /* shadow / NEE rays traced */
+	uint32_t	kernel_launches;
+	int32_t		status;         /* device status word (mrt_status) */
+}	mrt_render_stats;
+
+typedef struct mrt_ctx	mrt_ctx;
+
+const char	*mrt_last_error(void);
+int			mrt_version(void);
+int			mrt_device_count(void);
+
+/* init_shader (init_shader.c:133): context + W*H accumulation buffer. */
+mrt_ctx		*mrt_create(int device, int width, int height);
+void		mrt_destroy(mrt_ctx *ctx);
+
+/* convert_scene_build (gpu_scene.c:104): repack, build the BVH, upload,
+ * build HDRI sampling tables on the device, emit photons if enabled. */
+int			mrt_scene_build(mrt_ctx *ctx, const mrt_scene_desc *scene);
+/* convert_scene (gpu_scene.c:62): camera / ambient ratio / ior only. */
+int			mrt_set_camera(mrt_ctx *ctx, const mrt_camera *camera,
+				double ior_all, double ambient_ratio);
+
+/* Render params->spp samples per pixel into the device accumulator. */
+int			mrt_render(mrt_ctx *ctx, const mrt_render_params *params,
+				mrt_render_stats *stats);
+/* Zero the device accumulator. */
+int			mrt_clear(mrt_ctx *ctx);
+/* Copy the device accumulator (sum over samples, W*H*3 floats, row-major,
+ * pixel i = y*W + x) to host memory. Returns the accumulated spp in *spp. */
+int			mrt_read_accum(mrt_ctx *ctx, float *rgb, int32_t *spp);
+/* Add the device accumulator into a caller-owned double buffer laid out
+ * like t_fcolor[W*H] (the reference's screen.float_render) and clear it. */
+int			mrt_accumulate_double(mrt_ctx *ctx, double *float_render);
+/* BVH heat map (render_mode 1): per-pixel node-visit count of the last call. */
+int			mrt_read_depth(mrt_ctx *ctx, int32_t *depth);
+
+/* ------------------------------------------------------- parity probes */
+
+/* A ray in the reference's double layout (t_ray, structs.h:63-67). */
+typedef struct mrt_ray
+{
+	double	orig[3];
+	double	dir[3];
+}	mrt_ray;
+
+/* Closest hit (hit_register_all, hit_register.c:109).
+ * prim: flat primitive id — spheres [0,S), triangles [S,S+T) in mesh order,
+ * planes [S+T, S+T+P) — or -1 for a miss. */
+typedef struct mrt_hit
+{
+	int32_t	prim;
+	int32_t	front_face;
+	float	t;
+	float	u;
+	float	v;
+	float	normal[3];
+	float	point[3];
+	int32_t	visits;         /* BVH nodes visited (heat-map counter) */
+}	mrt_hit;
+
+int			mrt_trace_first_hit(mrt_ctx *ctx, const mrt_ray *rays, int64_t n,
+				mrt_hit *hits);
+
+/* HDRI tables (importance_sampling_manager.c:41) as built on the device:
+ * pdf_joint W*H f32, cdf_marginal_inverse H f32, cdf_conditional_inverse W*H f32.
+ * Any pointer may be NULL. */
+int			mrt_read_env_tables(mrt_ctx *ctx, float *pdf_joint,
+				float *cdf_marginal_inverse, float *cdf_conditional_inverse);
+
+/* Photon map (caustic_manager.c:83): number of stored photons, and their
+ * positions / powers as float4 (x,y,z,_) pairs if the pointers are non-NULL. */
+int64_t		mrt_photon_count(mrt_ctx *ctx);
+int			mrt_read_photons(mrt_ctx *ctx, float *pos4, float *power4, int64_t cap);
+/* Upload an explicit photon set (replacing the emitted one) and rebuild the grid. */
+int			mrt_set_photons(mrt_ctx *ctx, const double *pos3, const double *power3,
+				int64_t n);
+/* Caustic radiance at query points (estimate_caustics_physically_based,
+ * get_caustic.c:67), k nearest photons, as RGB doubles. */
+int			mrt_caustic_query(mrt_ctx *ctx, const double *points3, int64_t n,
+				int32_t k, double *rgb_out);
+
+# ifdef __cplusplus
+}
+# endif
+
+#endif
