@@ -1,0 +1,968 @@
+// api.cu — the C-ABI of libmrt.so (include/mrt.h).
+//
+// Host side of the boundary that replaces miniRT's GL bridge (src/gpu):
+// mrt_create ~ init_shader (init_shader.c:133), mrt_scene_build ~
+// convert_scene_build (gpu_scene.c:104), mrt_set_camera ~ convert_scene
+// (gpu_scene.c:62), mrt_render ~ compute_frame_gpu (use_shader.c:81) for many
+// samples at once, mrt_destroy ~ clean_shaders / clean_scene
+// (clean_shaders.c:32,69). The scene is repacked into the device layout of
+// mrt_internal.h; the context owns all device memory.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/mrt.h"
+#include "bvh_build.h"
+#include "kernels.h"
+
+using namespace mrt;
+
+namespace {
+
+thread_local std::string g_err;
+
+int set_err(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define CK(call)                                                                          \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      return set_err(e_ == cudaErrorMemoryAllocation ? MRT_ERR_OOM : MRT_ERR_CUDA,        \
+                     "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+  } while (0)
+
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  cudaError_t alloc(size_t count) {
+    release();
+    n = count;
+    if (count == 0) return cudaSuccess;
+    return cudaMalloc(&p, sizeof(T) * count);
+  }
+  cudaError_t upload(const T* src, size_t count, cudaStream_t st) {
+    cudaError_t e = alloc(count);
+    if (e != cudaSuccess || count == 0) return e;
+    return cudaMemcpyAsync(p, src, sizeof(T) * count, cudaMemcpyHostToDevice, st);
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  size_t bytes() const { return n * sizeof(T); }
+};
+
+struct V3 { double x, y, z; };
+inline V3 v3(const double* p) { return {p[0], p[1], p[2]}; }
+inline V3 add(V3 a, V3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline V3 sub(V3 a, V3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline V3 mul(V3 a, double s) { return {a.x * s, a.y * s, a.z * s}; }
+inline V3 dv(V3 a, double s) { return s != 0.0 ? V3{a.x / s, a.y / s, a.z / s} : V3{0, 0, 0}; }
+inline V3 cross(V3 a, V3 b) { return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+inline double len(V3 a) { return std::sqrt(a.x * a.x + a.y * a.y + a.z * a.z); }
+inline V3 unitv(V3 a) { double l = len(a); return l > 0.0 ? dv(a, l) : V3{0, 0, 0}; }
+inline void put3(float* d, V3 a) { d[0] = (float)a.x; d[1] = (float)a.y; d[2] = (float)a.z; }
+
+constexpr double kPiD = 3.1415926535897;
+
+inline float int_bits_as_float(int i) {
+  float f;
+  std::memcpy(&f, &i, sizeof(f));
+  return f;
+}
+
+}  // namespace
+
+struct mrt_ctx {
+  int device = 0;
+  int W = 0, H = 0;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  DevBuf<float4> accum;
+  DevBuf<int> depth;
+  DevBuf<int> status;
+  DevBuf<unsigned long long> counters;
+  int accum_spp = 0;
+  bool has_scene = false;
+  // scene
+  DevBuf<Node> nodes;
+  DevBuf<float4> geom, shade;
+  DevBuf<int4> meta;
+  DevBuf<PlaneD> planes;
+  DevBuf<MaterialD> mats;
+  DevBuf<LightD> lights;
+  DevBuf<int> point_lights;
+  int n_point_lights = 0;
+  DevBuf<uint32_t> rgbe;
+  DevBuf<float> pdf_joint, cdf_m, cdf_c;
+  DevBuf<float2> alias;
+  DevBuf<float4> env_rec0, env_rec1;
+  DevBuf<float4> ph_pos, ph_pow, ph_pos_raw, ph_pow_raw;
+  DevBuf<uint32_t> cell_start, cell_of;
+  DevBuf<unsigned int> ph_count;
+  uint64_t photons_per_light = 0;
+  int64_t n_photons = 0;
+  mrt_caustic caustic{};
+  SceneView view{};
+  size_t scene_bytes = 0;
+  int bvh_depth = 0;
+};
+
+namespace {
+
+int check_ctx(mrt_ctx* c) {
+  if (!c) return set_err(MRT_ERR_INVALID, "null context");
+  cudaError_t e = cudaSetDevice(c->device);
+  if (e != cudaSuccess) return set_err(MRT_ERR_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
+  return MRT_OK;
+}
+
+// init_viewport (viewport.c:38-87) in double, stored to float.
+void set_viewport(SceneView& v, const mrt_camera& cam, int W, int H) {
+  const double focus = cam.focus_dist == 0 ? 1.0 : cam.focus_dist;
+  const V3 dir = unitv(v3(cam.orientation));
+  const V3 pos = v3(cam.position);
+  const float vw = (float)(2.0 * std::tan(cam.fov * (kPiD / 180.0) / 2.0) * focus);
+  const float vh = (float)(vw / ((double)W / (double)H));
+  V3 up = {0, 1, 0};
+  if (std::fabs(dir.y) > 0.999) up = {1, 0, 0};
+  const V3 u = unitv(cross(up, mul(dir, -1.0)));
+  const V3 vu = mul(u, vw);
+  const V3 vv = mul(cross(dir, u), vh);
+  const V3 pdu = dv(vu, W), pdv = dv(vv, H);
+  const V3 upper = sub(sub(add(pos, mul(dir, focus)), dv(vu, 2)), dv(vv, 2));
+  const V3 p00 = add(upper, mul(add(pdu, pdv), 0.5));
+  const double rad = focus * std::tan(cam.defocus_angle * kPiD / 360);
+  put3(v.cam, pos);
+  put3(v.pixel00, p00);
+  put3(v.pdu, pdu);
+  put3(v.pdv, pdv);
+  put3(v.defocus_u, mul(u, rad));
+  put3(v.defocus_v, mul(cross(dir, u), rad));
+  v.defocus_angle = (float)cam.defocus_angle;
+}
+
+void set_ambient(SceneView& v, const mrt_ambient& a, bool has_tex) {
+  for (int k = 0; k < 3; ++k) v.amb_const[k] = (float)(a.color[k] / 255.0 * a.ratio);
+  const double exposure = (double)a.hdr_exposure + a.ratio - 1;
+  v.env_exposure_zero = exposure == 0;
+  v.env_scale_exp = powf(2.0f, (float)exposure);
+  v.env_inv_gamma = a.hdr_gamma == 1.0f || a.hdr_gamma == 0.0f ? 1.0f : (float)(1.0 / a.hdr_gamma);
+  v.has_env = has_tex;
+}
+
+uint32_t pack_color(const uint8_t* c) {
+  return (uint32_t)c[0] | ((uint32_t)c[1] << 8) | ((uint32_t)c[2] << 16);
+}
+
+// Vose's alias method on the outcome probabilities (normalised here).
+void build_alias(const std::vector<double>& p, std::vector<float2>& out) {
+  const size_t n = p.size();
+  out.assign(n, make_float2(1.0f, 0.0f));
+  double total = 0;
+  for (double x : p) total += x;
+  if (total <= 0) return;
+  std::vector<double> q(n);
+  std::vector<uint32_t> small, large;
+  small.reserve(n);
+  large.reserve(n);
+  for (size_t i = 0; i < n; ++i) {
+    q[i] = p[i] / total * (double)n;
+    (q[i] < 1.0 ? small : large).push_back((uint32_t)i);
+  }
+  while (!small.empty() && !large.empty()) {
+    uint32_t s = small.back(); small.pop_back();
+    uint32_t l = large.back();
+    out[s] = make_float2((float)q[s], int_bits_as_float((int)l));
+    q[l] = (q[l] + q[s]) - 1.0;
+    if (q[l] < 1.0) { large.pop_back(); small.push_back(l); }
+  }
+  for (uint32_t l : large) out[l] = make_float2(1.0f, int_bits_as_float((int)l));
+  for (uint32_t s : small) out[s] = make_float2(1.0f, int_bits_as_float((int)s));
+}
+
+// Per-outcome records of the two-step sampler, with the reference's double
+// arithmetic: direction of calc_inverse_transform_sampling_dir (get_dir.c:29-41,
+// float theta/phi), pdf_joint at the reference's index (material_default.c:57-59)
+// and the unclamped sky radiance get_background_color returns for that
+// direction (background.c:15-70, get_hdr_value.c:43-68). The sampled
+// directions sit exactly on texel boundaries, so the texel choice has to come
+// from the same double-precision libm calls as the reference.
+void env_records(const mrt_ambient& a, const std::vector<float>& pdf, const std::vector<float>& cm,
+                 const std::vector<float>& cc, std::vector<float4>& r0, std::vector<float4>& r1) {
+  const int W = a.hdr_width, H = a.hdr_height;
+  const size_t no = (size_t)(H - 1) * W;
+  r0.assign(no, make_float4(0.f, 1.f, 0.f, 0.f));
+  r1.assign(no, make_float4(0.f, 0.f, 0.f, 0.f));
+  const double exposure = (double)a.hdr_exposure + a.ratio - 1;
+  const double gcorr = 1.0 / a.hdr_gamma;
+  auto work = [&](int y0, int y1) {
+    for (int iy = y0; iy < y1; ++iy) {
+      const double v = (double)cm[iy];
+      const double A = v * (H - 1) * W;
+      const double j0 = std::floor(A);
+      for (int d = 0; d < W; ++d) {
+        const long long j = (long long)j0 + d;
+        if (j < 0 || j >= (long long)W * H) continue;
+        const double u = (double)cc[j];
+        const float theta = (float)((v - 0.5) * kPiD);
+        const float phi = (float)((0.5 - u) * 2 * kPiD);
+        V3 dir = {std::cos(theta) * std::cos(phi), std::sin(theta), std::cos(theta) * std::sin(phi)};
+        const long long pi = (long long)(v * (H - 1) * W + u * (W - 1));
+        const float pd = (pi >= 0 && pi < (long long)W * H) ? pdf[pi] : 0.0f;
+        const size_t k = (size_t)iy * W + d;
+        r0[k] = make_float4((float)dir.x, (float)dir.y, (float)dir.z, pd);
+        const V3 un = unitv(dir);
+        const double vv = 0.5 + std::asin(un.y) / kPiD;
+        const double uu = 0.5 - std::atan2(un.z, un.x) / (2.0 * kPiD);
+        int x = (int)(uu * (W - 1)), yy = (int)(vv * (H - 1));
+        x = std::min(std::max(x, 0), W - 1);
+        yy = std::min(std::max(yy, 0), H - 1);
+        const uint8_t* px = a.hdr_rgbe + 4 * ((size_t)yy * W + x);
+        double scale = std::ldexp(1.0, px[3] - 128);
+        if (exposure != 0) scale *= powf(2.0f, (float)exposure);
+        double c3[3] = {px[0] * scale / 255.0, px[1] * scale / 255.0, px[2] * scale / 255.0};
+        if (a.hdr_gamma != 1.0f)
+          for (double& q : c3) q = std::pow(q, gcorr);
+        r1[k] = make_float4((float)c3[0], (float)c3[1], (float)c3[2], 0.f);
+      }
+    }
+  };
+  const int nt = std::max(1, std::min((int)std::thread::hardware_concurrency(), 32));
+  std::vector<std::thread> pool;
+  const int rows = H - 1;
+  for (int t = 0; t < nt; ++t)
+    pool.emplace_back(work, rows * t / nt, rows * (t + 1) / nt);
+  for (auto& th : pool) th.join();
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ C-ABI
+
+extern "C" {
+
+const char* mrt_last_error(void) { return g_err.c_str(); }
+int mrt_version(void) { return MRT_ABI_VERSION; }
+
+int mrt_device_count(void) {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+  return n;
+}
+
+mrt_ctx* mrt_create(int device, int width, int height) {
+  if (width <= 0 || height <= 0 || (int64_t)width * height > (1ll << 30)) {
+    set_err(MRT_ERR_INVALID, "invalid render size %dx%d", width, height);
+    return nullptr;
+  }
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    set_err(MRT_ERR_NO_DEVICE, "no CUDA device: %s", cudaGetErrorString(e));
+    return nullptr;
+  }
+  if (device < 0 || device >= n) {
+    set_err(MRT_ERR_INVALID, "device %d out of range (%d devices)", device, n);
+    return nullptr;
+  }
+  mrt_ctx* c = new mrt_ctx();
+  c->device = device;
+  c->W = width;
+  c->H = height;
+  auto fail = [&](cudaError_t err, const char* what) -> mrt_ctx* {
+    set_err(err == cudaErrorMemoryAllocation ? MRT_ERR_OOM : MRT_ERR_CUDA, "%s: %s", what,
+            cudaGetErrorString(err));
+    mrt_destroy(c);
+    return nullptr;
+  };
+  if ((e = cudaSetDevice(device)) != cudaSuccess) return fail(e, "cudaSetDevice");
+  if ((e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)) != cudaSuccess)
+    return fail(e, "cudaStreamCreate");
+  if ((e = cudaEventCreate(&c->ev0)) != cudaSuccess) return fail(e, "cudaEventCreate");
+  if ((e = cudaEventCreate(&c->ev1)) != cudaSuccess) return fail(e, "cudaEventCreate");
+  const size_t np = (size_t)width * height;
+  if ((e = c->accum.alloc(np)) != cudaSuccess) return fail(e, "accumulator");
+  if ((e = c->depth.alloc(np)) != cudaSuccess) return fail(e, "depth buffer");
+  if ((e = c->status.alloc(1)) != cudaSuccess) return fail(e, "status word");
+  if ((e = c->counters.alloc(8)) != cudaSuccess) return fail(e, "counters");
+  cudaMemsetAsync(c->accum.p, 0, c->accum.bytes(), c->stream);
+  cudaMemsetAsync(c->depth.p, 0, c->depth.bytes(), c->stream);
+  cudaMemsetAsync(c->status.p, 0, sizeof(int), c->stream);
+  cudaMemsetAsync(c->counters.p, 0, c->counters.bytes(), c->stream);
+  if ((e = cudaStreamSynchronize(c->stream)) != cudaSuccess) return fail(e, "init");
+  c->view.width = width;
+  c->view.height = height;
+  return c;
+}
+
+void mrt_destroy(mrt_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  c->accum.release(); c->depth.release(); c->status.release(); c->counters.release();
+  c->nodes.release(); c->geom.release(); c->shade.release(); c->meta.release();
+  c->planes.release(); c->mats.release(); c->lights.release(); c->point_lights.release();
+  c->rgbe.release(); c->pdf_joint.release(); c->cdf_m.release(); c->cdf_c.release();
+  c->alias.release(); c->env_rec0.release(); c->env_rec1.release();
+  c->ph_pos.release(); c->ph_pow.release(); c->ph_pos_raw.release(); c->ph_pow_raw.release();
+  c->cell_start.release(); c->cell_of.release(); c->ph_count.release();
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------- photon map build
+
+static int build_grid(mrt_ctx* c, double radius2) {
+  SceneView& v = c->view;
+  const uint32_t n = (uint32_t)c->n_photons;
+  std::vector<float4> pos(n);
+  if (n) {
+    CK(cudaMemcpyAsync(pos.data(), c->ph_pos_raw.p, sizeof(float4) * n, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  float mn[3] = {0, 0, 0}, mx[3] = {0, 0, 0};
+  for (uint32_t i = 0; i < n; ++i) {
+    const float p[3] = {pos[i].x, pos[i].y, pos[i].z};
+    for (int k = 0; k < 3; ++k) {
+      if (i == 0 || p[k] < mn[k]) mn[k] = p[k];
+      if (i == 0 || p[k] > mx[k]) mx[k] = p[k];
+    }
+  }
+  double r = std::sqrt(std::max(radius2, 1e-12));
+  double ext = std::max({(double)mx[0] - mn[0], (double)mx[1] - mn[1], (double)mx[2] - mn[2], 1e-6});
+  double cell = std::max(r, ext / 1024.0) * 1.0001;
+  int dim[3];
+  for (;;) {
+    uint64_t tot = 1;
+    for (int k = 0; k < 3; ++k) {
+      dim[k] = std::max(1, (int)std::ceil(((double)mx[k] - mn[k]) / cell) + 1);
+      tot *= (uint64_t)dim[k];
+    }
+    if (tot <= (1u << 24)) break;
+    cell *= 1.25;
+  }
+  const uint32_t n_cells = (uint32_t)((uint64_t)dim[0] * dim[1] * dim[2]);
+  CK(c->cell_start.alloc((size_t)n_cells + 1));
+  CK(c->cell_of.alloc(std::max<size_t>(n, 1)));
+  CK(c->ph_pos.alloc(std::max<size_t>(n, 1)));
+  CK(c->ph_pow.alloc(std::max<size_t>(n, 1)));
+  GridBuild G{};
+  G.pos_in = c->ph_pos_raw.p;
+  G.pow_in = c->ph_pow_raw.p;
+  G.n = n;
+  G.pos_out = c->ph_pos.p;
+  G.pow_out = c->ph_pow.p;
+  G.cell_of = c->cell_of.p;
+  G.cell_start = c->cell_start.p;
+  G.n_cells = n_cells;
+  for (int k = 0; k < 3; ++k) { G.grid_min[k] = mn[k]; G.dim[k] = dim[k]; }
+  G.inv_cell = (float)(1.0 / cell);
+  CK(launch_grid_build(G, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int k = 0; k < 3; ++k) { v.grid_min[k] = mn[k]; v.grid_dim[k] = dim[k]; }
+  v.grid_inv_cell = (float)(1.0 / cell);
+  v.grid_cell = (float)cell;
+  v.photon_pos = c->ph_pos.p;
+  v.photon_pow = c->ph_pow.p;
+  v.cell_start = c->cell_start.p;
+  v.n_photons = (int)n;
+  return MRT_OK;
+}
+
+// Emits the photons of `pass` and rebuilds the grid (caustic_manager.c:83).
+static int emit_photons(mrt_ctx* c, uint32_t pass, double radius2) {
+  SceneView& v = c->view;
+  const uint64_t cap = c->photons_per_light * (uint64_t)c->n_point_lights;
+  v.caustic = 0;   // emission traces without gathering
+  if (cap == 0) {
+    c->n_photons = 0;
+    v.n_photons = 0;
+    return MRT_OK;
+  }
+  if (c->ph_pos_raw.n < cap) {
+    CK(c->ph_pos_raw.alloc(cap));
+    CK(c->ph_pow_raw.alloc(cap));
+  }
+  if (!c->ph_count.p) CK(c->ph_count.alloc(1));
+  CK(cudaMemsetAsync(c->ph_count.p, 0, sizeof(unsigned), c->stream));
+  PhotonEmit E{};
+  E.seed = 0x5eed5eedULL;
+  E.pass = pass;
+  E.per_light = c->photons_per_light;
+  E.n_point_lights = c->n_point_lights;
+  E.light_index = c->point_lights.p;
+  E.pos = c->ph_pos_raw.p;
+  E.pow = c->ph_pow_raw.p;
+  E.count = c->ph_count.p;
+  E.capacity = cap;
+  CK(launch_photon_emit(v, E, c->status.p, c->stream));
+  unsigned cnt = 0;
+  CK(cudaMemcpyAsync(&cnt, c->ph_count.p, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->n_photons = std::min<uint64_t>(cnt, cap);
+  int rc = build_grid(c, radius2);
+  if (rc != MRT_OK) return rc;
+  v.caustic = 1;
+  return MRT_OK;
+}
+
+// ------------------------------------------------------------ scene build
+
+extern "C" int mrt_scene_build(mrt_ctx* c, const mrt_scene_desc* d) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!d) return set_err(MRT_ERR_INVALID, "null scene");
+  if (d->abi_version != MRT_ABI_VERSION)
+    return set_err(MRT_ERR_INVALID, "scene abi_version %u != %d", d->abi_version, MRT_ABI_VERSION);
+  if (d->render_width != c->W || d->render_height != c->H)
+    return set_err(MRT_ERR_INVALID, "scene size %dx%d does not match the context %dx%d",
+                   d->render_width, d->render_height, c->W, c->H);
+  if (d->n_materials < 0 || d->n_spheres < 0 || d->n_planes < 0 || d->n_meshes < 0 || d->n_lights < 0)
+    return set_err(MRT_ERR_INVALID, "negative element count");
+  if ((d->n_materials && !d->materials) || (d->n_spheres && !d->spheres) ||
+      (d->n_planes && !d->planes) || (d->n_meshes && !d->meshes) || (d->n_lights && !d->lights))
+    return set_err(MRT_ERR_INVALID, "null element array with a non-zero count");
+  c->has_scene = false;
+  SceneView v{};
+  v.width = c->W;
+  v.height = c->H;
+  v.max_bounces = d->max_bounces;
+  v.one_sided = d->triangle_one_sided ? 1 : 0;
+  v.ior_all = (float)d->ior_all;
+  cudaStream_t st = c->stream;
+
+  // materials (t_mat after set_values_mat)
+  std::vector<MaterialD> mats(std::max(1, d->n_materials));
+  for (int i = 0; i < d->n_materials; ++i) {
+    const mrt_material& m = d->materials[i];
+    MaterialD& o = mats[i];
+    for (int k = 0; k < 3; ++k) {
+      o.color[k] = (float)(m.color[k] / 255.0);
+      o.emission[k] = (float)(m.emission_color[k] / 255.0);
+    }
+    auto clamp01 = [](double x) { return x < 0 ? 0.0 : (x > 1 ? 1.0 : x); };
+    const double rough = clamp01(m.roughness);
+    o.metallic = (float)clamp01(m.metallic);
+    o.roughness = (float)rough;
+    o.ior = (float)m.ior;
+    o.transmission = (float)m.transmission;
+    o.ao = (float)m.ao;
+    o.emission_strength = (float)m.emission_strength;
+    o.f0 = powf((float)((m.ior - 1) / (m.ior + 1)), 2.0f);
+    o.alpha4 = (float)((rough * rough) * (rough * rough));
+  }
+
+  // primitives: spheres then triangles (flat ids), double boxes -> float
+  size_t n_tris = 0;
+  for (int i = 0; i < d->n_meshes; ++i) {
+    const mrt_mesh& me = d->meshes[i];
+    if (me.n_triangles && (!me.positions || !me.normals))
+      return set_err(MRT_ERR_INVALID, "mesh %d has no positions or normals", i);
+    if (me.indices)
+      for (size_t k = 0; k < 3 * (size_t)me.n_triangles; ++k)
+        if (me.indices[k] >= me.n_vertices)
+          return set_err(MRT_ERR_INVALID, "mesh %d index %u out of range", i, me.indices[k]);
+    if (!me.indices && (uint64_t)me.n_vertices < 3ull * me.n_triangles)
+      return set_err(MRT_ERR_INVALID, "mesh %d has too few vertices for implicit indices", i);
+    n_tris += me.n_triangles;
+  }
+  const size_t n_prims = (size_t)d->n_spheres + n_tris;
+  std::vector<PrimBox> boxes(n_prims);
+  struct TriRef { const mrt_mesh* m; uint32_t t; };
+  std::vector<TriRef> tris;
+  tris.reserve(n_tris);
+  for (int i = 0; i < d->n_spheres; ++i) {
+    const mrt_sphere& s = d->spheres[i];
+    if (!(s.radius >= 0) || !std::isfinite(s.center[0]) || !std::isfinite(s.center[1]) ||
+        !std::isfinite(s.center[2]))
+      return set_err(MRT_ERR_INVALID, "sphere %d is not finite", i);
+    double mn[3], mx[3];
+    const double r = (s.radius * 2.0) * 0.5;
+    for (int k = 0; k < 3; ++k) { mn[k] = s.center[k] - r; mx[k] = s.center[k] + r; }
+    prim_box_from_double(boxes[i], mn, mx);
+  }
+  {
+    size_t p = d->n_spheres;
+    for (int i = 0; i < d->n_meshes; ++i) {
+      const mrt_mesh& me = d->meshes[i];
+      for (uint32_t t = 0; t < me.n_triangles; ++t, ++p) {
+        double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (int cidx = 0; cidx < 3; ++cidx) {
+          uint32_t vi = me.indices ? me.indices[3 * (size_t)t + cidx] : 3 * t + cidx;
+          const double* q = me.positions + 3 * (size_t)vi;
+          for (int k = 0; k < 3; ++k) {
+            if (!std::isfinite(q[k]))
+              return set_err(MRT_ERR_INVALID, "mesh %d triangle %u has a non-finite vertex", i, t);
+            mn[k] = std::min(mn[k], q[k]);
+            mx[k] = std::max(mx[k], q[k]);
+          }
+        }
+        prim_box_from_double(boxes[p], mn, mx);
+        tris.push_back({&me, t});
+      }
+    }
+  }
+  BvhResult bvh;
+  std::string err;
+  if (!build_bvh(boxes, bvh, err)) return set_err(MRT_ERR_INVALID, "BVH: %s", err.c_str());
+  c->bvh_depth = bvh.max_depth;
+
+  // leaf-order geometry, metadata and shading records
+  std::vector<float4> geom(3 * std::max<size_t>(n_prims, 1));
+  std::vector<int4> meta(std::max<size_t>(n_prims, 1));
+  std::vector<float4> shade(4 * std::max<size_t>(n_prims, 1));
+  for (size_t k = 0; k < n_prims; ++k) {
+    const uint32_t src = bvh.order[k];
+    if (src < (uint32_t)d->n_spheres) {
+      const mrt_sphere& s = d->spheres[src];
+      const double r = (s.radius * 2.0) * 0.5;
+      geom[3 * k] = make_float4((float)s.center[0], (float)s.center[1], (float)s.center[2],
+                                int_bits_as_float(PRIM_SPHERE));
+      geom[3 * k + 1] = make_float4((float)r, (float)(r * r), 0.f, 0.f);
+      geom[3 * k + 2] = make_float4(0.f, 0.f, 0.f, 0.f);
+      const int mat = s.material < d->n_materials ? s.material : -1;
+      meta[k] = make_int4((int)src, mat, PRIM_SPHERE, (int)pack_color(s.color));
+    } else {
+      const TriRef& tr = tris[src - d->n_spheres];
+      const mrt_mesh& me = *tr.m;
+      uint32_t vi[3];
+      for (int cidx = 0; cidx < 3; ++cidx)
+        vi[cidx] = me.indices ? me.indices[3 * (size_t)tr.t + cidx] : 3 * tr.t + cidx;
+      const double* p0 = me.positions + 3 * (size_t)vi[0];
+      const double* p1 = me.positions + 3 * (size_t)vi[1];
+      const double* p2 = me.positions + 3 * (size_t)vi[2];
+      geom[3 * k] = make_float4((float)p0[0], (float)p0[1], (float)p0[2], int_bits_as_float(PRIM_TRI));
+      geom[3 * k + 1] = make_float4((float)(p1[0] - p0[0]), (float)(p1[1] - p0[1]), (float)(p1[2] - p0[2]), 0.f);
+      geom[3 * k + 2] = make_float4((float)(p2[0] - p0[0]), (float)(p2[1] - p0[1]), (float)(p2[2] - p0[2]), 0.f);
+      float uvv[3][2] = {{0, 0}, {0, 0}, {0, 0}};
+      for (int cidx = 0; cidx < 3; ++cidx) {
+        const double* nn = me.normals + 3 * (size_t)vi[cidx];
+        if (me.uvs) {
+          uvv[cidx][0] = (float)me.uvs[2 * (size_t)vi[cidx]];
+          uvv[cidx][1] = (float)me.uvs[2 * (size_t)vi[cidx] + 1];
+        }
+        shade[4 * k + cidx] = make_float4((float)nn[0], (float)nn[1], (float)nn[2], uvv[cidx][0]);
+      }
+      shade[4 * k + 3] = make_float4(uvv[0][1], uvv[1][1], uvv[2][1], 0.f);
+      int32_t mat = me.tri_material ? me.tri_material[tr.t] : me.material;
+      if (mat >= d->n_materials) mat = -1;
+      meta[k] = make_int4((int)src, mat, PRIM_TRI, (int)pack_color(me.color));
+    }
+  }
+  std::vector<PlaneD> planes(std::max(1, d->n_planes));
+  const int plane_base = (int)n_prims;
+  for (int i = 0; i < d->n_planes; ++i) {
+    const mrt_plane& p = d->planes[i];
+    V3 n = unitv(v3(p.normal));
+    planes[i].pn = make_float4((float)p.point[0], (float)p.point[1], (float)p.point[2], 0.f);
+    planes[i].nn = make_float4((float)n.x, (float)n.y, (float)n.z, 0.f);
+    const int mat = p.material < d->n_materials ? p.material : -1;
+    planes[i].meta = make_int4(plane_base + i, mat, 0, (int)pack_color(p.color));
+  }
+  std::vector<LightD> lights(std::max(1, d->n_lights));
+  std::vector<int> point_lights;
+  for (int i = 0; i < d->n_lights; ++i) {
+    const mrt_light& L = d->lights[i];
+    LightD& o = lights[i];
+    V3 p = L.type == MRT_LIGHT_DIRECTIONAL ? unitv(v3(L.position)) : v3(L.position);
+    put3(o.pos, p);
+    double br = L.brightness;
+    if (L.type == MRT_LIGHT_POINT && br < 0) br = 0;
+    o.brightness = (float)br;
+    for (int k = 0; k < 3; ++k) o.color[k] = (float)L.color[k];
+    o.radius = L.radius;
+    o.type = L.type;
+    o.shadow_sample = L.shadow_sample;
+    if (L.type == MRT_LIGHT_POINT) point_lights.push_back(i);
+  }
+
+  CK(c->nodes.upload(bvh.nodes.data(), bvh.nodes.size(), st));
+  CK(c->geom.upload(geom.data(), geom.size(), st));
+  CK(c->meta.upload(meta.data(), meta.size(), st));
+  CK(c->shade.upload(shade.data(), shade.size(), st));
+  CK(c->planes.upload(planes.data(), planes.size(), st));
+  CK(c->mats.upload(mats.data(), mats.size(), st));
+  CK(c->lights.upload(lights.data(), lights.size(), st));
+  CK(c->point_lights.upload(point_lights.data(), point_lights.size(), st));
+  c->n_point_lights = (int)point_lights.size();
+  v.nodes = c->nodes.p;
+  v.geom = c->geom.p;
+  v.meta = c->meta.p;
+  v.shade = c->shade.p;
+  v.planes = c->planes.p;
+  v.mats = c->mats.p;
+  v.lights = c->lights.p;
+  v.n_nodes = (int)bvh.nodes.size();
+  v.n_prims = (int)n_prims;
+  v.n_planes = d->n_planes;
+  v.n_mats = d->n_materials;
+  v.n_lights = d->n_lights;
+  v.has_bvh = n_prims > 0;
+  v.root_leaf = bvh.root_leaf;
+  set_viewport(v, d->camera, c->W, c->H);
+
+  // sky and importance-sampling tables
+  const mrt_ambient& a = d->ambient;
+  const bool has_tex = a.hdr_rgbe && a.hdr_width > 0 && a.hdr_height > 0;
+  set_ambient(v, a, has_tex);
+  if (has_tex) {
+    const int W = a.hdr_width, H = a.hdr_height;
+    const size_t n = (size_t)W * H;
+    std::vector<uint32_t> px(n);
+    std::memcpy(px.data(), a.hdr_rgbe, n * 4);
+    CK(c->rgbe.upload(px.data(), n, st));
+    v.rgbe = c->rgbe.p;
+    v.env_w = W;
+    v.env_h = H;
+    if (H >= 2 && W >= 2) {
+      DevBuf<double> gray, raw, rowcdf, scal, cdfh, prob;
+      CK(gray.alloc(n));
+      CK(raw.alloc(H));
+      CK(rowcdf.alloc(n));
+      CK(scal.alloc(8));
+      CK(cdfh.alloc(H));
+      CK(c->pdf_joint.alloc(n));
+      CK(c->cdf_m.alloc(H));
+      CK(c->cdf_c.alloc(n));
+      const size_t no = (size_t)(H - 1) * W;
+      CK(prob.alloc(no));
+      EnvBuild E{};
+      E.rgbe = c->rgbe.p;
+      E.W = W;
+      E.H = H;
+      E.exposure_zero = a.hdr_exposure == 0;
+      E.exposure_scale = (double)powf(2.0f, a.hdr_exposure);
+      E.gray = gray.p;
+      E.raw = raw.p;
+      E.row_cdf = rowcdf.p;
+      E.scal = scal.p;
+      E.cdf_h = cdfh.p;
+      E.pdf_joint = c->pdf_joint.p;
+      E.cdf_m_inv = c->cdf_m.p;
+      E.cdf_c_inv = c->cdf_c.p;
+      E.out_prob = prob.p;
+      CK(launch_env_tables(E, st));
+      std::vector<double> hp(no);
+      std::vector<float> t_pdf(n), t_cm(H), t_cc(n);
+      CK(cudaMemcpyAsync(hp.data(), prob.p, no * sizeof(double), cudaMemcpyDeviceToHost, st));
+      CK(cudaMemcpyAsync(t_pdf.data(), c->pdf_joint.p, n * sizeof(float), cudaMemcpyDeviceToHost, st));
+      CK(cudaMemcpyAsync(t_cm.data(), c->cdf_m.p, H * sizeof(float), cudaMemcpyDeviceToHost, st));
+      CK(cudaMemcpyAsync(t_cc.data(), c->cdf_c.p, n * sizeof(float), cudaMemcpyDeviceToHost, st));
+      CK(cudaStreamSynchronize(st));
+      std::vector<float2> al;
+      build_alias(hp, al);
+      std::vector<float4> r0, r1;
+      env_records(a, t_pdf, t_cm, t_cc, r0, r1);
+      CK(c->alias.upload(al.data(), al.size(), st));
+      CK(c->env_rec0.upload(r0.data(), r0.size(), st));
+      CK(c->env_rec1.upload(r1.data(), r1.size(), st));
+      CK(cudaStreamSynchronize(st));
+      gray.release(); raw.release(); rowcdf.release(); scal.release(); cdfh.release(); prob.release();
+      v.alias = c->alias.p;
+      v.env_rec0 = c->env_rec0.p;
+      v.env_rec1 = c->env_rec1.p;
+      v.n_env_outcomes = (int)no;
+      v.pdf_joint = c->pdf_joint.p;
+      v.cdf_m_inv = c->cdf_m.p;
+      v.cdf_c_inv = c->cdf_c.p;
+      v.env_nee = 1;
+    }
+  } else {
+    c->rgbe.release();
+  }
+
+  // photon map
+  c->caustic = d->caustic;
+  c->view = v;
+  c->n_photons = 0;
+  if (d->caustic.enable) {
+    if (d->caustic.knn <= 0 || d->caustic.knn > 32)
+      return set_err(MRT_ERR_INVALID, "caustic k=%d outside [1,32]", d->caustic.knn);
+    c->photons_per_light = d->caustic.photons_per_light;
+    c->view.knn = d->caustic.knn;
+    c->view.caustic_radius2 = (float)d->caustic.radius;
+    c->view.inv_norm = (float)(1.0 / d->caustic.norm_factor);
+    c->view.caustic_mode = d->caustic.mode;
+    c->view.fixed_radius2 = (float)d->caustic.radius;
+    int rc2 = emit_photons(c, 0, d->caustic.radius);
+    if (rc2) return rc2;
+  }
+  CK(cudaStreamSynchronize(st));
+  c->scene_bytes = c->nodes.bytes() + c->geom.bytes() + c->meta.bytes() + c->shade.bytes() +
+                   c->planes.bytes() + c->mats.bytes() + c->lights.bytes() + c->rgbe.bytes() +
+                   c->pdf_joint.bytes() + c->cdf_m.bytes() + c->cdf_c.bytes() + c->alias.bytes() +
+                   c->env_rec0.bytes() + c->env_rec1.bytes() + c->ph_pos.bytes() + c->ph_pow.bytes() + c->cell_start.bytes();
+  c->has_scene = true;
+  return MRT_OK;
+}
+
+extern "C" int mrt_set_camera(mrt_ctx* c, const mrt_camera* cam, double ior_all, double ambient_ratio) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!cam) return set_err(MRT_ERR_INVALID, "null camera");
+  set_viewport(c->view, *cam, c->W, c->H);
+  c->view.ior_all = (float)ior_all;
+  (void)ambient_ratio;
+  return MRT_OK;
+}
+
+// ---------------------------------------------------------------- render
+
+static int read_status(mrt_ctx* c, int* out) {
+  int s = 0;
+  CK(cudaMemcpyAsync(&s, c->status.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  *out = s;
+  return MRT_OK;
+}
+
+int mrt_render_wavefront(mrt_ctx* c, const SceneView& v, const LaunchParams& L, int spp,
+                         const mrt_render_params* p, mrt_render_stats* stats);
+
+extern "C" int mrt_render(mrt_ctx* c, const mrt_render_params* p, mrt_render_stats* stats) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!p) return set_err(MRT_ERR_INVALID, "null params");
+  if (!c->has_scene) return set_err(MRT_ERR_INVALID, "no scene: call mrt_scene_build first");
+  if (p->spp < 0 || p->sample_base < 0) return set_err(MRT_ERR_INVALID, "negative spp / sample_base");
+  if (p->render_mode < 0 || p->render_mode > 2) return set_err(MRT_ERR_INVALID, "render_mode %d", p->render_mode);
+  if (p->form < 0 || p->form > 2) return set_err(MRT_ERR_INVALID, "form %d", p->form);
+  if (p->offset && p->spp != 1) return set_err(MRT_ERR_INVALID, "explicit offset needs spp == 1");
+  if (p->block_size && (p->block_size % 32 || p->block_size > 256))
+    return set_err(MRT_ERR_INVALID, "block_size %d", p->block_size);
+  if (p->env_sampler < 0 || p->env_sampler > 1) return set_err(MRT_ERR_INVALID, "env_sampler %d", p->env_sampler);
+  SceneView v = c->view;
+  v.env_lookup = p->env_sampler;
+  const uint64_t npix = (uint64_t)c->W * c->H;
+  LaunchParams L{};
+  L.seed = p->seed;
+  L.max_bounces = p->max_bounces > 0 ? p->max_bounces : v.max_bounces;
+  L.jitter = p->jitter;
+  L.render_mode = p->render_mode;
+  if (p->offset) { L.has_offset = 1; L.ox = (float)p->offset[0]; L.oy = (float)p->offset[1]; }
+  CK(cudaMemsetAsync(c->status.p, 0, sizeof(int), c->stream));
+  CK(cudaMemsetAsync(c->counters.p, 0, c->counters.bytes(), c->stream));
+  if (p->render_mode == 1) CK(cudaMemsetAsync(c->depth.p, 0xff, c->depth.bytes(), c->stream));
+  int launches = 0;
+  CK(cudaEventRecord(c->ev0, c->stream));
+  if (p->form == MRT_FORM_WAVEFRONT && p->render_mode == 0) {
+    L.sample_base = (uint32_t)p->sample_base;
+    int r2 = mrt_render_wavefront(c, v, L, p->spp, p, stats);
+    if (r2) return r2;
+  } else {
+    // chunks of spp so a single launch stays well under a second
+    const uint64_t max_paths = 1ull << 25;
+    int spp_chunk = (int)std::max<uint64_t>(1, max_paths / std::max<uint64_t>(npix, 1));
+    for (int s = 0; s < p->spp; s += spp_chunk) {
+      int k = std::min(spp_chunk, p->spp - s);
+      L.sample_base = (uint32_t)(p->sample_base + s);
+      L.n_paths = npix * (uint64_t)k;
+      CK(launch_megakernel(v, L, c->accum.p, c->depth.p, c->status.p, stats ? c->counters.p : nullptr,
+                           p->block_size, c->stream));
+      launches++;
+    }
+  }
+  CK(cudaEventRecord(c->ev1, c->stream));
+  CK(cudaEventSynchronize(c->ev1));
+  int status = 0;
+  rc = read_status(c, &status);
+  if (rc) return rc;
+  if (p->render_mode != 1) c->accum_spp += p->spp;
+  if (stats) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    unsigned long long cnt[8] = {};
+    CK(cudaMemcpy(cnt, c->counters.p, sizeof(cnt), cudaMemcpyDeviceToHost));
+    stats->ms = ms;
+    stats->paths = npix * (uint64_t)p->spp;
+    stats->segments = cnt[0];
+    stats->shadow_rays = cnt[1];
+    if (p->form != MRT_FORM_WAVEFRONT) stats->kernel_launches = launches;
+    stats->status = status;
+  }
+  if (status & ST_STACK) return set_err(MRT_ERR_STACK, "traversal stack overflow (status 0x%x)", status);
+  if (status & ST_BUDGET) return set_err(MRT_ERR_BUDGET, "traversal iteration budget exhausted (status 0x%x)", status);
+  if (status & ST_QUEUE) return set_err(MRT_ERR_QUEUE_OVERFLOW, "queue overflow (status 0x%x)", status);
+  if (status & ST_ABORT) return set_err(MRT_ERR_ABORTED, "aborted (status 0x%x)", status);
+  return MRT_OK;
+}
+
+extern "C" int mrt_clear(mrt_ctx* c) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  CK(cudaMemsetAsync(c->accum.p, 0, c->accum.bytes(), c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->accum_spp = 0;
+  return MRT_OK;
+}
+
+extern "C" int mrt_read_accum(mrt_ctx* c, float* rgb, int32_t* spp) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!rgb) return set_err(MRT_ERR_INVALID, "null output");
+  const size_t n = (size_t)c->W * c->H;
+  float* d = nullptr;
+  CK(cudaMallocAsync(&d, n * 3 * sizeof(float), c->stream));
+  CK(launch_accum_to_rgb(c->accum.p, d, (int)n, c->stream));
+  CK(cudaMemcpyAsync(rgb, d, n * 3 * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaFreeAsync(d, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (spp) *spp = c->accum_spp;
+  return MRT_OK;
+}
+
+extern "C" int mrt_accumulate_double(mrt_ctx* c, double* float_render) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!float_render) return set_err(MRT_ERR_INVALID, "null output");
+  const size_t n = (size_t)c->W * c->H;
+  std::vector<float> rgb(n * 3);
+  rc = mrt_read_accum(c, rgb.data(), nullptr);
+  if (rc) return rc;
+  for (size_t i = 0; i < 3 * n; ++i) float_render[i] += rgb[i];
+  return mrt_clear(c);
+}
+
+extern "C" int mrt_read_depth(mrt_ctx* c, int32_t* depth) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!depth) return set_err(MRT_ERR_INVALID, "null output");
+  CK(cudaMemcpyAsync(depth, c->depth.p, c->depth.bytes(), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return MRT_OK;
+}
+
+extern "C" int mrt_trace_first_hit(mrt_ctx* c, const mrt_ray* rays, int64_t n, mrt_hit* hits) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (n < 0 || (n && (!rays || !hits))) return set_err(MRT_ERR_INVALID, "bad ray buffer");
+  if (!c->has_scene) return set_err(MRT_ERR_INVALID, "no scene");
+  if (n == 0) return MRT_OK;
+  static_assert(sizeof(HitOut) == sizeof(mrt_hit), "HitOut must mirror mrt_hit");
+  double* dr = nullptr;
+  HitOut* dh = nullptr;
+  CK(cudaMallocAsync(&dr, sizeof(mrt_ray) * n, c->stream));
+  CK(cudaMallocAsync(&dh, sizeof(HitOut) * n, c->stream));
+  CK(cudaMemcpyAsync(dr, rays, sizeof(mrt_ray) * n, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemsetAsync(c->status.p, 0, sizeof(int), c->stream));
+  CK(launch_first_hit(c->view, dr, n, dh, c->status.p, c->stream));
+  CK(cudaMemcpyAsync(hits, dh, sizeof(HitOut) * n, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaFreeAsync(dr, c->stream));
+  CK(cudaFreeAsync(dh, c->stream));
+  int status = 0;
+  rc = read_status(c, &status);
+  if (rc) return rc;
+  if (status) return set_err(status & ST_STACK ? MRT_ERR_STACK : MRT_ERR_BUDGET, "traversal status 0x%x", status);
+  return MRT_OK;
+}
+
+extern "C" int mrt_read_env_tables(mrt_ctx* c, float* pdf_joint, float* cdf_m, float* cdf_c) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!c->view.env_nee) return set_err(MRT_ERR_INVALID, "scene has no HDRI tables");
+  if (pdf_joint) CK(cudaMemcpy(pdf_joint, c->pdf_joint.p, c->pdf_joint.bytes(), cudaMemcpyDeviceToHost));
+  if (cdf_m) CK(cudaMemcpy(cdf_m, c->cdf_m.p, c->cdf_m.bytes(), cudaMemcpyDeviceToHost));
+  if (cdf_c) CK(cudaMemcpy(cdf_c, c->cdf_c.p, c->cdf_c.bytes(), cudaMemcpyDeviceToHost));
+  return MRT_OK;
+}
+
+extern "C" int mrt_env_sample(mrt_ctx* c, int64_t n, uint64_t seed, int32_t sampler, int32_t* outcome,
+                              float* out4) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!c->view.env_nee) return set_err(MRT_ERR_INVALID, "scene has no HDRI tables");
+  if (n < 0 || (n && (!out4 || !outcome))) return set_err(MRT_ERR_INVALID, "bad output buffer");
+  if (sampler < 0 || sampler > 1) return set_err(MRT_ERR_INVALID, "sampler %d", sampler);
+  if (n == 0) return MRT_OK;
+  SceneView v = c->view;
+  v.env_lookup = sampler;
+  float4* d = nullptr;
+  int* dk = nullptr;
+  CK(cudaMallocAsync(&d, sizeof(float4) * n, c->stream));
+  CK(cudaMallocAsync(&dk, sizeof(int) * n, c->stream));
+  CK(launch_env_sample(v, n, seed, dk, d, c->stream));
+  CK(cudaMemcpyAsync(out4, d, sizeof(float4) * n, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(outcome, dk, sizeof(int) * n, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaFreeAsync(d, c->stream));
+  CK(cudaFreeAsync(dk, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return MRT_OK;
+}
+
+extern "C" int64_t mrt_photon_count(mrt_ctx* c) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  return c->n_photons;
+}
+
+extern "C" int mrt_read_photons(mrt_ctx* c, float* pos4, float* pow4, int64_t cap) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  const int64_t n = std::min<int64_t>(cap, c->n_photons);
+  if (n <= 0) return MRT_OK;
+  if (pos4) CK(cudaMemcpy(pos4, c->ph_pos.p, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+  if (pow4) CK(cudaMemcpy(pow4, c->ph_pow.p, sizeof(float4) * n, cudaMemcpyDeviceToHost));
+  return MRT_OK;
+}
+
+extern "C" int mrt_set_photons(mrt_ctx* c, const double* pos3, const double* pow3, int64_t n) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (n < 0 || (n && (!pos3 || !pow3))) return set_err(MRT_ERR_INVALID, "bad photon buffers");
+  if (!c->caustic.enable) return set_err(MRT_ERR_INVALID, "scene has caustics disabled");
+  std::vector<float4> a(std::max<int64_t>(n, 1)), b(std::max<int64_t>(n, 1));
+  for (int64_t i = 0; i < n; ++i) {
+    a[i] = make_float4((float)pos3[3 * i], (float)pos3[3 * i + 1], (float)pos3[3 * i + 2], 0.f);
+    b[i] = make_float4((float)pow3[3 * i], (float)pow3[3 * i + 1], (float)pow3[3 * i + 2], 0.f);
+  }
+  CK(c->ph_pos_raw.upload(a.data(), a.size(), c->stream));
+  CK(c->ph_pow_raw.upload(b.data(), b.size(), c->stream));
+  c->n_photons = n;
+  rc = build_grid(c, c->caustic.radius);
+  if (rc) return rc;
+  c->view.caustic = 1;
+  return MRT_OK;
+}
+
+extern "C" int mrt_caustic_query(mrt_ctx* c, const double* pts3, int64_t n, int32_t k, double* rgb) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (n < 0 || (n && (!pts3 || !rgb))) return set_err(MRT_ERR_INVALID, "bad query buffers");
+  if (k <= 0 || k > 32) return set_err(MRT_ERR_INVALID, "k=%d outside [1,32]", k);
+  if (n == 0) return MRT_OK;
+  SceneView v = c->view;
+  v.knn = k;
+  double *dp = nullptr, *dout = nullptr;
+  CK(cudaMallocAsync(&dp, sizeof(double) * 3 * n, c->stream));
+  CK(cudaMallocAsync(&dout, sizeof(double) * 3 * n, c->stream));
+  CK(cudaMemcpyAsync(dp, pts3, sizeof(double) * 3 * n, cudaMemcpyHostToDevice, c->stream));
+  CausticQuery Q{dp, n, dout};
+  CK(launch_caustic_query(v, Q, c->stream));
+  CK(cudaMemcpyAsync(rgb, dout, sizeof(double) * 3 * n, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaFreeAsync(dp, c->stream));
+  CK(cudaFreeAsync(dout, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return MRT_OK;
+}

@@ -1,0 +1,336 @@
+// bvh_build.cpp — host BVH builder for the device layout in mrt_internal.h.
+//
+// The reference builds a median-split BVH with one primitive per leaf and
+// traverses it exhaustively (bvh_build.c:16-127, bvh_hit.c:16-43). Closest-hit
+// results do not depend on the tree, so the library builds its own tree for
+// speed: binned SAH (32 bins on each axis, Wald 2007) with up to 8 primitives
+// per leaf, object-median splits below depth 40 so the depth stays within the
+// traversal stack, and top-level subtrees built on several threads. Boxes are
+// rounded outward to float so float traversal never culls a hit that the
+// double-precision reference finds inside the box.
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <future>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "bvh_build.h"
+
+namespace mrt {
+
+namespace {
+
+struct Box {
+  float mn[3], mx[3];
+  void reset() {
+    for (int k = 0; k < 3; ++k) { mn[k] = INFINITY; mx[k] = -INFINITY; }
+  }
+  void grow(const Box& b) {
+    for (int k = 0; k < 3; ++k) { mn[k] = std::min(mn[k], b.mn[k]); mx[k] = std::max(mx[k], b.mx[k]); }
+  }
+  void grow(const float* p) {
+    for (int k = 0; k < 3; ++k) { mn[k] = std::min(mn[k], p[k]); mx[k] = std::max(mx[k], p[k]); }
+  }
+  float area() const {
+    float d[3];
+    for (int k = 0; k < 3; ++k) d[k] = std::max(0.0f, mx[k] - mn[k]);
+    return 2.0f * (d[0] * d[1] + d[1] * d[2] + d[2] * d[0]);
+  }
+};
+
+struct BNode {
+  Box box;
+  int left = -1, right = -1;
+  uint32_t first = 0, count = 0;
+  int depth = 0;
+};
+
+constexpr int kBins = 32;
+constexpr int kMedianDepth = 40;
+constexpr float kTraversalCost = 1.0f;
+constexpr float kIsectCost = 1.0f;
+
+struct Builder {
+  const std::vector<PrimBox>& prims;
+  std::vector<uint32_t>& order;
+  std::vector<BNode> nodes;
+  std::atomic<int> max_depth{0};
+
+  Builder(const std::vector<PrimBox>& p, std::vector<uint32_t>& o) : prims(p), order(o) {}
+
+  Box bounds(uint32_t b, uint32_t e, Box* cbox) const {
+    Box bb, cb;
+    bb.reset();
+    cb.reset();
+    for (uint32_t i = b; i < e; ++i) {
+      const PrimBox& p = prims[order[i]];
+      Box pb;
+      std::memcpy(pb.mn, p.mn, sizeof(pb.mn));
+      std::memcpy(pb.mx, p.mx, sizeof(pb.mx));
+      bb.grow(pb);
+      cb.grow(p.c);
+    }
+    if (cbox) *cbox = cb;
+    return bb;
+  }
+
+  // Returns split position in [b,e) or 0 for "make a leaf".
+  uint32_t split(uint32_t b, uint32_t e, const Box& box, const Box& cb, int depth) {
+    const uint32_t n = e - b;
+    if (n <= 1) return 0;
+    int axis = 0;
+    float ext[3];
+    for (int k = 0; k < 3; ++k) ext[k] = cb.mx[k] - cb.mn[k];
+    if (ext[1] > ext[axis]) axis = 1;
+    if (ext[2] > ext[axis]) axis = 2;
+    if (depth >= kMedianDepth || ext[axis] <= 0.0f) {
+      if (n <= (uint32_t)kLeafMax && depth < kMedianDepth) return 0;
+      uint32_t mid = b + n / 2;
+      std::nth_element(order.begin() + b, order.begin() + mid, order.begin() + e,
+                       [&](uint32_t x, uint32_t y) { return prims[x].c[axis] < prims[y].c[axis]; });
+      return mid;
+    }
+    float best_cost = INFINITY;
+    int best_axis = -1, best_bin = -1;
+    for (int a = 0; a < 3; ++a) {
+      if (ext[a] <= 0.0f) continue;
+      Box bin_box[kBins];
+      uint32_t bin_n[kBins] = {};
+      for (int i = 0; i < kBins; ++i) bin_box[i].reset();
+      const float scale = kBins / ext[a];
+      for (uint32_t i = b; i < e; ++i) {
+        const PrimBox& p = prims[order[i]];
+        int bi = std::min(kBins - 1, (int)((p.c[a] - cb.mn[a]) * scale));
+        bi = std::max(0, bi);
+        Box pb;
+        std::memcpy(pb.mn, p.mn, sizeof(pb.mn));
+        std::memcpy(pb.mx, p.mx, sizeof(pb.mx));
+        bin_box[bi].grow(pb);
+        bin_n[bi]++;
+      }
+      float right_area[kBins];
+      uint32_t right_n[kBins];
+      Box acc;
+      acc.reset();
+      uint32_t cnt = 0;
+      for (int i = kBins - 1; i > 0; --i) {
+        acc.grow(bin_box[i]);
+        cnt += bin_n[i];
+        right_area[i] = acc.area();
+        right_n[i] = cnt;
+      }
+      acc.reset();
+      cnt = 0;
+      for (int i = 0; i < kBins - 1; ++i) {
+        acc.grow(bin_box[i]);
+        cnt += bin_n[i];
+        if (cnt == 0 || right_n[i + 1] == 0) continue;
+        float c = acc.area() * cnt + right_area[i + 1] * right_n[i + 1];
+        if (c < best_cost) { best_cost = c; best_axis = a; best_bin = i; }
+      }
+    }
+    const float parent_area = std::max(box.area(), 1e-30f);
+    const float split_cost = kTraversalCost + kIsectCost * best_cost / parent_area;
+    const float leaf_cost = kIsectCost * n;
+    if (best_axis < 0 || (n <= (uint32_t)kLeafMax && leaf_cost <= split_cost)) {
+      if (n <= (uint32_t)kLeafMax) return 0;
+      uint32_t mid = b + n / 2;
+      std::nth_element(order.begin() + b, order.begin() + mid, order.begin() + e,
+                       [&](uint32_t x, uint32_t y) { return prims[x].c[axis] < prims[y].c[axis]; });
+      return mid;
+    }
+    const float scale = kBins / ext[best_axis];
+    auto it = std::partition(order.begin() + b, order.begin() + e, [&](uint32_t x) {
+      int bi = std::min(kBins - 1, (int)((prims[x].c[best_axis] - cb.mn[best_axis]) * scale));
+      return std::max(0, bi) <= best_bin;
+    });
+    uint32_t mid = (uint32_t)(it - order.begin());
+    if (mid == b || mid == e) mid = b + n / 2;
+    return mid;
+  }
+
+  // Builds the subtree for [b,e) into `out` (its own node vector, root first).
+  void build_range(uint32_t b, uint32_t e, int depth0, std::vector<BNode>& out) {
+    struct Task { uint32_t b, e; int node; int depth; };
+    std::vector<Task> stack;
+    out.emplace_back();
+    stack.push_back({b, e, 0, depth0});
+    while (!stack.empty()) {
+      Task t = stack.back();
+      stack.pop_back();
+      Box cb;
+      Box box = bounds(t.b, t.e, &cb);
+      out[t.node].box = box;
+      out[t.node].depth = t.depth;
+      int d = max_depth.load();
+      while (t.depth > d && !max_depth.compare_exchange_weak(d, t.depth)) {}
+      uint32_t mid = split(t.b, t.e, box, cb, t.depth);
+      if (mid == 0) {
+        out[t.node].first = t.b;
+        out[t.node].count = t.e - t.b;
+        continue;
+      }
+      int l = (int)out.size();
+      out.emplace_back();
+      int r = (int)out.size();
+      out.emplace_back();
+      out[t.node].left = l;
+      out[t.node].right = r;
+      stack.push_back({mid, t.e, r, t.depth + 1});
+      stack.push_back({t.b, mid, l, t.depth + 1});
+    }
+  }
+};
+
+inline float round_down(double x) {
+  float f = (float)x;
+  if ((double)f > x) f = std::nextafter(f, -INFINITY);
+  return f;
+}
+inline float round_up(double x) {
+  float f = (float)x;
+  if ((double)f < x) f = std::nextafter(f, INFINITY);
+  return f;
+}
+
+}  // namespace
+
+void prim_box_from_double(PrimBox& p, const double* mn, const double* mx) {
+  for (int k = 0; k < 3; ++k) {
+    p.mn[k] = round_down(mn[k]);
+    p.mx[k] = round_up(mx[k]);
+    p.c[k] = (float)(0.5 * (mn[k] + mx[k]));
+  }
+}
+
+bool build_bvh(const std::vector<PrimBox>& prims, BvhResult& out, std::string& err) {
+  out = BvhResult();
+  const uint32_t n = (uint32_t)prims.size();
+  if (n == 0) return true;
+  if (n >= (1u << 28)) {
+    err = "too many primitives for the leaf encoding (max 2^28)";
+    return false;
+  }
+  out.order.resize(n);
+  for (uint32_t i = 0; i < n; ++i) out.order[i] = i;
+  Builder B(prims, out.order);
+
+  // Top levels single-threaded down to ~4x hardware threads subtrees, then
+  // subtrees in parallel, then stitched into one node vector.
+  std::vector<BNode>& nodes = B.nodes;
+  struct Pending { uint32_t b, e; int node; int depth; };
+  std::vector<Pending> leaves_to_build;
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  const uint32_t par_threshold = std::max<uint32_t>(4096, n / (4 * hw));
+  {
+    struct Task { uint32_t b, e; int node; int depth; };
+    std::vector<Task> stack;
+    nodes.emplace_back();
+    stack.push_back({0, n, 0, 0});
+    while (!stack.empty()) {
+      Task t = stack.back();
+      stack.pop_back();
+      if (t.e - t.b <= par_threshold && n > par_threshold) {
+        leaves_to_build.push_back({t.b, t.e, t.node, t.depth});
+        continue;
+      }
+      Box cb;
+      Box box = B.bounds(t.b, t.e, &cb);
+      nodes[t.node].box = box;
+      nodes[t.node].depth = t.depth;
+      uint32_t mid = B.split(t.b, t.e, box, cb, t.depth);
+      if (mid == 0) {
+        nodes[t.node].first = t.b;
+        nodes[t.node].count = t.e - t.b;
+        continue;
+      }
+      int l = (int)nodes.size();
+      nodes.emplace_back();
+      int r = (int)nodes.size();
+      nodes.emplace_back();
+      nodes[t.node].left = l;
+      nodes[t.node].right = r;
+      stack.push_back({mid, t.e, r, t.depth + 1});
+      stack.push_back({t.b, mid, l, t.depth + 1});
+    }
+  }
+  if (!leaves_to_build.empty()) {
+    std::vector<std::vector<BNode>> parts(leaves_to_build.size());
+    std::atomic<size_t> next{0};
+    std::vector<std::thread> pool;
+    for (unsigned w = 0; w < hw; ++w)
+      pool.emplace_back([&]() {
+        for (size_t i; (i = next.fetch_add(1)) < leaves_to_build.size();)
+          B.build_range(leaves_to_build[i].b, leaves_to_build[i].e, leaves_to_build[i].depth, parts[i]);
+      });
+    for (auto& th : pool) th.join();
+    for (size_t i = 0; i < parts.size(); ++i) {
+      const int base = (int)nodes.size();
+      const int dst = leaves_to_build[i].node;
+      std::vector<BNode>& p = parts[i];
+      nodes[dst] = p[0];
+      if (nodes[dst].left >= 0) {
+        nodes[dst].left += base - 1;
+        nodes[dst].right += base - 1;
+      }
+      for (size_t k = 1; k < p.size(); ++k) {
+        BNode q = p[k];
+        if (q.left >= 0) { q.left += base - 1; q.right += base - 1; }
+        nodes.push_back(q);
+      }
+    }
+  }
+  out.max_depth = B.max_depth.load();
+  for (const BNode& b : nodes) out.max_depth = std::max(out.max_depth, b.depth);
+  if (out.max_depth >= kMaxTreeDepth) {
+    err = "BVH deeper than the traversal stack";
+    return false;
+  }
+
+  // Flatten to dual-child device nodes in depth-first order.
+  if (nodes[0].left < 0) {
+    out.root_leaf = leaf_link(nodes[0].first, nodes[0].count);
+    Node dn;
+    const BNode& r = nodes[0];
+    dn.lxy = make_float4(r.box.mn[0], r.box.mx[0], r.box.mn[1], r.box.mx[1]);
+    dn.rxy = make_float4(INFINITY, -INFINITY, INFINITY, -INFINITY);
+    dn.z = make_float4(r.box.mn[2], r.box.mx[2], INFINITY, -INFINITY);
+    dn.link = make_int4(out.root_leaf, out.root_leaf, 0, 0);
+    out.nodes.push_back(dn);
+    out.leaves = 1;
+    return true;
+  }
+  std::vector<int> dev_index(nodes.size(), -1);
+  std::vector<int> stack{0};
+  std::vector<int> order_nodes;
+  while (!stack.empty()) {
+    int i = stack.back();
+    stack.pop_back();
+    dev_index[i] = (int)order_nodes.size();
+    order_nodes.push_back(i);
+    if (nodes[nodes[i].right].left >= 0) stack.push_back(nodes[i].right);
+    if (nodes[nodes[i].left].left >= 0) stack.push_back(nodes[i].left);
+  }
+  out.nodes.resize(order_nodes.size());
+  for (size_t k = 0; k < order_nodes.size(); ++k) {
+    const BNode& p = nodes[order_nodes[k]];
+    const BNode& L = nodes[p.left];
+    const BNode& R = nodes[p.right];
+    Node dn;
+    dn.lxy = make_float4(L.box.mn[0], L.box.mx[0], L.box.mn[1], L.box.mx[1]);
+    dn.rxy = make_float4(R.box.mn[0], R.box.mx[0], R.box.mn[1], R.box.mx[1]);
+    dn.z = make_float4(L.box.mn[2], L.box.mx[2], R.box.mn[2], R.box.mx[2]);
+    int ll = L.left >= 0 ? dev_index[p.left] : leaf_link(L.first, L.count);
+    int rl = R.left >= 0 ? dev_index[p.right] : leaf_link(R.first, R.count);
+    if (L.left < 0) out.leaves++;
+    if (R.left < 0) out.leaves++;
+    dn.link = make_int4(ll, rl, 0, 0);
+    out.nodes[k] = dn;
+  }
+  return true;
+}
+
+}  // namespace mrt

@@ -1,0 +1,144 @@
+// mrt_internal.h — device data layout shared by the host repack and the
+// kernels. Everything here lives in HBM (or constant memory for the small
+// per-scene block) and is read-only while rendering.
+//
+// Layout (all arrays 16-byte aligned, read with 128-bit loads):
+//   nodes   : BVH2 with both child boxes stored in the parent, 64 B per node
+//             (float4 x-y of left, float4 x-y of right, float4 z of both,
+//             int4 child links). A negative link is a leaf:
+//             ~(first_prim << 3 | (count - 1)), up to 8 primitives.
+//   geom    : 48 B per primitive in leaf order. Triangle: (v0, type) (e1, -)
+//             (e2, -). Sphere: (centre, type) (radius, r^2, -, -) (-).
+//   meta    : int4 per primitive in leaf order: (flat id, material, type,
+//             packed rgb8 object colour).
+//   shade   : 64 B per triangle in leaf order: (n0, u0) (n1, u1) (n2, u2)
+//             (v0, v1, v2, -). Read once per closest hit.
+//   planes  : 2 float4 + int4 per plane.
+//   env     : RGBE texels as uint32; for importance sampling an alias table
+//             (float prob, int alias) over the outcomes of the reference's
+//             two-step lookup and two float4 records per outcome
+//             (direction + pdf, sky radiance of that direction).
+#pragma once
+#include <stdint.h>
+#include <cuda_runtime.h>
+
+namespace mrt {
+
+enum PrimType : int { PRIM_TRI = 0, PRIM_SPHERE = 1 };
+
+constexpr int kLeafMax = 8;          // primitives per leaf (3-bit count)
+constexpr int kStackSize = 64;       // traversal stack; the builder bounds depth below it
+constexpr int kMaxTreeDepth = 60;
+constexpr float kTMin = 0.001f;      // IT_MIN (minirt.h:44)
+constexpr float kTMax = 1000.0f;     // IT_MAX and the initial closest_t (hit_register.c:21)
+
+struct __align__(16) Node {
+  float4 lxy;   // left  (min.x, max.x, min.y, max.y)
+  float4 rxy;   // right (min.x, max.x, min.y, max.y)
+  float4 z;     // (left min.z, left max.z, right min.z, right max.z)
+  int4 link;    // (left, right, -, -)
+};
+
+__host__ __device__ inline int leaf_link(uint32_t first, uint32_t count) {
+  return ~(int)((first << 3) | (count - 1));
+}
+
+struct MaterialD {
+  float color[3];        // color_value / 255
+  float metallic;
+  float roughness;
+  float ior;
+  float transmission;
+  float ao;
+  float emission_strength;
+  float emission[3];     // emission_color / 255
+  float f0;              // powf(((ior-1)/(ior+1)), 2) (material/utils.c:29-37)
+  float alpha4;          // roughness^4 for the GGX-like sampler (utils.c:47-48)
+};
+
+struct LightD {
+  float pos[3];          // point: position; directional: unit orientation
+  float brightness;
+  float color[3];        // 0..255 scale, as the reference accumulates it
+  float radius;
+  int type;
+  int shadow_sample;
+  int pad[2];
+};
+
+struct PlaneD {
+  float4 pn;             // point.xyz, -
+  float4 nn;             // normal.xyz, -
+  int4 meta;             // flat id, material, -, packed colour
+};
+
+// Everything a kernel needs, passed by value (kernel parameter space).
+struct SceneView {
+  const Node* nodes;
+  const float4* geom;
+  const int4* meta;
+  const float4* shade;
+  const PlaneD* planes;
+  const MaterialD* mats;
+  const LightD* lights;
+  int n_nodes;
+  int n_prims;
+  int n_planes;
+  int n_mats;
+  int n_lights;
+  int one_sided;
+  int root_leaf;         // scene with a single leaf: the link of that leaf, else 0
+  int has_bvh;
+  // camera (viewport.c:38-87), float
+  float cam[3];
+  float pixel00[3];
+  float pdu[3];
+  float pdv[3];
+  float defocus_u[3];
+  float defocus_v[3];
+  float defocus_angle;
+  int width;
+  int height;
+  int max_bounces;
+  float ior_all;
+  // ambient / sky
+  float amb_const[3];    // colour * ratio / 255 when there is no sky texture
+  const uint32_t* rgbe;
+  int env_w;
+  int env_h;
+  float env_scale_exp;   // powf(2, exposure) or 1 (get_hdr_value.c:47-53)
+  int env_exposure_zero;
+  float env_inv_gamma;   // 1/gamma, 1 = linear
+  int has_env;           // sky texture present
+  int env_nee;           // importance-sampling tables present
+  const float2* alias;   // (prob, alias as int bits), n_env_outcomes entries
+  const float4* env_rec0;  // per outcome: direction .xyz, pdf
+  const float4* env_rec1;  // per outcome: sky radiance of that direction (unclamped) .rgb
+  int n_env_outcomes;
+  int env_lookup;        // 1: sample with the two-step inverse-CDF tables instead
+  const float* pdf_joint;  // W*H   (calc_pdf.c:93)
+  const float* cdf_m_inv;  // H     (calc_cdf.c:39)
+  const float* cdf_c_inv;  // W*H   (calc_cdf.c:112)
+  // caustics (photon hash grid)
+  int caustic;
+  int knn;
+  float caustic_radius2; // compared against the k-th squared distance (get_caustic.c:45)
+  float inv_norm;        // 1 / norm_factor
+  const float4* photon_pos;    // sorted by cell
+  const float4* photon_pow;
+  const uint32_t* cell_start;  // grid cells, cell_start[c]..cell_start[c+1]
+  float grid_min[3];
+  float grid_inv_cell;
+  int grid_dim[3];
+  float grid_cell;
+  int caustic_mode;      // 0 kNN, 1 fixed radius
+  float fixed_radius2;
+  int n_photons;
+};
+
+// Device status word bits -> mrt_status on the host.
+enum StatusBits : int {
+  ST_STACK = 1, ST_BUDGET = 2, ST_QUEUE = 4, ST_ABORT = 8,
+};
+
+}  // namespace mrt

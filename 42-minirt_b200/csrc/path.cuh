@@ -1,0 +1,163 @@
+// path.cuh — one camera path through the reference's estimator
+// (calc_one_sample_task -> path_trace -> material_manager_v3), in float.
+#pragma once
+#include "caustic.cuh"
+#include "shade.cuh"
+
+namespace mrt {
+
+struct PathCounters {
+  uint32_t segments;
+  uint32_t shadow;
+  uint32_t visits;
+};
+
+// importance_sampling (material_default.c:41-69): HDRI next-event estimate.
+__device__ __forceinline__ void env_nee(const SceneView& S, PathState& P, const Surf& s,
+                                        int* status, PathCounters& C) {
+  const int k = env_sample(S, P.rng);
+  const float4 e = __ldg(S.env_rec0 + k);
+  const float3 dir = f3(e.x, e.y, e.z);
+  P.d = dir;
+  C.shadow++;
+  if (any_hit(S, s.p, dir, INFINITY, status)) return;
+  float ct = dot(s.n, dir);
+  float pdf = e.w;
+  if (pdf <= 0.0f) return;
+  const float4 r = __ldg(S.env_rec1 + k);
+  float3 rad = f3(r.x, r.y, r.z);
+  if (s.mat >= 0) rad = rad * S.mats[s.mat].ao;
+  rad = rad * P.power;
+  rad = rad * (ct / pdf);
+  P.acc = P.acc + rad;
+  P.power = P.power * (1.0f - ct);
+}
+
+// default_mat (material_default.c:71-92).
+__device__ __forceinline__ void default_mat(const SceneView& S, PathState& P, const Surf& s,
+                                            int* status, PathCounters& C) {
+  float3 direct = compute_light(S, P.rng, s, status, C.shadow);
+  float3 caus = caustic_estimate(S, s.p);
+  float3 total = direct + caus;
+  P.acc = P.acc + (s.color * P.power) * total;
+  P.power = P.power * s.color;
+  if (S.env_nee) env_nee(S, P, s, status, C);
+  P.d = cos_hemisphere(P.rng, s.n);
+}
+
+// dielectric_mat (dielectric.c:37-64) with reflected_dielectric_color (:15-33).
+__device__ __forceinline__ void dielectric_mat(const SceneView& S, const MaterialD& M, PathState& P,
+                                               const Surf& s, int* status, PathCounters& C) {
+  if (M.ior > 0.0f) {
+    float ct = -dot(unit(P.d), s.n);
+    float refl = M.f0 + (1.0f - M.f0) * pow5(1.0f - ct);
+    if (refl >= P.rng.next() && M.ior != 1.0f) {
+      float3 m = M.roughness > 0.0f ? ggx_sample(P.rng, s.n, M.alpha4) : s.n;
+      P.d = unit(P.d - m * (2.0f * dot(P.d, m)));
+    } else if (M.transmission == 1.0f) {
+      refract(S, M, P, s);
+    } else if (M.transmission == 0.0f) {
+      default_mat(S, P, s, status, C);
+    } else if (M.transmission < P.rng.next()) {
+      default_mat(S, P, s, status, C);
+    } else {
+      refract(S, M, P, s);
+    }
+  } else {
+    default_mat(S, P, s, status, C);
+  }
+}
+
+// material_manager_v3 (path_trace.c:15-35).
+__device__ __forceinline__ void material_manager(const SceneView& S, PathState& P, const Surf& s,
+                                                 int* status, PathCounters& C) {
+  if (s.mat < 0) {
+    default_mat(S, P, s, status, C);
+    return;
+  }
+  const MaterialD& M = S.mats[s.mat];
+  if (M.emission_strength > 0.0f)
+    P.acc = P.acc + (ld3(M.emission) * M.emission_strength) * P.power;
+  if (M.metallic == 1.0f) metallic(M, P, s);
+  else if (M.metallic == 0.0f) dielectric_mat(S, M, P, s, status, C);
+  else if (M.metallic > P.rng.next()) metallic(M, P, s);
+  else dielectric_mat(S, M, P, s, status, C);
+}
+
+// Camera ray of calc_one_sample_task (calc_sample.c:44-59) plus the shared
+// (render.c:33) or per-pixel sub-pixel offset, and focus.c:31 defocus.
+__device__ __forceinline__ void camera_ray(const SceneView& S, PathState& P, uint32_t pixel,
+                                           float ox, float oy) {
+  float3 orig = ld3(S.cam);
+  if (S.defocus_angle > 0.0f) {
+    float px, py;
+    for (int it = 0; it < 64; ++it) {       // rejection in the unit disk, bounded
+      px = -1.0f + P.rng.next() * 2.0f;
+      py = -1.0f + P.rng.next() * 2.0f;
+      if (px * px + py * py < 1.0f) break;
+      px = py = 0.0f;
+    }
+    orig = orig + ld3(S.defocus_u) * px + ld3(S.defocus_v) * py;
+  }
+  float fx = (float)(pixel % (uint32_t)S.width) + ox;
+  float fy = (float)(pixel / (uint32_t)S.width) + oy;
+  P.o = orig;
+  P.d = ld3(S.pixel00) + ld3(S.pdu) * fx + ld3(S.pdv) * fy - orig;
+}
+
+// path_trace + add_skybox (path_trace.c:37-76). render_mode 2 returns the
+// normal colour of the first hit (path_trace_normal, :78-89); render_mode 1
+// returns the node-visit count in .x (path_trace_bvh, :91-102).
+__device__ __forceinline__ float3 trace_path(const SceneView& S, PathState& P, int max_depth,
+                                             int render_mode, int* status, PathCounters& C) {
+  P.power = f3(1.f, 1.f, 1.f);
+  P.acc = f3(0.f, 0.f, 0.f);
+  P.last_mat = -1;
+  if (render_mode != 0) {
+    HitInfo h;
+    int visits = 0;
+    bool hit = closest_hit<true>(S, P.o, P.d, h, visits, status);
+    C.segments++;
+    C.visits += visits;
+    if (render_mode == 1) return f3(hit ? (float)visits : -1.0f, 0.f, 0.f);
+    if (!hit) return f3(0.f, 0.f, 0.f);
+    return make_surf(S, h, P.o, P.d, 2).color;
+  }
+  while (--max_depth >= 0) {
+    HitInfo h;
+    int visits = 0;
+    C.segments++;
+    bool hit = closest_hit<true>(S, P.o, P.d, h, visits, status);
+    C.visits += visits;
+    if (!hit) {
+      float3 bg = background(S, P.d, true);
+      if (P.last_mat >= 0) bg = bg * S.mats[P.last_mat].ao;
+      P.acc = P.acc + bg * P.power;
+      break;
+    }
+    Surf s = make_surf(S, h, P.o, P.d, 0);
+    P.o = s.p;
+    P.last_mat = s.mat;
+    material_manager(S, P, s, status, C);
+    // Every later term is multiplied by the path power: a path whose power
+    // reached exactly zero contributes nothing more.
+    if (P.power.x == 0.0f && P.power.y == 0.0f && P.power.z == 0.0f) break;
+  }
+  return P.acc;
+}
+
+// Sub-pixel offset of a sample: shared by every pixel of the sample
+// (draw_pixels, render.c:33) or per pixel, from the path's own stream.
+__device__ __forceinline__ void sample_offset(uint64_t seed, uint32_t sample, int jitter, Rng& rng,
+                                              float& ox, float& oy) {
+  if (jitter == 0) {
+    Rng j{path_seed(seed, 0xFFFFFFFFu, sample)};
+    ox = j.next();
+    oy = j.next();
+  } else {
+    ox = rng.next();
+    oy = rng.next();
+  }
+}
+
+}  // namespace mrt

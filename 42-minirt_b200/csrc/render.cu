@@ -1,0 +1,168 @@
+// render.cu — the plain megakernel form and the first-hit probe kernel.
+//
+// Megakernel: one thread = one camera path (pixel, sample), all bounces in
+// registers, one vector atomic into the float4 accumulator at the end.
+// Threads are laid out so that a warp covers an 8x4 pixel tile of one
+// sample (coherent primary rays), and samples vary slowest.
+#include "kernels.h"
+#include "path.cuh"
+
+namespace mrt {
+
+__device__ __forceinline__ uint32_t tile_pixel(uint32_t lin, int W, int H) {
+  // 8x4 tiles in row-major tile order; ragged edge tiles fall back to row-major
+  const uint32_t tw = 8, th = 4;
+  const uint32_t tiles_x = (W + tw - 1) / tw;
+  const uint32_t full_h = (H / th) * th;
+  const uint32_t full_rows_pixels = full_h * W;
+  if (lin < full_rows_pixels && (W % tw) == 0) {
+    uint32_t tile = lin / (tw * th), in = lin % (tw * th);
+    uint32_t tx = tile % tiles_x, ty = tile / tiles_x;
+    return (ty * th + in / tw) * W + tx * tw + in % tw;
+  }
+  return lin;
+}
+
+template <bool kCount, int kBlock>
+__global__ void __launch_bounds__(kBlock) megakernel(SceneView S, LaunchParams L, float4* accum,
+                                                   int* depth, int* status,
+                                                   unsigned long long* counters) {
+  const uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  PathCounters C{0, 0, 0};
+  if (idx < L.n_paths) {
+    const uint32_t npix = (uint32_t)S.width * (uint32_t)S.height;
+    const uint32_t lin = (uint32_t)(idx % npix);
+    const uint32_t sample = L.sample_base + (uint32_t)(idx / npix);
+    const uint32_t pixel = tile_pixel(lin, S.width, S.height);
+    PathState P;
+    P.rng.s = path_seed(L.seed, pixel, sample);
+    float ox, oy;
+    if (L.has_offset) { ox = L.ox; oy = L.oy; }
+    else sample_offset(L.seed, sample, L.jitter, P.rng, ox, oy);
+    camera_ray(S, P, pixel, ox, oy);
+    float3 c = trace_path(S, P, L.max_bounces, L.render_mode, status, C);
+    if (L.render_mode == 1) {
+      depth[pixel] = (int)c.x;
+    } else {
+      atomicAdd(accum + pixel, make_float4(c.x, c.y, c.z, 1.0f));
+    }
+  }
+  if (kCount) {
+    // warp-aggregated counters
+    unsigned long long seg = C.segments, sh = C.shadow, vi = C.visits;
+    for (int off = 16; off > 0; off >>= 1) {
+      seg += __shfl_down_sync(0xffffffffu, seg, off);
+      sh += __shfl_down_sync(0xffffffffu, sh, off);
+      vi += __shfl_down_sync(0xffffffffu, vi, off);
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicAdd(counters + 0, seg);
+      atomicAdd(counters + 1, sh);
+      atomicAdd(counters + 2, vi);
+    }
+  }
+}
+
+__global__ void first_hit_kernel(SceneView S, const double* rays, int64_t n, HitOut* out,
+                                 int* status) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double* r = rays + 6 * i;
+  float3 o = f3((float)r[0], (float)r[1], (float)r[2]);
+  float3 d = f3((float)r[3], (float)r[4], (float)r[5]);
+  HitInfo h;
+  int visits = 0;
+  HitOut res;
+  bool hit = closest_hit<true>(S, o, d, h, visits, status);
+  res.visits = visits;
+  if (!hit) {
+    res.prim = -1;
+    res.front_face = 0;
+    res.t = res.u = res.v = 0.f;
+    res.n[0] = res.n[1] = res.n[2] = 0.f;
+    res.p[0] = res.p[1] = res.p[2] = 0.f;
+  } else {
+    Surf s = make_surf(S, h, o, d, 0);
+    res.prim = h.prim >= 0 ? __ldg(S.meta + h.prim).x : S.planes[-1 - h.prim].meta.x;
+    res.front_face = s.front;
+    res.t = h.t;
+    res.u = h.u;
+    res.v = h.v;
+    res.n[0] = s.n.x; res.n[1] = s.n.y; res.n[2] = s.n.z;
+    res.p[0] = s.p.x; res.p[1] = s.p.y; res.p[2] = s.p.z;
+  }
+  out[i] = res;
+}
+
+// Adds the float accumulator into a double t_fcolor buffer (device side) and clears it.
+__global__ void accumulate_double_kernel(float4* accum, double* out, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 a = accum[i];
+  out[3 * i] += a.x;
+  out[3 * i + 1] += a.y;
+  out[3 * i + 2] += a.z;
+  accum[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+}
+
+__global__ void accum_to_rgb_kernel(const float4* accum, float* rgb, int n) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 a = accum[i];
+  rgb[3 * i] = a.x;
+  rgb[3 * i + 1] = a.y;
+  rgb[3 * i + 2] = a.z;
+}
+
+__global__ void env_sample_kernel(SceneView S, int64_t n, uint64_t seed, int* k_out, float4* out) {
+  int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  Rng rng{path_seed(seed, (uint32_t)i, (uint32_t)(i >> 32))};
+  const int k = env_sample(S, rng);
+  k_out[i] = k;
+  out[i] = __ldg(S.env_rec0 + k);
+}
+
+cudaError_t launch_env_sample(const SceneView& S, int64_t n, uint64_t seed, int* k_out, float4* out,
+                              cudaStream_t st) {
+  env_sample_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(S, n, seed, k_out, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_megakernel(const SceneView& S, const LaunchParams& L, float4* accum, int* depth,
+                              int* status, unsigned long long* counters, int block,
+                              cudaStream_t st) {
+  if (L.n_paths == 0) return cudaSuccess;
+  block = block > 0 ? block : 128;
+  const unsigned grid = (unsigned)((L.n_paths + block - 1) / block);
+#define MRT_MK(B)                                                                          \
+  if (block <= B) {                                                                        \
+    if (counters) megakernel<true, B><<<grid, block, 0, st>>>(S, L, accum, depth, status, counters); \
+    else megakernel<false, B><<<grid, block, 0, st>>>(S, L, accum, depth, status, counters);      \
+    return cudaGetLastError();                                                             \
+  }
+  MRT_MK(64)
+  MRT_MK(128)
+  MRT_MK(256)
+#undef MRT_MK
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_first_hit(const SceneView& S, const double* rays, int64_t n, HitOut* out,
+                             int* status, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  first_hit_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(S, rays, n, out, status);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_accumulate_double(float4* accum, double* out, int n, cudaStream_t st) {
+  accumulate_double_kernel<<<(n + 255) / 256, 256, 0, st>>>(accum, out, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_accum_to_rgb(const float4* accum, float* rgb, int n, cudaStream_t st) {
+  accum_to_rgb_kernel<<<(n + 255) / 256, 256, 0, st>>>(accum, rgb, n);
+  return cudaGetLastError();
+}
+
+}  // namespace mrt

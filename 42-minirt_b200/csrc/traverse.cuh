@@ -1,0 +1,218 @@
+// traverse.cuh — closest-hit and any-hit queries over the BVH2 + planes.
+//
+// Semantics follow hit_register_all (hit_register.c:79-120): BVH primitives
+// (spheres, triangles) count when t in [0.001, 1000) (valid_t.c:16 and the
+// closest_t = 1000 start, hit_register.c:21), then every infinite plane is
+// tested and replaces the BVH hit only with a strictly smaller t
+// (hit_plane.c:43-71, t in [0.001, 1000]). The tree is walked near child
+// first with boxes culled beyond the best t; the stack lives in registers /
+// local memory (64 entries; the builder keeps the depth below that).
+#pragma once
+#include "device_common.cuh"
+
+namespace mrt {
+
+struct HitInfo {
+  float t;
+  float u, v;        // barycentrics (triangles)
+  int prim;          // leaf-order primitive index, -1 - plane index, or INT_MIN for a miss
+};
+
+constexpr int kMiss = -2147483647 - 1;
+
+__device__ __forceinline__ float4 ldg4(const float4* p) { return __ldg(p); }
+__device__ __forceinline__ int4 ldg4(const int4* p) { return __ldg(p); }
+
+// Slab test against one child box; returns entry distance or +inf.
+__device__ __forceinline__ float box_hit(float x0, float x1, float y0, float y1, float z0, float z1,
+                                         float3 oi, float3 inv, float tmax) {
+  // t = b * inv - o * inv, NaN-tolerant through fminf/fmaxf
+  float tx0 = fmaf(x0, inv.x, -oi.x), tx1 = fmaf(x1, inv.x, -oi.x);
+  float ty0 = fmaf(y0, inv.y, -oi.y), ty1 = fmaf(y1, inv.y, -oi.y);
+  float tz0 = fmaf(z0, inv.z, -oi.z), tz1 = fmaf(z1, inv.z, -oi.z);
+  float tn = fmaxf(fmaxf(fminf(tx0, tx1), fminf(ty0, ty1)), fmaxf(fminf(tz0, tz1), 0.0f));
+  float tf = fminf(fminf(fmaxf(tx0, tx1), fmaxf(ty0, ty1)), fminf(fmaxf(tz0, tz1), tmax));
+  return tn <= tf ? tn : INFINITY;
+}
+
+// Moller-Trumbore with the reference's epsilon and windows (hit_triangle.c:38-93).
+__device__ __forceinline__ bool tri_hit(const float4& a, const float4& b, const float4& c, float3 o,
+                                        float3 d, int one_sided, float tbest, float& t, float& u,
+                                        float& v) {
+  float3 v0 = f3(a.x, a.y, a.z), e1 = f3(b.x, b.y, b.z), e2 = f3(c.x, c.y, c.z);
+  float3 h = cross(d, e2);
+  float det = dot(e1, h);
+  if (one_sided ? (det < 1e-6f) : (fabsf(det) < 1e-6f)) return false;
+  float f = 1.0f / det;
+  float3 s = o - v0;
+  u = f * dot(s, h);
+  if (u < 0.0f || u > 1.0f) return false;
+  float3 q = cross(s, e1);
+  v = f * dot(d, q);
+  if (v < 0.0f || u + v > 1.0f) return false;
+  t = f * dot(e2, q);
+  return t >= kTMin && t < tbest;
+}
+
+// Sphere: quadratic of init_sphere_quadratic (quadratique.c:32) in a
+// cancellation-free form, nearer root first then the farther one (valid_t.c:16).
+__device__ __forceinline__ bool sphere_hit(const float4& a, const float4& b, float3 o, float3 d,
+                                           float tbest, float& t) {
+  float3 oc = o - f3(a.x, a.y, a.z);
+  float A = dot(d, d);
+  float bh = dot(d, oc);
+  float3 l = oc - d * (bh / A);
+  float disc = A * (b.y - dot(l, l));
+  if (disc < 0.0f) return false;
+  float sq = sqrtf(disc);
+  float qv = -(bh + copysignf(sq, bh));
+  float c = dot(oc, oc) - b.y;
+  float r0 = qv / A, r1 = (qv != 0.0f) ? c / qv : r0;
+  float t0 = fminf(r0, r1), t1 = fmaxf(r0, r1);
+  if (t0 >= kTMin && t0 <= kTMax) t = t0;
+  else if (t1 >= kTMin && t1 <= kTMax) t = t1;
+  else return false;
+  return t < tbest;
+}
+
+__device__ __forceinline__ bool plane_hit(const PlaneD& p, float3 o, float3 d, float& t) {
+  float3 n = f3(p.nn.x, p.nn.y, p.nn.z);
+  float denom = dot(n, d);
+  if (fabsf(denom) < 1e-8f) return false;
+  t = dot(f3(p.pn.x, p.pn.y, p.pn.z) - o, n) / denom;
+  return t >= kTMin && t <= kTMax;
+}
+
+// Closest hit. `visits` counts node fetches (heat-map / roofline counter).
+// Returns false on a miss. `status` receives ST_BUDGET if the bounded loop
+// ran out (a corrupted tree), never hangs.
+template <bool kCount>
+__device__ __forceinline__ bool closest_hit(const SceneView& S, float3 o, float3 d, HitInfo& hit,
+                                            int& visits, int* status) {
+  float tbest = kTMax;
+  int best = kMiss;
+  float bu = 0.f, bv = 0.f;
+  if (S.has_bvh) {
+    float3 inv = f3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+    float3 oi = o * inv;
+    int stack[kStackSize];
+    int sp = 0;
+    int cur = 0;
+    int budget = 4 * S.n_nodes + 4 * S.n_prims + 64;
+    while (true) {
+      if (--budget < 0) {
+        if (status) atomicOr(status, ST_BUDGET);
+        break;
+      }
+      if (cur >= 0) {
+        const Node* nd = S.nodes + cur;
+        float4 lxy = ldg4(&nd->lxy), rxy = ldg4(&nd->rxy), z = ldg4(&nd->z);
+        int4 ln = ldg4(&nd->link);
+        if (kCount) visits++;
+        float tl = box_hit(lxy.x, lxy.y, lxy.z, lxy.w, z.x, z.y, oi, inv, tbest);
+        float tr = box_hit(rxy.x, rxy.y, rxy.z, rxy.w, z.z, z.w, oi, inv, tbest);
+        bool hl = tl < INFINITY, hr = tr < INFINITY;
+        if (hl && hr) {
+          int nearc = tl <= tr ? ln.x : ln.y;
+          int farc = tl <= tr ? ln.y : ln.x;
+          if (sp < kStackSize) stack[sp++] = farc;
+          else if (status) atomicOr(status, ST_STACK);
+          cur = nearc;
+          continue;
+        }
+        if (hl) { cur = ln.x; continue; }
+        if (hr) { cur = ln.y; continue; }
+      } else {
+        int code = ~cur;
+        int first = code >> 3, count = (code & 7) + 1;
+        for (int i = first; i < first + count; ++i) {
+          const float4* g = S.geom + 3 * (size_t)i;
+          float4 a = ldg4(g), b = ldg4(g + 1);
+          float t, u = 0.f, v = 0.f;
+          bool ok;
+          if (__float_as_int(a.w) == PRIM_TRI) {
+            float4 c = ldg4(g + 2);
+            ok = tri_hit(a, b, c, o, d, S.one_sided, tbest, t, u, v);
+          } else {
+            ok = sphere_hit(a, b, o, d, tbest, t);
+          }
+          if (ok) { tbest = t; best = i; bu = u; bv = v; }
+        }
+      }
+      if (sp == 0) break;
+      cur = stack[--sp];
+    }
+  }
+  const bool bvh_hit = best != kMiss;
+  for (int i = 0; i < S.n_planes; ++i) {
+    float t;
+    if (plane_hit(S.planes[i], o, d, t) && (!bvh_hit && best == kMiss ? true : t < tbest)) {
+      tbest = t;
+      best = -1 - i;
+    }
+  }
+  hit.t = tbest;
+  hit.u = bu;
+  hit.v = bv;
+  hit.prim = best;
+  return best != kMiss;
+}
+
+// Any hit with t < tmax (shadow rays). Planes first: they are cheap.
+__device__ __forceinline__ bool any_hit(const SceneView& S, float3 o, float3 d, float tmax,
+                                        int* status) {
+  for (int i = 0; i < S.n_planes; ++i) {
+    float t;
+    if (plane_hit(S.planes[i], o, d, t) && t < tmax) return true;
+  }
+  if (!S.has_bvh) return false;
+  float3 inv = f3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+  float3 oi = o * inv;
+  int stack[kStackSize];
+  int sp = 0;
+  int cur = 0;
+  int budget = 4 * S.n_nodes + 4 * S.n_prims + 64;
+  const float tlim = fminf(tmax, kTMax);
+  while (true) {
+    if (--budget < 0) {
+      if (status) atomicOr(status, ST_BUDGET);
+      return false;
+    }
+    if (cur >= 0) {
+      const Node* nd = S.nodes + cur;
+      float4 lxy = ldg4(&nd->lxy), rxy = ldg4(&nd->rxy), z = ldg4(&nd->z);
+      int4 ln = ldg4(&nd->link);
+      float tl = box_hit(lxy.x, lxy.y, lxy.z, lxy.w, z.x, z.y, oi, inv, tlim);
+      float tr = box_hit(rxy.x, rxy.y, rxy.z, rxy.w, z.z, z.w, oi, inv, tlim);
+      bool hl = tl < INFINITY, hr = tr < INFINITY;
+      if (hl && hr) {
+        if (sp < kStackSize) stack[sp++] = ln.y;
+        else if (status) atomicOr(status, ST_STACK);
+        cur = ln.x;
+        continue;
+      }
+      if (hl) { cur = ln.x; continue; }
+      if (hr) { cur = ln.y; continue; }
+    } else {
+      int code = ~cur;
+      int first = code >> 3, count = (code & 7) + 1;
+      for (int i = first; i < first + count; ++i) {
+        const float4* g = S.geom + 3 * (size_t)i;
+        float4 a = ldg4(g), b = ldg4(g + 1);
+        float t, u, v;
+        bool ok;
+        if (__float_as_int(a.w) == PRIM_TRI) {
+          float4 c = ldg4(g + 2);
+          ok = tri_hit(a, b, c, o, d, S.one_sided, tlim, t, u, v);
+        } else {
+          ok = sphere_hit(a, b, o, d, tlim, t);
+        }
+        if (ok) return true;
+      }
+    }
+    if (sp == 0) return false;
+    cur = stack[--sp];
+  }
+}
+
+}  // namespace mrt

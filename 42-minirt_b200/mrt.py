@@ -107,7 +107,8 @@ class RenderParams(C.Structure):
                 ("max_bounces", C.c_int32), ("form", C.c_int32), ("jitter", C.c_int32),
                 ("render_mode", C.c_int32), ("block_size", C.c_int32),
                 ("queue_capacity", C.c_int32), ("sort_threshold", C.c_int32),
-                ("use_graph", C.c_int32), ("offset", C.POINTER(C.c_double))]
+                ("use_graph", C.c_int32), ("env_sampler", C.c_int32),
+                ("offset", C.POINTER(C.c_double))]
 
 
 class RenderStats(C.Structure):
@@ -148,6 +149,7 @@ SIGNATURES = {
     "mrt_read_depth": (C.c_int, [_P, _P]),
     "mrt_trace_first_hit": (C.c_int, [_P, _P, C.c_int64, _P]),
     "mrt_read_env_tables": (C.c_int, [_P, _P, _P, _P]),
+    "mrt_env_sample": (C.c_int, [_P, C.c_int64, C.c_uint64, C.c_int32, _P, _P]),
     "mrt_photon_count": (C.c_int64, [_P]),
     "mrt_read_photons": (C.c_int, [_P, _P, _P, C.c_int64]),
     "mrt_set_photons": (C.c_int, [_P, _P, _P, C.c_int64]),
@@ -225,11 +227,12 @@ class Context:
     def render(self, spp: int, seed: int = 1, sample_base: int = 0, form: int = FORM_MEGAKERNEL,
                jitter: int = JITTER_SHARED, max_bounces: int = 0, render_mode: int = 0,
                block_size: int = 0, queue_capacity: int = 0, sort_threshold: int = 0,
-               use_graph: int = 0, offset=None) -> RenderStats:
+               use_graph: int = 0, env_sampler: int = 0, offset=None) -> RenderStats:
         p = RenderParams(spp=spp, sample_base=sample_base, seed=seed, max_bounces=max_bounces,
                          form=form, jitter=jitter, render_mode=render_mode,
                          block_size=block_size, queue_capacity=queue_capacity,
-                         sort_threshold=sort_threshold, use_graph=use_graph)
+                         sort_threshold=sort_threshold, use_graph=use_graph,
+                         env_sampler=env_sampler)
         off = None
         if offset is not None:
             off = (C.c_double * 2)(float(offset[0]), float(offset[1]))
@@ -270,6 +273,14 @@ class Context:
         check(self.lib.mrt_read_env_tables(self.h, _ptr(pdf), _ptr(cm), _ptr(cc)),
               "mrt_read_env_tables")
         return pdf, cm, cc
+
+    def env_sample(self, n: int, seed: int = 1, sampler: int = 0):
+        """(outcome index, float4 dir+pdf) of n importance samples."""
+        out = np.zeros((n, 4), np.float32)
+        k = np.zeros(n, np.int32)
+        check(self.lib.mrt_env_sample(self.h, n, seed, sampler, _ptr(k), _ptr(out)),
+              "mrt_env_sample")
+        return k, out
 
     def photon_count(self) -> int:
         n = self.lib.mrt_photon_count(self.h)

@@ -1,0 +1,288 @@
+"""Benchmark of the path-tracing hot path (one JSON line on rank 0).
+
+Metric: Mpaths/s (camera paths through the reference's estimator per second,
+whole job) on the 1920x1080 / 256 spp / depth 12 workload: a 1,310,720
+triangle displaced geodesic sphere with 16 materials under a 2048x1024 RGBE
+sky sampled by importance (seeded synthetic scene; the reference publishes no
+benchmark scene). One step = one pass over the frame at --spp-per-step
+samples per pixel (16 steps = the 256 spp render).
+
+  value       device time (CUDA events on the library's stream) of the timed
+              steps, inputs resident in HBM; the best of the two forms
+              (plain megakernel, wavefront), both reported under "forms".
+  e2e         the same render through the C-ABI a reference host calls:
+              per step a camera upload, the render and a device->host read of
+              the frame accumulated into a pinned double buffer
+              (t_fcolor float_render), wall-clocked.
+  roofline    canonical algorithmic bytes per path (oracle/algorithmic_bytes.json,
+              reference BVH topology) x paths per launch / mean launch time,
+              against the measured HBM copy bandwidth.
+  cpu_baseline the reference's own CPU code (compiled from its sources) on
+              this host's cores, timed in a separate process.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Under torchrun each rank renders its own sample range (weak scaling); the
+frames are summed with one NCCL reduce at the end of the timed region.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO / "42-minirt_b200"))
+
+METRIC = "Mpaths/s and time to relMSE<=1e-3, wavefront vs plain megakernel, 1 B200"
+UNIT = "Mpaths/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c1")
+    ap.add_argument("--spp-per-step", type=int, default=16)
+    ap.add_argument("--forms", default="megakernel,wavefront")
+    ap.add_argument("--cpu-seconds", type=float, default=8.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region (clocks and throttle reasons)."""
+
+    def __init__(self, index: int):
+        self.path = Path(tempfile.mkstemp(suffix=".csv")[1])
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), f"--query-gpu={q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait()
+        rows = [r.split(", ") for r in self.path.read_text().strip().splitlines() if r.strip()]
+        self.path.unlink(missing_ok=True)
+        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            if len(r) < 9:
+                continue
+            for k, name in enumerate(names):
+                if r[5 + k].strip() == "Active":
+                    reasons.add(name)
+        loaded = sorted(sm)[len(sm) // 2:] if sm else []
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
+                "samples": len(rows)}
+
+
+def cpu_baseline(config: str, seconds: float, steps: int = 1, warmup: int = 0) -> dict | None:
+    """The reference's CPU path, in a fresh process (it forks workers)."""
+    script = REPO / "oracle" / "cpu_baseline.py"
+    if not (REPO / "oracle" / "_ref" / "liboracle_ref.so").exists():
+        return None
+    out = subprocess.run([sys.executable, str(script), "--config", config, "--seconds", str(seconds),
+                          "--steps", str(steps), "--warmup", str(warmup)],
+                         capture_output=True, text=True, timeout=1800)
+    for line in out.stdout.splitlines()[::-1]:
+        if line.startswith("{"):
+            return json.loads(line)
+    raise RuntimeError("cpu baseline failed: " + out.stderr[-2000:])
+
+
+def run_reference_arm(a) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    r = cpu_baseline(a.config, a.cpu_seconds, steps=a.steps, warmup=a.warmup)
+    if r is None:
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "oracle/_ref/liboracle_ref.so (the reference compiled from its "
+                          "sources) is not present"}))
+        return
+    line = {"impl": "reference", "metric": METRIC, "value": r["mpaths_s"], "unit": UNIT,
+            "n_gpus": 0, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": 1000.0 * r["seconds"] / max(a.steps, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(a, None),
+            "cpu_baseline": {"value": r["mpaths_s"], "unit": UNIT, "cores": r["procs"],
+                             "kind": "reference", "sample": r["sample"]},
+            "e2e": {"value": r["mpaths_s"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def workload_config(a, sc) -> dict:
+    return {"workload": f"{a.config}: 1920x1080, 256 spp, depth 12, 1,310,720-triangle displaced "
+                        "geodesic sphere, 16 materials, 2048x1024 RGBE sky with importance sampling"
+                        if a.config == "c1" else a.config,
+            "spp_per_step": a.spp_per_step,
+            "l2": "scene arrays (BVH, triangles, shading, sky tables) exceed the 126 MB L2",
+            "parallelism": f"sample-parallel dp{a.gpus}"}
+
+
+def main() -> int:
+    a = parse()
+    if a.impl == "reference":
+        run_reference_arm(a)
+        return 0
+    import mrt
+    import scenes
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as tdist
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+        dist = tdist
+
+    # CPU baseline first, before this process touches CUDA (it forks).
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        cpu = cpu_baseline(a.config, a.cpu_seconds)
+
+    sc = scenes.CONFIGS[a.config]()
+    ctx = mrt.Context(sc.width, sc.height, device=local)
+    t0 = time.perf_counter()
+    ctx.build(sc)
+    build_s = time.perf_counter() - t0
+    npix = sc.width * sc.height
+    spp = a.spp_per_step
+    paths_per_step = npix * spp
+    algo = json.loads((REPO / "oracle" / "algorithmic_bytes.json").read_text())
+    bpp = algo["configs"][a.config]["bytes_per_path"]
+    peaks = {}
+    pk = REPO / "MEASURED_PEAKS.json"
+    if pk.exists():
+        peaks = json.loads(pk.read_text())
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    hbm_src = "of measured" if "hbm_gbs" in peaks else "of fallback"
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    forms = {}
+    form_ids = {"megakernel": mrt.FORM_MEGAKERNEL, "wavefront": mrt.FORM_WAVEFRONT}
+    clocks = Clocks(local)
+    launches_total = 0
+    best = None
+    for name in a.forms.split(","):
+        fid = form_ids[name]
+        try:
+            ctx.clear()
+            for w in range(a.warmup):
+                ctx.render(spp, seed=99, sample_base=w * spp, form=fid)
+        except mrt.MRTError as e:
+            forms[name] = {"error": str(e)[:200]}
+            continue
+        ctx.clear()
+        barrier()
+        ms = 0.0
+        launches = 0
+        base = rank * a.steps * spp
+        for s in range(a.steps):
+            st = ctx.render(spp, seed=1, sample_base=base + s * spp, form=fid)
+            ms += st.ms
+            launches += st.kernel_launches
+        barrier()
+        t_max = ms
+        if dist:
+            import torch
+            t = torch.tensor([ms], device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            t_max = float(t.item())
+        total_paths = paths_per_step * a.steps * world
+        mps = total_paths / (t_max / 1000.0) / 1e6
+        per_launch_ms = ms / max(launches, 1)
+        forms[name] = {"value": mps, "ms_per_step": t_max / a.steps, "launches": launches,
+                       "launch_ms": per_launch_ms}
+        if best is None or mps > forms[best]["value"]:
+            best = name
+        launches_total = launches
+    clk = clocks.stop()
+    if best is None:
+        raise SystemExit("no render form ran: " + json.dumps(forms))
+
+    # end to end through the C-ABI with host buffers, best form
+    fid = form_ids[best]
+    host = np.zeros(npix * 3, np.float64)
+    cam = sc.desc().camera
+    ctx.clear()
+    barrier()
+    t0 = time.perf_counter()
+    for s in range(a.steps):
+        ctx.set_camera(cam, sc.ior_all, sc.ambient_ratio)
+        ctx.render(spp, seed=2, sample_base=rank * a.steps * spp + s * spp, form=fid)
+        ctx.accumulate_double(host)
+    barrier()
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        import torch
+        t = torch.tensor([e2e_s], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+        # the frames of all ranks summed on rank 0 (one NCCL reduce)
+        frame = torch.from_numpy(host.astype(np.float32)).cuda(local)
+        dist.reduce(frame, dst=0)
+    e2e = paths_per_step * a.steps * world / e2e_s / 1e6
+
+    f = forms[best]
+    achieved = bpp * (paths_per_step / max(f["launches"] / a.steps, 1)) / (f["launch_ms"] / 1000.0) / 1e9
+    traffic = None
+    tf = REPO / "profiles" / "traffic.json"
+    if tf.exists():
+        traffic = json.loads(tf.read_text()).get(best)
+    line = {
+        "metric": METRIC, "value": forms[best]["value"], "unit": UNIT, "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": f["ms_per_step"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded generator; the reference publishes no benchmark scene)",
+        "config": workload_config(a, sc), "form": best, "forms": forms,
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": int(__import__("ctypes").sizeof(mrt.Camera)),
+                "d2h_bytes_per_step": int(npix * 3 * 4)},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": traffic, "peak_source": hbm_src,
+                     "bytes_per_path": bpp},
+        "gpu_launches": launches_total,
+        "clocks": clk,
+        "scene_build_s": build_s,
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = {"value": cpu["mpaths_s"], "unit": UNIT, "cores": cpu["procs"],
+                                "kind": "reference", "sample": cpu["sample"]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -38,6 +38,12 @@ extern "C" {
 
 # define MRT_ABI_VERSION 1
 
+# if defined(__GNUC__)
+#  define MRT_API __attribute__((visibility("default")))
+# else
+#  define MRT_API
+# endif
+
 typedef enum mrt_status
 {
 	MRT_OK = 0,
@@ -219,10 +225,12 @@ typedef struct mrt_render_params
 	int32_t		form;           /* mrt_form */
 	int32_t		jitter;         /* mrt_jitter */
 	int32_t		render_mode;    /* 0 path trace, 1 BVH heat map, 2 normals (minirt->render_mode) */
-	int32_t		block_size;     /* 0 = tuned default */
+	int32_t		block_size;     /* threads per block, multiple of 32, <= 256; 0 = tuned default */
 	int32_t		queue_capacity; /* wavefront paths in flight, 0 = tuned default */
 	int32_t		sort_threshold; /* wavefront: sort shading queue above this many paths */
 	int32_t		use_graph;      /* capture the spp loop in a CUDA graph */
+	int32_t		env_sampler;    /* HDRI sampler: 0 alias table, 1 the reference's two-step
+	                             * inverse-CDF lookup (get_dir.c:15-27), same distribution */
 	const double *offset;       /* optional explicit shared jitter (x,y) for spp == 1 */
 }	mrt_render_params;
 
@@ -238,34 +246,34 @@ typedef struct mrt_render_stats
 
 typedef struct mrt_ctx	mrt_ctx;
 
-const char	*mrt_last_error(void);
-int			mrt_version(void);
-int			mrt_device_count(void);
+MRT_API const char	*mrt_last_error(void);
+MRT_API int			mrt_version(void);
+MRT_API int			mrt_device_count(void);
 
 /* init_shader (init_shader.c:133): context + W*H accumulation buffer. */
-mrt_ctx		*mrt_create(int device, int width, int height);
-void		mrt_destroy(mrt_ctx *ctx);
+MRT_API mrt_ctx		*mrt_create(int device, int width, int height);
+MRT_API void		mrt_destroy(mrt_ctx *ctx);
 
 /* convert_scene_build (gpu_scene.c:104): repack, build the BVH, upload,
  * build HDRI sampling tables on the device, emit photons if enabled. */
-int			mrt_scene_build(mrt_ctx *ctx, const mrt_scene_desc *scene);
+MRT_API int			mrt_scene_build(mrt_ctx *ctx, const mrt_scene_desc *scene);
 /* convert_scene (gpu_scene.c:62): camera / ambient ratio / ior only. */
-int			mrt_set_camera(mrt_ctx *ctx, const mrt_camera *camera,
+MRT_API int			mrt_set_camera(mrt_ctx *ctx, const mrt_camera *camera,
 				double ior_all, double ambient_ratio);
 
 /* Render params->spp samples per pixel into the device accumulator. */
-int			mrt_render(mrt_ctx *ctx, const mrt_render_params *params,
+MRT_API int			mrt_render(mrt_ctx *ctx, const mrt_render_params *params,
 				mrt_render_stats *stats);
 /* Zero the device accumulator. */
-int			mrt_clear(mrt_ctx *ctx);
+MRT_API int			mrt_clear(mrt_ctx *ctx);
 /* Copy the device accumulator (sum over samples, W*H*3 floats, row-major,
  * pixel i = y*W + x) to host memory. Returns the accumulated spp in *spp. */
-int			mrt_read_accum(mrt_ctx *ctx, float *rgb, int32_t *spp);
+MRT_API int			mrt_read_accum(mrt_ctx *ctx, float *rgb, int32_t *spp);
 /* Add the device accumulator into a caller-owned double buffer laid out
  * like t_fcolor[W*H] (the reference's screen.float_render) and clear it. */
-int			mrt_accumulate_double(mrt_ctx *ctx, double *float_render);
+MRT_API int			mrt_accumulate_double(mrt_ctx *ctx, double *float_render);
 /* BVH heat map (render_mode 1): per-pixel node-visit count of the last call. */
-int			mrt_read_depth(mrt_ctx *ctx, int32_t *depth);
+MRT_API int			mrt_read_depth(mrt_ctx *ctx, int32_t *depth);
 
 /* ------------------------------------------------------- parity probes */
 
@@ -291,25 +299,32 @@ typedef struct mrt_hit
 	int32_t	visits;         /* BVH nodes visited (heat-map counter) */
 }	mrt_hit;
 
-int			mrt_trace_first_hit(mrt_ctx *ctx, const mrt_ray *rays, int64_t n,
+MRT_API int			mrt_trace_first_hit(mrt_ctx *ctx, const mrt_ray *rays, int64_t n,
 				mrt_hit *hits);
 
 /* HDRI tables (importance_sampling_manager.c:41) as built on the device:
  * pdf_joint W*H f32, cdf_marginal_inverse H f32, cdf_conditional_inverse W*H f32.
  * Any pointer may be NULL. */
-int			mrt_read_env_tables(mrt_ctx *ctx, float *pdf_joint,
+MRT_API int			mrt_read_env_tables(mrt_ctx *ctx, float *pdf_joint,
 				float *cdf_marginal_inverse, float *cdf_conditional_inverse);
+
+/* Draw n HDRI importance samples on the device (seed, sampler as in
+ * mrt_render_params.env_sampler): outcome[i] is the sampled outcome of the
+ * reference's two-step lookup (row * W + column offset), out4 holds n float4
+ * (dir.x, dir.y, dir.z, pdf). */
+MRT_API int			mrt_env_sample(mrt_ctx *ctx, int64_t n, uint64_t seed, int32_t sampler,
+				int32_t *outcome, float *out4);
 
 /* Photon map (caustic_manager.c:83): number of stored photons, and their
  * positions / powers as float4 (x,y,z,_) pairs if the pointers are non-NULL. */
-int64_t		mrt_photon_count(mrt_ctx *ctx);
-int			mrt_read_photons(mrt_ctx *ctx, float *pos4, float *power4, int64_t cap);
+MRT_API int64_t		mrt_photon_count(mrt_ctx *ctx);
+MRT_API int			mrt_read_photons(mrt_ctx *ctx, float *pos4, float *power4, int64_t cap);
 /* Upload an explicit photon set (replacing the emitted one) and rebuild the grid. */
-int			mrt_set_photons(mrt_ctx *ctx, const double *pos3, const double *power3,
+MRT_API int			mrt_set_photons(mrt_ctx *ctx, const double *pos3, const double *power3,
 				int64_t n);
 /* Caustic radiance at query points (estimate_caustics_physically_based,
  * get_caustic.c:67), k nearest photons, as RGB doubles. */
-int			mrt_caustic_query(mrt_ctx *ctx, const double *points3, int64_t n,
+MRT_API int			mrt_caustic_query(mrt_ctx *ctx, const double *points3, int64_t n,
 				int32_t k, double *rgb_out);
 
 # ifdef __cplusplus

@@ -267,6 +267,7 @@ def rst_lib():
             "ro_pcg_float": (C.c_float, [C.POINTER(C.c_uint64)]),
             "ro_set_mesh_transform": (None, [C.c_int]),
             "ro_triangle_positions": (C.c_int, [_P, _P]),
+            "ro_counters_read": (C.c_int, [_P, _P]),
         }
         for k, (r, a) in sig.items():
             f = getattr(lib, k)
