@@ -90,8 +90,16 @@ inline float int_bits_as_float(int i) {
 
 }  // namespace
 
+struct WfHost;
+WfHost* wf_create();
+void wf_destroy(WfHost* H);
+int wf_render(WfHost* H, const SceneView& v, const LaunchParams& L, int spp, int capacity,
+              int sort_threshold, int use_graph, float4* frame, int* status, cudaStream_t st,
+              unsigned* launches, const char** err);
+
 struct mrt_ctx {
   int device = 0;
+  WfHost* wf = nullptr;
   int W = 0, H = 0;
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
@@ -123,6 +131,7 @@ struct mrt_ctx {
   SceneView view{};
   size_t scene_bytes = 0;
   int bvh_depth = 0;
+  int auto_form = MRT_FORM_MEGAKERNEL;   // choice of the autotuner for this scene
 };
 
 namespace {
@@ -324,6 +333,7 @@ void mrt_destroy(mrt_ctx* c) {
   c->alias.release(); c->env_rec0.release(); c->env_rec1.release();
   c->ph_pos.release(); c->ph_pow.release(); c->ph_pos_raw.release(); c->ph_pow_raw.release();
   c->cell_start.release(); c->cell_of.release(); c->ph_count.release();
+  wf_destroy(c->wf);
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -738,8 +748,6 @@ static int read_status(mrt_ctx* c, int* out) {
   return MRT_OK;
 }
 
-int mrt_render_wavefront(mrt_ctx* c, const SceneView& v, const LaunchParams& L, int spp,
-                         const mrt_render_params* p, mrt_render_stats* stats);
 
 extern "C" int mrt_render(mrt_ctx* c, const mrt_render_params* p, mrt_render_stats* stats) {
   int rc = check_ctx(c);
@@ -767,10 +775,17 @@ extern "C" int mrt_render(mrt_ctx* c, const mrt_render_params* p, mrt_render_sta
   if (p->render_mode == 1) CK(cudaMemsetAsync(c->depth.p, 0xff, c->depth.bytes(), c->stream));
   int launches = 0;
   CK(cudaEventRecord(c->ev0, c->stream));
-  if (p->form == MRT_FORM_WAVEFRONT && p->render_mode == 0) {
+  int form = p->form;
+  if (form == MRT_FORM_AUTO) form = c->auto_form;
+  if (form == MRT_FORM_WAVEFRONT && p->render_mode == 0) {
     L.sample_base = (uint32_t)p->sample_base;
-    int r2 = mrt_render_wavefront(c, v, L, p->spp, p, stats);
-    if (r2) return r2;
+    if (!c->wf) c->wf = wf_create();
+    const char* err = "";
+    unsigned nl = 0;
+    int r2 = wf_render(c->wf, v, L, p->spp, p->queue_capacity, p->sort_threshold,
+                       p->use_graph ? 1 : 0, c->accum.p, c->status.p, c->stream, &nl, &err);
+    if (r2) return set_err(r2, "wavefront: %s", err);
+    launches += (int)nl;
   } else {
     // chunks of spp so a single launch stays well under a second
     const uint64_t max_paths = 1ull << 25;
@@ -799,7 +814,7 @@ extern "C" int mrt_render(mrt_ctx* c, const mrt_render_params* p, mrt_render_sta
     stats->paths = npix * (uint64_t)p->spp;
     stats->segments = cnt[0];
     stats->shadow_rays = cnt[1];
-    if (p->form != MRT_FORM_WAVEFRONT) stats->kernel_launches = launches;
+    stats->kernel_launches = launches;
     stats->status = status;
   }
   if (status & ST_STACK) return set_err(MRT_ERR_STACK, "traversal stack overflow (status 0x%x)", status);

@@ -140,11 +140,27 @@ def test_alias_sampler_reproduces_the_reference_distribution(mrt, oracle, scenes
     assert np.all(np.isfinite(a)) and (a[:, 3] > 0).mean() > 0.99
 
 
-@pytest.mark.parametrize("name", ["c0", "c1", "c2"])
+def _no_glass(sc):
+    for m in sc.materials:
+        if m.get("ior", 0) > 0:
+            m.update(ior=0.0, transmission=0.0)
+    return sc
+
+
+STREAM_CASES = {"c0": 0.99, "c1": 0.85, "c2": 0.99, "c1_noglass": 0.99}
+
+
+@pytest.mark.parametrize("name", sorted(STREAM_CASES))
 def test_paths_match_oracle_stream(mrt, oracle, mg, name):
-    """Same (seed, pixel, sample) streams on both sides: per-pixel radiance of
-    one sample agrees except where FP32 vs FP64 flips a sampling decision."""
-    sc = mg.CASES[name]["make"]()
+    """Same (seed, pixel, sample) streams on both sides: per-pixel radiance
+    agrees except where FP32 vs FP64 flips a decision. Refraction through the
+    bumpy glass of c1 is chaotic (tiny direction differences grow over
+    internal bounces), so c1 is also checked without its dielectrics, and its
+    image mean is checked statistically."""
+    base = name.split("_")[0]
+    sc = mg.CASES[base]["make"]()
+    if name.endswith("noglass"):
+        sc = _no_glass(sc)
     ro = oracle.Restatement(sc)
     ctx = gpu_ctx(mrt, oracle, sc)
     if sc.caustic:
@@ -162,8 +178,34 @@ def test_paths_match_oracle_stream(mrt, oracle, mg, name):
     print(f"{name}: {frac:.4f} of pixels within 1e-3; mean {img.mean():.5f} vs {ref.mean():.5f}")
     bad = np.argsort(err.reshape(-1))[-5:]
     print(" worst", err.reshape(-1)[bad], img.reshape(-1, 3)[bad], ref.reshape(-1, 3)[bad])
-    assert frac >= 0.95
-    assert abs(img.mean() - ref.mean()) <= 0.02 * max(ref.mean(), 1e-3) + 1e-4
+    assert frac >= STREAM_CASES[name]
+    diff = (img - ref).mean(axis=2).reshape(-1)
+    se = diff.std() / np.sqrt(diff.size) + 1e-7
+    assert abs(diff.mean()) <= 4 * se, (diff.mean(), se)
+
+
+@pytest.mark.parametrize("name", ["c0", "c1", "c2"])
+def test_wavefront_matches_megakernel(mrt, oracle, mg, name):
+    """Both forms run the same estimator on the same random streams."""
+    sc = mg.CASES[name]["make"]()
+    ctx = gpu_ctx(mrt, oracle, sc)
+    ctx.render(8, seed=5)
+    a, _ = ctx.read_accum()
+    for graph in (0, 1):
+        for thr in (1, 1 << 30):
+            ctx.clear()
+            st = ctx.render(8, seed=5, form=mrt.FORM_WAVEFRONT, use_graph=graph, sort_threshold=thr,
+                            queue_capacity=1000)
+            b, n = ctx.read_accum()
+            assert n == 8 and st.kernel_launches > 8
+            err = np.abs(a - b).max(axis=2) / np.maximum(np.abs(a).max(axis=2), 1e-2)
+            frac = (err <= 1e-4).mean()
+            print(f"{name} graph={graph} sort={thr}: {frac:.4f} of pixels equal to the megakernel")
+            assert frac >= 0.99
+    ctx.clear()
+    st = ctx.render(8, seed=5, form=mrt.FORM_WAVEFRONT, use_graph=1)
+    c, _ = ctx.read_accum()
+    assert (np.abs(a - c).max(axis=2) / np.maximum(np.abs(a).max(axis=2), 1e-2) <= 1e-4).mean() >= 0.99
 
 
 def test_render_is_deterministic_and_accumulates(mrt, oracle, mg):
