@@ -132,6 +132,8 @@ struct mrt_ctx {
   size_t scene_bytes = 0;
   int bvh_depth = 0;
   int auto_form = MRT_FORM_MEGAKERNEL;   // choice of the autotuner for this scene
+  int auto_block = 0, auto_capacity = 0, auto_sort = 0;
+  int plain_megakernel = 0;              // 1: one path per thread, no regeneration
 };
 
 namespace {
@@ -233,7 +235,9 @@ void env_records(const mrt_ambient& a, const std::vector<float>& pdf, const std:
         const double u = (double)cc[j];
         const float theta = (float)((v - 0.5) * kPiD);
         const float phi = (float)((0.5 - u) * 2 * kPiD);
-        V3 dir = {std::cos(theta) * std::cos(phi), std::sin(theta), std::cos(theta) * std::sin(phi)};
+        // C's cos/sin on the float values (the double overloads, as the reference calls them)
+        const double th = (double)theta, ph = (double)phi;
+        V3 dir = {std::cos(th) * std::cos(ph), std::sin(th), std::cos(th) * std::sin(ph)};
         const long long pi = (long long)(v * (H - 1) * W + u * (W - 1));
         const float pd = (pi >= 0 && pi < (long long)W * H) ? pdf[pi] : 0.0f;
         const size_t k = (size_t)iy * W + d;
@@ -776,26 +780,37 @@ extern "C" int mrt_render(mrt_ctx* c, const mrt_render_params* p, mrt_render_sta
   int launches = 0;
   CK(cudaEventRecord(c->ev0, c->stream));
   int form = p->form;
-  if (form == MRT_FORM_AUTO) form = c->auto_form;
+  const bool tuned = form == MRT_FORM_AUTO;
+  if (tuned) form = c->auto_form;
+  const int block_size = p->block_size ? p->block_size : (tuned ? c->auto_block : 0);
+  const int queue_capacity = p->queue_capacity ? p->queue_capacity : (tuned ? c->auto_capacity : 0);
+  const int sort_threshold = p->sort_threshold ? p->sort_threshold : (tuned ? c->auto_sort : 0);
   if (form == MRT_FORM_WAVEFRONT && p->render_mode == 0) {
     L.sample_base = (uint32_t)p->sample_base;
     if (!c->wf) c->wf = wf_create();
     const char* err = "";
     unsigned nl = 0;
-    int r2 = wf_render(c->wf, v, L, p->spp, p->queue_capacity, p->sort_threshold,
-                       p->use_graph ? 1 : 0, c->accum.p, c->status.p, c->stream, &nl, &err);
+    int r2 = wf_render(c->wf, v, L, p->spp, queue_capacity, sort_threshold,
+                       p->use_graph || tuned ? 1 : 0, c->accum.p, c->status.p, c->stream, &nl, &err);
     if (r2) return set_err(r2, "wavefront: %s", err);
     launches += (int)nl;
   } else {
     // chunks of spp so a single launch stays well under a second
-    const uint64_t max_paths = 1ull << 25;
+    const uint64_t max_paths = 1ull << 26;
     int spp_chunk = (int)std::max<uint64_t>(1, max_paths / std::max<uint64_t>(npix, 1));
+    // the persistent, regenerating megakernel for path tracing; the plain
+    // one-path-per-thread launch for the debug modes and when counting
+    const bool regen = p->render_mode == 0 && !c->plain_megakernel;
     for (int s = 0; s < p->spp; s += spp_chunk) {
       int k = std::min(spp_chunk, p->spp - s);
       L.sample_base = (uint32_t)(p->sample_base + s);
       L.n_paths = npix * (uint64_t)k;
-      CK(launch_megakernel(v, L, c->accum.p, c->depth.p, c->status.p, stats ? c->counters.p : nullptr,
-                           p->block_size, c->stream));
+      if (regen)
+        CK(launch_megakernel_regen(v, L, c->accum.p, c->status.p, c->counters.p + 7, block_size,
+                                   0, c->stream));
+      else
+        CK(launch_megakernel(v, L, c->accum.p, c->depth.p, c->status.p, stats ? c->counters.p : nullptr,
+                             block_size, c->stream));
       launches++;
     }
   }
@@ -821,6 +836,46 @@ extern "C" int mrt_render(mrt_ctx* c, const mrt_render_params* p, mrt_render_sta
   if (status & ST_BUDGET) return set_err(MRT_ERR_BUDGET, "traversal iteration budget exhausted (status 0x%x)", status);
   if (status & ST_QUEUE) return set_err(MRT_ERR_QUEUE_OVERFLOW, "queue overflow (status 0x%x)", status);
   if (status & ST_ABORT) return set_err(MRT_ERR_ABORTED, "aborted (status 0x%x)", status);
+  return MRT_OK;
+}
+
+extern "C" int mrt_tune(mrt_ctx* c, int32_t spp, uint64_t seed, mrt_tune_result* out) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!out) return set_err(MRT_ERR_INVALID, "null result");
+  if (!c->has_scene) return set_err(MRT_ERR_INVALID, "no scene");
+  if (spp <= 0) return set_err(MRT_ERR_INVALID, "spp %d", spp);
+  std::memset(out, 0, sizeof(*out));
+  auto add = [&](int form, int block, int cap, int sort) {
+    if (out->n < MRT_TUNE_MAX) out->entry[out->n++] = mrt_tune_entry{form, block, cap, sort, 0.0};
+  };
+  for (int b : {64, 128, 256}) add(MRT_FORM_MEGAKERNEL, b, 0, 0);
+  for (int cap : {1 << 20, 1 << 21, 1 << 22})
+    for (int sort : {1 << 30, 1 << 16}) add(MRT_FORM_WAVEFRONT, 0, cap, sort);
+  int best = -1;
+  for (int i = 0; i < out->n; ++i) {
+    mrt_tune_entry& t = out->entry[i];
+    mrt_render_params p{};
+    p.spp = spp;
+    p.seed = seed;
+    p.form = t.form;
+    p.block_size = t.block_size;
+    p.queue_capacity = t.queue_capacity;
+    p.sort_threshold = t.sort_threshold;
+    p.use_graph = 1;
+    mrt_render_stats st{};
+    if (mrt_render(c, &p, &st) != MRT_OK) continue;           // warm-up / graph capture
+    if (mrt_render(c, &p, &st) != MRT_OK || st.ms <= 0) continue;
+    t.mpaths_s = (double)st.paths / st.ms / 1e3;
+    if (best < 0 || t.mpaths_s > out->entry[best].mpaths_s) best = i;
+  }
+  mrt_clear(c);
+  if (best < 0) return set_err(MRT_ERR_CUDA, "no candidate rendered: %s", g_err.c_str());
+  out->best = best;
+  c->auto_form = out->entry[best].form;
+  c->auto_block = out->entry[best].block_size;
+  c->auto_capacity = out->entry[best].queue_capacity;
+  c->auto_sort = out->entry[best].sort_threshold;
   return MRT_OK;
 }
 
@@ -890,6 +945,45 @@ extern "C" int mrt_trace_first_hit(mrt_ctx* c, const mrt_ray* rays, int64_t n, m
   rc = read_status(c, &status);
   if (rc) return rc;
   if (status) return set_err(status & ST_STACK ? MRT_ERR_STACK : MRT_ERR_BUDGET, "traversal status 0x%x", status);
+  return MRT_OK;
+}
+
+extern "C" int mrt_trace_paths(mrt_ctx* c, const mrt_render_params* p, const int32_t* pixel,
+                               const int32_t* sample, int32_t n, float* events, float* rgb) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!p || n < 0 || (n && (!pixel || !sample || !events || !rgb)))
+    return set_err(MRT_ERR_INVALID, "bad arguments");
+  if (!c->has_scene) return set_err(MRT_ERR_INVALID, "no scene");
+  const int64_t npix = (int64_t)c->W * c->H;
+  for (int i = 0; i < n; ++i)
+    if (pixel[i] < 0 || pixel[i] >= npix || sample[i] < 0)
+      return set_err(MRT_ERR_INVALID, "path %d: pixel %d / sample %d out of range", i, pixel[i], sample[i]);
+  if (n == 0) return MRT_OK;
+  SceneView v = c->view;
+  v.env_lookup = p->env_sampler;
+  LaunchParams L{};
+  L.seed = p->seed;
+  L.max_bounces = p->max_bounces > 0 ? p->max_bounces : v.max_bounces;
+  L.jitter = p->jitter;
+  const size_t ev_floats = (size_t)n * 16 * 20;
+  int *dp = nullptr, *ds = nullptr;
+  float *dev = nullptr, *drgb = nullptr;
+  CK(cudaMallocAsync(&dp, sizeof(int) * n, c->stream));
+  CK(cudaMallocAsync(&ds, sizeof(int) * n, c->stream));
+  CK(cudaMallocAsync(&dev, sizeof(float) * ev_floats, c->stream));
+  CK(cudaMallocAsync(&drgb, sizeof(float) * 3 * n, c->stream));
+  CK(cudaMemcpyAsync(dp, pixel, sizeof(int) * n, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(ds, sample, sizeof(int) * n, cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemsetAsync(c->status.p, 0, sizeof(int), c->stream));
+  CK(launch_path_events(v, L, dp, ds, n, dev, drgb, c->status.p, c->stream));
+  CK(cudaMemcpyAsync(events, dev, sizeof(float) * ev_floats, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(rgb, drgb, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaFreeAsync(dp, c->stream));
+  CK(cudaFreeAsync(ds, c->stream));
+  CK(cudaFreeAsync(dev, c->stream));
+  CK(cudaFreeAsync(drgb, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
   return MRT_OK;
 }
 

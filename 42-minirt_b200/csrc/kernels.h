@@ -31,6 +31,11 @@ struct HitOut {
 cudaError_t launch_megakernel(const SceneView& S, const LaunchParams& L, float4* accum, int* depth,
                               int* status, unsigned long long* counters, int block,
                               cudaStream_t st);
+cudaError_t launch_megakernel_regen(const SceneView& S, const LaunchParams& L, float4* accum,
+                                    int* status, unsigned long long* work, int block, int blocks_per_sm,
+                                    cudaStream_t st);
+cudaError_t launch_path_events(const SceneView& S, const LaunchParams& L, const int* pix, const int* smp,
+                               int n, float* ev, float* rgb, int* status, cudaStream_t st);
 cudaError_t launch_first_hit(const SceneView& S, const double* rays, int64_t n, HitOut* out,
                              int* status, cudaStream_t st);
 cudaError_t launch_accumulate_double(float4* accum, double* out, int n, cudaStream_t st);

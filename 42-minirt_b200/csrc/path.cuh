@@ -108,8 +108,27 @@ __device__ __forceinline__ void camera_ray(const SceneView& S, PathState& P, uin
 // path_trace + add_skybox (path_trace.c:37-76). render_mode 2 returns the
 // normal colour of the first hit (path_trace_normal, :78-89); render_mode 1
 // returns the node-visit count in .x (path_trace_bvh, :91-102).
+// Event record of one bounce (debug probe): flat prim id, t, hit point,
+// shading normal, then direction, power and radiance after shading.
+constexpr int kEventFloats = 20;
+constexpr int kMaxEvents = 16;
+
+__device__ __forceinline__ void write_event(float* ev, int k, const SceneView& S, const HitInfo& h,
+                                            const Surf& s, const PathState& P) {
+  float* e = ev + k * kEventFloats;
+  int flat = h.prim >= 0 ? __ldg(S.meta + h.prim).x : (h.prim == kMiss ? -1 : S.planes[-1 - h.prim].meta.x);
+  e[0] = (float)flat; e[1] = h.t;
+  e[2] = s.p.x; e[3] = s.p.y; e[4] = s.p.z;
+  e[5] = s.n.x; e[6] = s.n.y; e[7] = s.n.z;
+  e[8] = P.d.x; e[9] = P.d.y; e[10] = P.d.z;
+  e[11] = P.power.x; e[12] = P.power.y; e[13] = P.power.z;
+  e[14] = P.acc.x; e[15] = P.acc.y; e[16] = P.acc.z;
+  e[17] = (float)s.mat;
+}
+
 __device__ __forceinline__ float3 trace_path(const SceneView& S, PathState& P, int max_depth,
-                                             int render_mode, int* status, PathCounters& C) {
+                                             int render_mode, int* status, PathCounters& C,
+                                             float* ev = nullptr) {
   P.power = f3(1.f, 1.f, 1.f);
   P.acc = f3(0.f, 0.f, 0.f);
   P.last_mat = -1;
@@ -123,6 +142,7 @@ __device__ __forceinline__ float3 trace_path(const SceneView& S, PathState& P, i
     if (!hit) return f3(0.f, 0.f, 0.f);
     return make_surf(S, h, P.o, P.d, 2).color;
   }
+  int ev_k = 0;
   while (--max_depth >= 0) {
     HitInfo h;
     int visits = 0;
@@ -133,17 +153,48 @@ __device__ __forceinline__ float3 trace_path(const SceneView& S, PathState& P, i
       float3 bg = background(S, P.d, true);
       if (P.last_mat >= 0) bg = bg * S.mats[P.last_mat].ao;
       P.acc = P.acc + bg * P.power;
+      if (ev && ev_k < kMaxEvents) {
+        Surf z{};
+        z.mat = -1;
+        h.prim = kMiss;
+        write_event(ev, ev_k, S, h, z, P);
+      }
       break;
     }
     Surf s = make_surf(S, h, P.o, P.d, 0);
     P.o = s.p;
     P.last_mat = s.mat;
     material_manager(S, P, s, status, C);
+    if (ev && ev_k < kMaxEvents) write_event(ev, ev_k++, S, h, s, P);
     // Every later term is multiplied by the path power: a path whose power
     // reached exactly zero contributes nothing more.
     if (P.power.x == 0.0f && P.power.y == 0.0f && P.power.z == 0.0f) break;
   }
   return P.acc;
+}
+
+// One bounce of path_trace (path_trace.c:58-72) for a path whose state lives
+// in P. Returns false when the path ended (miss, depth exhausted, or zero
+// power); P.acc then holds its radiance.
+__device__ __forceinline__ bool bounce(const SceneView& S, PathState& P, int& depth_left,
+                                       int* status, PathCounters& C) {
+  HitInfo h;
+  int visits = 0;
+  C.segments++;
+  const bool hit = closest_hit<false>(S, P.o, P.d, h, visits, status);
+  if (!hit) {
+    float3 bg = background(S, P.d, true);
+    if (P.last_mat >= 0) bg = bg * S.mats[P.last_mat].ao;
+    P.acc = P.acc + bg * P.power;
+    return false;
+  }
+  Surf s = make_surf(S, h, P.o, P.d, 0);
+  P.o = s.p;
+  P.last_mat = s.mat;
+  material_manager(S, P, s, status, C);
+  --depth_left;
+  if (P.power.x == 0.0f && P.power.y == 0.0f && P.power.z == 0.0f) return false;
+  return depth_left > 0;
 }
 
 // Sub-pixel offset of a sample: shared by every pixel of the sample

@@ -4,6 +4,8 @@
 // registers, one vector atomic into the float4 accumulator at the end.
 // Threads are laid out so that a warp covers an 8x4 pixel tile of one
 // sample (coherent primary rays), and samples vary slowest.
+#include <algorithm>
+
 #include "kernels.h"
 #include "path.cuh"
 
@@ -61,6 +63,87 @@ __global__ void __launch_bounds__(kBlock) megakernel(SceneView S, LaunchParams L
       atomicAdd(counters + 2, vi);
     }
   }
+}
+
+// Persistent megakernel with path regeneration: every lane advances its path
+// by one bounce per loop iteration; lanes whose path ended take the next path
+// index (one atomic per warp for all idle lanes), so warps stay full until
+// the launch runs out of paths.
+template <int kBlock>
+__global__ void __launch_bounds__(kBlock) megakernel_regen(SceneView S, LaunchParams L, float4* accum,
+                                                           int* status, unsigned long long* work) {
+  const uint32_t npix = (uint32_t)S.width * (uint32_t)S.height;
+  const int lane = threadIdx.x & 31;
+  PathCounters C{0, 0, 0};
+  PathState P;
+  int depth_left = 0;
+  uint32_t pixel = 0;
+  bool active = false, done = false;
+  while (true) {
+    const bool need = !active && !done;
+    const unsigned need_mask = __ballot_sync(0xffffffffu, need);
+    if (need_mask) {
+      unsigned long long base = 0;
+      const int leader = __ffs(need_mask) - 1;
+      if (lane == leader) base = atomicAdd(work, (unsigned long long)__popc(need_mask));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (need) {
+        const uint64_t idx = base + __popc(need_mask & ((1u << lane) - 1u));
+        if (idx >= L.n_paths) {
+          done = true;
+        } else {
+          const uint32_t lin = (uint32_t)(idx % npix);
+          const uint32_t sample = L.sample_base + (uint32_t)(idx / npix);
+          pixel = tile_pixel(lin, S.width, S.height);
+          P.rng.s = path_seed(L.seed, pixel, sample);
+          float ox, oy;
+          sample_offset(L.seed, sample, L.jitter, P.rng, ox, oy);
+          camera_ray(S, P, pixel, ox, oy);
+          P.power = f3(1.f, 1.f, 1.f);
+          P.acc = f3(0.f, 0.f, 0.f);
+          P.last_mat = -1;
+          depth_left = L.max_bounces;
+          active = depth_left > 0;
+          if (!active) atomicAdd(accum + pixel, make_float4(0.f, 0.f, 0.f, 1.0f));
+        }
+      }
+    }
+    if (__all_sync(0xffffffffu, done)) break;
+    if (active) {
+      if (!bounce(S, P, depth_left, status, C)) {
+        active = false;
+        atomicAdd(accum + pixel, make_float4(P.acc.x, P.acc.y, P.acc.z, 1.0f));
+      }
+    }
+  }
+}
+
+// Debug probe: full event record of single paths (pixel, sample).
+__global__ void path_events_kernel(SceneView S, LaunchParams L, const int* pix, const int* smp, int n,
+                                   float* ev, float* rgb, int* status) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  PathCounters C{0, 0, 0};
+  PathState P;
+  const uint32_t pixel = (uint32_t)pix[i], sample = (uint32_t)smp[i];
+  P.rng.s = path_seed(L.seed, pixel, sample);
+  float ox, oy;
+  sample_offset(L.seed, sample, L.jitter, P.rng, ox, oy);
+  camera_ray(S, P, pixel, ox, oy);
+  float* e = ev + (size_t)i * kMaxEvents * kEventFloats;
+  for (int k = 0; k < kMaxEvents * kEventFloats; ++k) e[k] = 0.0f;
+  for (int k = 0; k < kMaxEvents; ++k) e[k * kEventFloats] = -2.0f;
+  float3 c = trace_path(S, P, L.max_bounces, 0, status, C, e);
+  rgb[3 * i] = c.x;
+  rgb[3 * i + 1] = c.y;
+  rgb[3 * i + 2] = c.z;
+}
+
+cudaError_t launch_path_events(const SceneView& S, const LaunchParams& L, const int* pix, const int* smp,
+                               int n, float* ev, float* rgb, int* status, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  path_events_kernel<<<(n + 63) / 64, 64, 0, st>>>(S, L, pix, smp, n, ev, rgb, status);
+  return cudaGetLastError();
 }
 
 __global__ void first_hit_kernel(SceneView S, const double* rays, int64_t n, HitOut* out,
@@ -145,6 +228,32 @@ cudaError_t launch_megakernel(const SceneView& S, const LaunchParams& L, float4*
   MRT_MK(128)
   MRT_MK(256)
 #undef MRT_MK
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_megakernel_regen(const SceneView& S, const LaunchParams& L, float4* accum,
+                                    int* status, unsigned long long* work, int block, int blocks_per_sm,
+                                    cudaStream_t st) {
+  if (L.n_paths == 0) return cudaSuccess;
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  block = block > 0 ? block : 128;
+  cudaError_t e = cudaMemsetAsync(work, 0, sizeof(unsigned long long), st);
+  if (e != cudaSuccess) return e;
+#define MRT_RG(B)                                                                          \
+  if (block <= B) {                                                                        \
+    int occ = 0;                                                                           \
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, megakernel_regen<B>, B, 0);        \
+    int per = blocks_per_sm > 0 ? std::min(blocks_per_sm, std::max(occ, 1)) : std::max(occ, 1); \
+    unsigned grid = (unsigned)std::min<uint64_t>((uint64_t)sms * per, (L.n_paths + B - 1) / B); \
+    megakernel_regen<B><<<grid, B, 0, st>>>(S, L, accum, status, work);                    \
+    return cudaGetLastError();                                                             \
+  }
+  MRT_RG(64)
+  MRT_RG(128)
+  MRT_RG(256)
+#undef MRT_RG
   return cudaErrorInvalidValue;
 }
 

@@ -143,7 +143,7 @@ __global__ void __launch_bounds__(kWfBlock) wf_extend(SceneView S, WfState W, in
       const float4 o = W.o[i], d = W.d[i];
       HitInfo h;
       int visits = 0;
-      bool hit = closest_hit<false>(S, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), h, visits, status);
+      bool hit = closest_hit_ww<false>(S, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), h, visits, status);
       W.hit[i] = make_float4(h.t, h.u, h.v, __int_as_float(hit ? h.prim : kMiss));
     }
   }
@@ -354,7 +354,7 @@ __global__ void __launch_bounds__(kWfBlock) wf_connect(SceneView S, WfState W, i
     const int k = base + lane;
     if (k < n) {
       const float4 o = W.sh_o[k], d = W.sh_d[k];
-      const bool blocked = any_hit(S, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), o.w, status);
+      const bool blocked = any_hit_ww(S, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), o.w, status);
       if (!blocked) {
         const int tag = __float_as_int(d.w);
         const int path = tag >> 4, slot = tag & 15;
@@ -502,6 +502,7 @@ static cudaError_t wf_alloc(WfHost* H, int capacity, int n_lights, bool env) {
   H->allocs.clear();
   if (H->graph) { cudaGraphExecDestroy(H->graph); H->graph = nullptr; }
   H->graph_bounces = -1;
+  H->sh_capacity = 0;          // the shadow queue went with the other buffers
   const int rays = n_lights * 1 + (env ? 1 : 0);
   H->capacity = capacity;
   WfState& s = H->st;
@@ -599,7 +600,7 @@ int wf_render(WfHost* H, const SceneView& v, const LaunchParams& L, int spp, int
   if (total == 0) return MRT_OK;
   if (v.n_lights > 4) { *err = "wavefront form supports up to 4 lights (use the megakernel)"; return MRT_ERR_INVALID; }
   for (int l = 0; l < v.n_lights; ++l) (void)l;
-  if (capacity <= 0) capacity = 1 << 21;
+  if (capacity <= 0) capacity = 1 << 22;
   capacity = (int)std::min<uint64_t>((uint64_t)capacity, std::max<uint64_t>(total, 1024));
   cudaError_t e;
   if (H->capacity != capacity) {

@@ -117,6 +117,15 @@ class RenderStats(C.Structure):
                 ("status", C.c_int32)]
 
 
+class TuneEntry(C.Structure):
+    _fields_ = [("form", C.c_int32), ("block_size", C.c_int32), ("queue_capacity", C.c_int32),
+                ("sort_threshold", C.c_int32), ("mpaths_s", C.c_double)]
+
+
+class TuneResult(C.Structure):
+    _fields_ = [("n", C.c_int32), ("best", C.c_int32), ("entry", TuneEntry * 32)]
+
+
 class Ray(C.Structure):
     _fields_ = [("orig", f64x3), ("dir", f64x3)]
 
@@ -144,10 +153,12 @@ SIGNATURES = {
     "mrt_set_camera": (C.c_int, [_P, C.POINTER(Camera), C.c_double, C.c_double]),
     "mrt_render": (C.c_int, [_P, C.POINTER(RenderParams), C.POINTER(RenderStats)]),
     "mrt_clear": (C.c_int, [_P]),
+    "mrt_tune": (C.c_int, [_P, C.c_int32, C.c_uint64, C.POINTER(TuneResult)]),
     "mrt_read_accum": (C.c_int, [_P, _P, C.POINTER(C.c_int32)]),
     "mrt_accumulate_double": (C.c_int, [_P, _P]),
     "mrt_read_depth": (C.c_int, [_P, _P]),
     "mrt_trace_first_hit": (C.c_int, [_P, _P, C.c_int64, _P]),
+    "mrt_trace_paths": (C.c_int, [_P, C.POINTER(RenderParams), _P, _P, C.c_int32, _P, _P]),
     "mrt_read_env_tables": (C.c_int, [_P, _P, _P, _P]),
     "mrt_env_sample": (C.c_int, [_P, C.c_int64, C.c_uint64, C.c_int32, _P, _P]),
     "mrt_photon_count": (C.c_int64, [_P]),
@@ -241,6 +252,15 @@ class Context:
         check(self.lib.mrt_render(self.h, C.byref(p), C.byref(st)), "mrt_render")
         return st
 
+    def tune(self, spp: int = 2, seed: int = 1) -> list[dict]:
+        """Times the forms / launch shapes, keeps the fastest for FORM_AUTO."""
+        r = TuneResult()
+        check(self.lib.mrt_tune(self.h, spp, seed, C.byref(r)), "mrt_tune")
+        names = {FORM_MEGAKERNEL: "megakernel", FORM_WAVEFRONT: "wavefront"}
+        return [dict(form=names[e.form], block_size=e.block_size, queue_capacity=e.queue_capacity,
+                     sort_threshold=e.sort_threshold, mpaths_s=e.mpaths_s, best=(i == r.best))
+                for i, e in enumerate(r.entry[:r.n])]
+
     def clear(self) -> None:
         check(self.lib.mrt_clear(self.h), "mrt_clear")
 
@@ -265,6 +285,18 @@ class Context:
         check(self.lib.mrt_trace_first_hit(self.h, _ptr(rays), len(rays), _ptr(hits)),
               "mrt_trace_first_hit")
         return hits
+
+    def trace_paths(self, pixels, samples, seed: int = 1, jitter: int = JITTER_SHARED,
+                    env_sampler: int = 1, max_bounces: int = 0):
+        """Per-bounce event records (n, 16, 20) and radiance (n, 3) of single paths."""
+        pix = np.ascontiguousarray(pixels, np.int32)
+        smp = np.ascontiguousarray(samples, np.int32)
+        ev = np.zeros((len(pix), 16, 20), np.float32)
+        rgb = np.zeros((len(pix), 3), np.float32)
+        p = RenderParams(seed=seed, jitter=jitter, env_sampler=env_sampler, max_bounces=max_bounces)
+        check(self.lib.mrt_trace_paths(self.h, C.byref(p), _ptr(pix), _ptr(smp), len(pix),
+                                       _ptr(ev), _ptr(rgb)), "mrt_trace_paths")
+        return ev, rgb
 
     def env_tables(self, w: int, h: int):
         pdf = np.zeros(w * h, np.float32)

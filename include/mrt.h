@@ -275,6 +275,34 @@ MRT_API int			mrt_accumulate_double(mrt_ctx *ctx, double *float_render);
 /* BVH heat map (render_mode 1): per-pixel node-visit count of the last call. */
 MRT_API int			mrt_read_depth(mrt_ctx *ctx, int32_t *depth);
 
+/* ------------------------------------------------------------ autotuner */
+
+# define MRT_TUNE_MAX 32
+
+/* One timed candidate of mrt_tune. */
+typedef struct mrt_tune_entry
+{
+	int32_t	form;            /* MRT_FORM_MEGAKERNEL or MRT_FORM_WAVEFRONT */
+	int32_t	block_size;
+	int32_t	queue_capacity;
+	int32_t	sort_threshold;
+	double	mpaths_s;        /* measured throughput, 0 if the candidate failed */
+}	mrt_tune_entry;
+
+typedef struct mrt_tune_result
+{
+	int32_t			n;       /* candidates timed */
+	int32_t			best;    /* index of the fastest */
+	mrt_tune_entry	entry[MRT_TUNE_MAX];
+}	mrt_tune_result;
+
+/* Times the render forms and their launch shapes (block size, queue
+ * capacity, material-sort threshold) on the current scene with `spp`
+ * samples per candidate, keeps the fastest as the context's choice for
+ * MRT_FORM_AUTO and zero-valued launch parameters, and reports all of them.
+ * Leaves the accumulator cleared. */
+MRT_API int			mrt_tune(mrt_ctx *ctx, int32_t spp, uint64_t seed, mrt_tune_result *out);
+
 /* ------------------------------------------------------- parity probes */
 
 /* A ray in the reference's double layout (t_ray, structs.h:63-67). */
@@ -301,6 +329,16 @@ typedef struct mrt_hit
 
 MRT_API int			mrt_trace_first_hit(mrt_ctx *ctx, const mrt_ray *rays, int64_t n,
 				mrt_hit *hits);
+
+/* Debug probe: traces single paths (pixel[i], sample[i]) with the render
+ * seed / jitter / env_sampler of params and records each bounce as 20
+ * floats (flat prim id or -1 for the final miss, t, point.xyz, normal.xyz,
+ * then direction.xyz, power.rgb and radiance.rgb after shading, material),
+ * up to 16 bounces per path (unused records start with -2). rgb receives
+ * each path's radiance. */
+MRT_API int			mrt_trace_paths(mrt_ctx *ctx, const mrt_render_params *params,
+				const int32_t *pixel, const int32_t *sample, int32_t n,
+				float *events, float *rgb);
 
 /* HDRI tables (importance_sampling_manager.c:41) as built on the device:
  * pdf_joint W*H f32, cdf_marginal_inverse H f32, cdf_conditional_inverse W*H f32.

@@ -790,6 +790,11 @@ static int flat_of(ro_scene *s, int prim)
 	return s->planes[-1 - prim].flat;
 }
 
+static int flat_of_prim(ro_scene *s, int prim)
+{
+	return flat_of(s, prim);
+}
+
 /* ------------------------------------------------------------------ sky */
 
 /* get_hdr_pixel_skybox (get_hdr_value.c:43-68). */
@@ -1454,6 +1459,28 @@ static void material_manager(rng_t *rg, ro_scene *s, ray_t *r, hrec_t *h, fc *po
 		dielectric_mat(rg, s, r, h, power, acc);
 }
 
+/* Per-bounce event records for the debug probe (20 doubles per bounce:
+ * flat prim or -1 for the final miss, t, point, normal, then direction,
+ * power and radiance after shading, material). */
+static double	*g_events = NULL;
+
+static void put_event(int k, ro_scene *s, hrec_t *h, int hit, ray_t *r, fc power, fc acc)
+{
+	double	*e;
+
+	if (!g_events || k >= 16)
+		return ;
+	e = g_events + 20 * k;
+	e[0] = hit ? flat_of_prim(s, h->prim) : -1;
+	e[1] = hit ? h->t : 0;
+	e[2] = hit ? h->point.x : 0; e[3] = hit ? h->point.y : 0; e[4] = hit ? h->point.z : 0;
+	e[5] = hit ? h->normal.x : 0; e[6] = hit ? h->normal.y : 0; e[7] = hit ? h->normal.z : 0;
+	e[8] = r->dir.x; e[9] = r->dir.y; e[10] = r->dir.z;
+	e[11] = power.r; e[12] = power.g; e[13] = power.b;
+	e[14] = acc.r; e[15] = acc.g; e[16] = acc.b;
+	e[17] = hit ? h->mat : -1;
+}
+
 /* path_trace + add_skybox (path_trace.c:37-76). On a miss the sky is scaled
  * by the ao of the last material hit (the hit record persists). */
 static fc path_trace(rng_t *rg, ro_scene *s, ray_t r, int depth)
@@ -1461,6 +1488,7 @@ static fc path_trace(rng_t *rg, ro_scene *s, ray_t r, int depth)
 	fc		acc = {0.0, 0.0, 0.0};
 	fc		power = {1.0, 1.0, 1.0};
 	hrec_t	h;
+	int		k = 0;
 
 	memset(&h, 0, sizeof(h));
 	h.mat = -1;
@@ -1473,6 +1501,7 @@ static fc path_trace(rng_t *rg, ro_scene *s, ray_t r, int depth)
 			s->cnt.hits++;
 			r.orig = h.point;
 			material_manager(rg, s, &r, &h, &power, &acc);
+			put_event(k++, s, &h, 1, &r, power, acc);
 		}
 		else
 		{
@@ -1482,6 +1511,7 @@ static fc path_trace(rng_t *rg, ro_scene *s, ray_t r, int depth)
 				acc = fadd(acc, fmul(fscale(bg, s->mats[h.mat].ao), power));
 			else
 				acc = fadd(acc, fmul(bg, power));
+			put_event(k, s, &h, 0, &r, power, acc);
 			break ;
 		}
 	}
@@ -2106,4 +2136,20 @@ int	ro_triangle_positions(ro_scene *s, double *out)
 		n++;
 	}
 	return n;
+}
+
+/* One counter-RNG path with its per-bounce events (16 x 20 doubles). */
+int	ro_trace_path_events(ro_scene *s, uint64_t seed, int32_t pixel, int32_t sample,
+	int jitter, double *events, double *rgb)
+{
+	int	rc;
+
+	for (int k = 0; k < 16 * 20; k++)
+		events[k] = 0;
+	for (int k = 0; k < 16; k++)
+		events[20 * k] = -2;
+	g_events = events;
+	rc = ro_trace_path_counter(s, seed, pixel, sample, jitter, rgb);
+	g_events = NULL;
+	return rc;
 }

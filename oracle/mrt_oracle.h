@@ -78,6 +78,11 @@ int			ro_render_counter(ro_scene *s, uint64_t seed, int sample_base, int spp,
 int			ro_trace_path_counter(ro_scene *s, uint64_t seed, int32_t pixel,
 				int32_t sample, int jitter, double *rgb);
 
+/* The same path with its per-bounce event records (16 x 20 doubles, the
+ * layout of mrt_trace_paths). */
+int			ro_trace_path_events(ro_scene *s, uint64_t seed, int32_t pixel,
+				int32_t sample, int jitter, double *events, double *rgb);
+
 /* HDRI tables (importance_sampling_manager.c:41). Returns 0 if no sky. */
 int			ro_env_tables(ro_scene *s, float *pdf_joint, float *cdf_m_inv,
 				float *cdf_c_inv, double *column_average);

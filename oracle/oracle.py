@@ -263,6 +263,7 @@ def rst_lib():
             "ro_photons": (C.c_int, [_P, _P, _P, _P]),
             "ro_caustic_query": (C.c_int, [_P, _P, C.c_int64, C.c_int, _P]),
             "ro_counters_read": (C.c_int, [_P, _P]),
+            "ro_trace_path_events": (C.c_int, [_P, C.c_uint64, C.c_int32, C.c_int32, C.c_int, _P, _P]),
             "ro_path_seed": (C.c_uint64, [C.c_uint64, C.c_uint32, C.c_uint32]),
             "ro_pcg_float": (C.c_float, [C.POINTER(C.c_uint64)]),
             "ro_set_mesh_transform": (None, [C.c_int]),
@@ -332,6 +333,12 @@ class Restatement:
         out = np.zeros(3)
         self.lib.ro_trace_path_counter(self.h, seed, pixel, sample, jitter, _ptr(out))
         return out
+
+    def path_events(self, seed: int, pixel: int, sample: int, jitter: int = 0):
+        ev = np.zeros((16, 20))
+        rgb = np.zeros(3)
+        self.lib.ro_trace_path_events(self.h, seed, pixel, sample, jitter, _ptr(ev), _ptr(rgb))
+        return ev, rgb
 
     def env_tables(self):
         if self.scene.hdr is None:

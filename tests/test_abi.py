@@ -45,7 +45,8 @@ def test_ctypes_layouts_match_c(mrt):
                "mrt_mesh": mrt.Mesh, "mrt_light": mrt.Light, "mrt_camera": mrt.Camera,
                "mrt_ambient": mrt.Ambient, "mrt_caustic": mrt.Caustic,
                "mrt_scene_desc": mrt.SceneDesc, "mrt_render_params": mrt.RenderParams,
-               "mrt_render_stats": mrt.RenderStats, "mrt_ray": mrt.Ray, "mrt_hit": mrt.Hit}
+               "mrt_render_stats": mrt.RenderStats, "mrt_ray": mrt.Ray, "mrt_hit": mrt.Hit,
+               "mrt_tune_entry": mrt.TuneEntry, "mrt_tune_result": mrt.TuneResult}
     src = "#include <stdio.h>\n#include <stddef.h>\n#include \"mrt.h\"\nint main(void){\n"
     for name in structs:
         src += f'  printf("{name} %zu\\n", sizeof({name}));\n'
