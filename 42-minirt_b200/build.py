@@ -51,22 +51,37 @@ def build_libmrt(verbose_ptxas: bool = False) -> Path:
     return out
 
 
-def build_minirt_adapter() -> Path | None:
-    """libmrt_minirt.so: the reference-named entry points (init_shader,
-    convert_scene_build, compute_frame_gpu, calc_one_sample, ...) compiled
-    against miniRT's own headers (overlaid with include/minirt_compat)."""
-    overlay = HERE.parent / "oracle" / "_ref" / "overlay"
-    if not overlay.exists():
-        return None
+def minirt_overlay(minirt_includes: Path) -> Path:
+    """Header overlay for compiling against miniRT: links to miniRT's own
+    includes/*.h, except its GL bridge headers (gpu.h, gpu_struct.h,
+    gpu_scene.h), which resolve to include/minirt_compat."""
+    ov = HERE / "_build" / "minirt_overlay"
+    ov.mkdir(parents=True, exist_ok=True)
+    compat = INCLUDE / "minirt_compat"
+    for h in sorted(minirt_includes.glob("*.h")):
+        target = compat / h.name if (compat / h.name).exists() else h
+        link = ov / h.name
+        if link.is_symlink() or link.exists():
+            link.unlink()
+        link.symlink_to(target)
+    return ov
+
+
+def build_minirt_adapter(minirt_includes: Path = Path("/root/reference/includes")) -> Path | None:
+    """libmrt_minirt.so: miniRT's GPU entry points (init_shader,
+    convert_scene_build, convert_scene, compute_frame_gpu, calc_one_sample,
+    clean_*) compiled against miniRT's own headers. Needs the miniRT
+    includes directory; without it the prebuilt library is kept."""
     out = HERE / "libmrt_minirt.so"
     src = HERE / "minirt" / "minirt_gpu.c"
-    if not src.exists():
-        return None
+    if not minirt_includes.exists():
+        return out if out.exists() else None
     if out.exists() and out.stat().st_mtime >= max(src.stat().st_mtime,
                                                      (HERE / "libmrt.so").stat().st_mtime):
         return out
-    _run(["gcc", "-O2", "-fPIC", "-shared", "-std=gnu99", "-w", "-I", str(overlay),
-          "-I", str(HERE.parent / "oracle" / "shim"), "-I", str(INCLUDE), str(src),
+    ov = minirt_overlay(minirt_includes)
+    _run(["gcc", "-O2", "-fPIC", "-shared", "-std=gnu99", "-w", "-I", str(ov),
+          "-I", str(HERE / "minirt" / "headless"), "-I", str(INCLUDE), str(src),
           "-o", str(out), "-L", str(HERE), "-lmrt", "-Wl,-rpath,$ORIGIN"])
     return out
 

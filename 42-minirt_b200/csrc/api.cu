@@ -839,6 +839,86 @@ extern "C" int mrt_render(mrt_ctx* c, const mrt_render_params* p, mrt_render_sta
   return MRT_OK;
 }
 
+extern "C" int mrt_render_batch(mrt_ctx** ctxs, const mrt_render_params* params, int32_t n,
+                                mrt_render_stats* stats) {
+  if (!ctxs || !params || n <= 0) return set_err(MRT_ERR_INVALID, "empty batch");
+  for (int i = 0; i < n; ++i) {
+    if (!ctxs[i]) return set_err(MRT_ERR_INVALID, "batch entry %d: null context", i);
+    if (!ctxs[i]->has_scene) return set_err(MRT_ERR_INVALID, "batch entry %d: no scene", i);
+    if (ctxs[i]->device != ctxs[0]->device)
+      return set_err(MRT_ERR_INVALID, "batch entry %d is on device %d, not %d", i, ctxs[i]->device,
+                     ctxs[0]->device);
+    if (params[i].spp < 0 || params[i].sample_base < 0 || params[i].offset || params[i].render_mode != 0)
+      return set_err(MRT_ERR_INVALID, "batch entry %d: spp / sample_base / offset / render_mode", i);
+  }
+  mrt_ctx* c0 = ctxs[0];
+  int rc = check_ctx(c0);
+  if (rc) return rc;
+  if (params[0].block_size && (params[0].block_size % 32 || params[0].block_size > 256))
+    return set_err(MRT_ERR_INVALID, "block_size %d", params[0].block_size);
+  // longest-first order by predicted cost
+  std::vector<int> order(n);
+  std::vector<double> cost(n);
+  for (int i = 0; i < n; ++i) {
+    order[i] = i;
+    const double paths = (double)ctxs[i]->W * ctxs[i]->H * params[i].spp;
+    const int depth = params[i].max_bounces > 0 ? params[i].max_bounces : ctxs[i]->view.max_bounces;
+    cost[i] = paths * depth * std::log2(2.0 + ctxs[i]->view.n_prims);
+  }
+  std::sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+  std::vector<SceneView> views(n);
+  std::vector<BatchItem> items(n);
+  uint64_t total = 0;
+  for (int k = 0; k < n; ++k) {
+    const int i = order[k];
+    views[k] = ctxs[i]->view;
+    views[k].env_lookup = params[i].env_sampler;
+    BatchItem& it = items[k];
+    it.start = total;
+    it.paths = (uint64_t)ctxs[i]->W * ctxs[i]->H * (uint64_t)params[i].spp;
+    it.seed = params[i].seed;
+    it.sample_base = (uint32_t)params[i].sample_base;
+    it.view = k;
+    it.max_bounces = params[i].max_bounces > 0 ? params[i].max_bounces : ctxs[i]->view.max_bounces;
+    it.jitter = params[i].jitter;
+    it.accum = ctxs[i]->accum.p;
+    total += it.paths;
+  }
+  SceneView* dv = nullptr;
+  BatchItem* di = nullptr;
+  cudaStream_t st = c0->stream;
+  CK(cudaMallocAsync(&dv, sizeof(SceneView) * n, st));
+  CK(cudaMallocAsync(&di, sizeof(BatchItem) * n, st));
+  CK(cudaMemcpyAsync(dv, views.data(), sizeof(SceneView) * n, cudaMemcpyHostToDevice, st));
+  CK(cudaMemcpyAsync(di, items.data(), sizeof(BatchItem) * n, cudaMemcpyHostToDevice, st));
+  CK(cudaMemsetAsync(c0->status.p, 0, sizeof(int), st));
+  // other contexts' streams may still be writing their accumulators
+  for (int i = 0; i < n; ++i)
+    if (ctxs[i]->stream != st) CK(cudaStreamSynchronize(ctxs[i]->stream));
+  CK(cudaEventRecord(c0->ev0, st));
+  CK(launch_megakernel_batch(dv, di, n, total, c0->status.p, c0->counters.p + 7, params[0].block_size, st));
+  CK(cudaEventRecord(c0->ev1, st));
+  CK(cudaFreeAsync(dv, st));
+  CK(cudaFreeAsync(di, st));
+  CK(cudaEventSynchronize(c0->ev1));
+  int status = 0;
+  rc = read_status(c0, &status);
+  if (rc) return rc;
+  for (int i = 0; i < n; ++i) ctxs[i]->accum_spp += params[i].spp;
+  if (stats) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c0->ev0, c0->ev1);
+    std::memset(stats, 0, sizeof(*stats));
+    stats->ms = ms;
+    stats->paths = total;
+    stats->kernel_launches = 1;
+    stats->status = status;
+  }
+  if (status & ST_STACK) return set_err(MRT_ERR_STACK, "traversal stack overflow (status 0x%x)", status);
+  if (status & ST_BUDGET) return set_err(MRT_ERR_BUDGET, "traversal budget exhausted (status 0x%x)", status);
+  return MRT_OK;
+}
+
 extern "C" int mrt_tune(mrt_ctx* c, int32_t spp, uint64_t seed, mrt_tune_result* out) {
   int rc = check_ctx(c);
   if (rc) return rc;

@@ -18,6 +18,18 @@ struct LaunchParams {
   float ox, oy;
 };
 
+// One scene of a multi-scene batch launch.
+struct BatchItem {
+  uint64_t start;          // first global path index of this scene
+  uint64_t paths;
+  uint64_t seed;
+  uint32_t sample_base;
+  int view;                // index into the device SceneView array
+  int max_bounces;
+  int jitter;
+  float4* accum;           // the scene's accumulator
+};
+
 // Matches mrt_hit (include/mrt.h) field for field.
 struct HitOut {
   int prim;
@@ -33,6 +45,9 @@ cudaError_t launch_megakernel(const SceneView& S, const LaunchParams& L, float4*
                               cudaStream_t st);
 cudaError_t launch_megakernel_regen(const SceneView& S, const LaunchParams& L, float4* accum,
                                     int* status, unsigned long long* work, int block, int blocks_per_sm,
+                                    cudaStream_t st);
+cudaError_t launch_megakernel_batch(const SceneView* views, const BatchItem* items, int n_items,
+                                    uint64_t total, int* status, unsigned long long* work, int block,
                                     cudaStream_t st);
 cudaError_t launch_path_events(const SceneView& S, const LaunchParams& L, const int* pix, const int* smp,
                                int n, float* ev, float* rgb, int* status, cudaStream_t st);

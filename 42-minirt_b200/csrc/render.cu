@@ -118,6 +118,96 @@ __global__ void __launch_bounds__(kBlock) megakernel_regen(SceneView S, LaunchPa
   }
 }
 
+// Multi-scene batch: one persistent launch over the paths of many scenes.
+// Scenes are ordered longest-first by the host (LPT); path index g maps to
+// the scene whose [start, start + paths) range holds it (binary search over
+// <= a few hundred prefix sums). Otherwise the regenerating loop above.
+template <int kBlock>
+__global__ void __launch_bounds__(kBlock) megakernel_batch(const SceneView* __restrict__ views,
+                                                           const BatchItem* __restrict__ items,
+                                                           int n_items, uint64_t total,
+                                                           int* status, unsigned long long* work) {
+  const int lane = threadIdx.x & 31;
+  PathCounters C{0, 0, 0};
+  PathState P;
+  int depth_left = 0, item = 0;
+  uint32_t pixel = 0;
+  bool active = false, done = false;
+  while (true) {
+    const bool need = !active && !done;
+    const unsigned need_mask = __ballot_sync(0xffffffffu, need);
+    if (need_mask) {
+      unsigned long long base = 0;
+      const int leader = __ffs(need_mask) - 1;
+      if (lane == leader) base = atomicAdd(work, (unsigned long long)__popc(need_mask));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (need) {
+        const uint64_t g = base + __popc(need_mask & ((1u << lane) - 1u));
+        if (g >= total) {
+          done = true;
+        } else {
+          int lo = 0, hi = n_items - 1;
+          while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (items[mid].start <= g) lo = mid; else hi = mid - 1;
+          }
+          item = lo;
+          const BatchItem it = items[item];
+          const SceneView& S = views[it.view];
+          const uint64_t idx = g - it.start;
+          const uint32_t npix = (uint32_t)S.width * (uint32_t)S.height;
+          const uint32_t lin = (uint32_t)(idx % npix);
+          const uint32_t sample = it.sample_base + (uint32_t)(idx / npix);
+          pixel = tile_pixel(lin, S.width, S.height);
+          P.rng.s = path_seed(it.seed, pixel, sample);
+          float ox, oy;
+          sample_offset(it.seed, sample, it.jitter, P.rng, ox, oy);
+          camera_ray(S, P, pixel, ox, oy);
+          P.power = f3(1.f, 1.f, 1.f);
+          P.acc = f3(0.f, 0.f, 0.f);
+          P.last_mat = -1;
+          depth_left = it.max_bounces;
+          active = depth_left > 0;
+          if (!active) atomicAdd(it.accum + pixel, make_float4(0.f, 0.f, 0.f, 1.0f));
+        }
+      }
+    }
+    if (__all_sync(0xffffffffu, done)) break;
+    if (active) {
+      const BatchItem& it = items[item];
+      if (!bounce(views[it.view], P, depth_left, status, C)) {
+        active = false;
+        atomicAdd(it.accum + pixel, make_float4(P.acc.x, P.acc.y, P.acc.z, 1.0f));
+      }
+    }
+  }
+}
+
+cudaError_t launch_megakernel_batch(const SceneView* views, const BatchItem* items, int n_items,
+                                    uint64_t total, int* status, unsigned long long* work, int block,
+                                    cudaStream_t st) {
+  if (total == 0 || n_items == 0) return cudaSuccess;
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  block = block > 0 ? block : 128;
+  cudaError_t e = cudaMemsetAsync(work, 0, sizeof(unsigned long long), st);
+  if (e != cudaSuccess) return e;
+#define MRT_BT(B)                                                                          \
+  if (block <= B) {                                                                        \
+    int occ = 0;                                                                           \
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, megakernel_batch<B>, B, 0);        \
+    unsigned grid = (unsigned)std::min<uint64_t>((uint64_t)sms * std::max(occ, 1), (total + B - 1) / B); \
+    megakernel_batch<B><<<grid, B, 0, st>>>(views, items, n_items, total, status, work);  \
+    return cudaGetLastError();                                                             \
+  }
+  MRT_BT(64)
+  MRT_BT(128)
+  MRT_BT(256)
+#undef MRT_BT
+  return cudaErrorInvalidValue;
+}
+
 // Debug probe: full event record of single paths (pixel, sample).
 __global__ void path_events_kernel(SceneView S, LaunchParams L, const int* pix, const int* smp, int n,
                                    float* ev, float* rgb, int* status) {

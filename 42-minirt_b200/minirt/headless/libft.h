@@ -1,11 +1,11 @@
 /*
- * Minimal stand-in for the miniRT project's libft interface (the libft git
- * submodule of the reference is not vendored). Test infrastructure only: it
- * lets the reference's own CPU path (src/ray_tracing, src/material,
- * src/caustic, src/math) compile into the oracle library. Only the types and
- * functions that path uses are declared; the implementations are in
- * libft_shim.c and follow the libft contracts the reference relies on
- * (ft_calloc zeroes, vector_add grows and returns -1 on failure, ...).
+ * Minimal stand-in for miniRT's libft.h (the libft git submodule of miniRT is
+ * not vendored here). It declares the types and functions miniRT's headers
+ * and its path-tracing sources need, so that the drop-in adapter
+ * (minirt_gpu.c) and the test oracle can be compiled headless. A project that
+ * has the real libft compiles against that instead; the adapter itself calls
+ * no libft function. Implementations for the oracle build live in
+ * oracle/shim/libft_shim.c.
  */
 #ifndef LIBFT_H
 # define LIBFT_H

@@ -153,6 +153,8 @@ SIGNATURES = {
     "mrt_set_camera": (C.c_int, [_P, C.POINTER(Camera), C.c_double, C.c_double]),
     "mrt_render": (C.c_int, [_P, C.POINTER(RenderParams), C.POINTER(RenderStats)]),
     "mrt_clear": (C.c_int, [_P]),
+    "mrt_render_batch": (C.c_int, [C.POINTER(_P), C.POINTER(RenderParams), C.c_int32,
+                                   C.POINTER(RenderStats)]),
     "mrt_tune": (C.c_int, [_P, C.c_int32, C.c_uint64, C.POINTER(TuneResult)]),
     "mrt_read_accum": (C.c_int, [_P, _P, C.POINTER(C.c_int32)]),
     "mrt_accumulate_double": (C.c_int, [_P, _P]),
@@ -170,6 +172,21 @@ SIGNATURES = {
 
 class MRTError(RuntimeError):
     pass
+
+
+def render_batch(ctxs: list, params: list[dict], block_size: int = 0) -> "RenderStats":
+    """One persistent launch over the scenes of several contexts (same device)."""
+    lib = load()
+    n = len(ctxs)
+    arr = (_P * n)(*[c.h for c in ctxs])
+    ps = (RenderParams * n)()
+    for i, p in enumerate(params):
+        ps[i] = RenderParams(spp=p["spp"], sample_base=p.get("sample_base", 0), seed=p.get("seed", 1),
+                             max_bounces=p.get("max_bounces", 0), jitter=p.get("jitter", 0),
+                             env_sampler=p.get("env_sampler", 0), block_size=block_size)
+    st = RenderStats()
+    check(lib.mrt_render_batch(arr, ps, n, C.byref(st)), "mrt_render_batch")
+    return st
 
 
 _lib = None

@@ -264,6 +264,15 @@ MRT_API int			mrt_set_camera(mrt_ctx *ctx, const mrt_camera *camera,
 /* Render params->spp samples per pixel into the device accumulator. */
 MRT_API int			mrt_render(mrt_ctx *ctx, const mrt_render_params *params,
 				mrt_render_stats *stats);
+/* Multi-scene batch: renders params[i] on ctx[i] for all i in ONE persistent
+ * launch (all contexts on the same device, each with a built scene). Paths of
+ * all scenes share one work queue, scenes ordered longest-first by predicted
+ * cost (paths x depth x log2 primitives). params[i].form / block_size apply
+ * to the whole batch; offset must be NULL. stats (may be NULL) receives the
+ * totals of the launch. */
+MRT_API int			mrt_render_batch(mrt_ctx **ctx, const mrt_render_params *params,
+				int32_t n, mrt_render_stats *stats);
+
 /* Zero the device accumulator. */
 MRT_API int			mrt_clear(mrt_ctx *ctx);
 /* Copy the device accumulator (sum over samples, W*H*3 floats, row-major,

@@ -46,7 +46,7 @@ def ref_lib():
     if _ref is None:
         if not REF_LIB.exists():
             raise FileNotFoundError(f"{REF_LIB} not built (make -C oracle ref)")
-        lib = C.CDLL(str(REF_LIB))
+        lib = C.CDLL(str(REF_LIB), mode=C.RTLD_GLOBAL)
         sig = {
             "refh_create": (_P, [_P]), "refh_destroy": (None, [_P]),
             "refh_set_seed": (None, [C.c_uint64]), "refh_get_seed": (C.c_uint64, []),
@@ -67,6 +67,11 @@ def ref_lib():
             "refh_photon_count": (C.c_int64, [_P]),
             "refh_photons": (C.c_int, [_P, _P, _P, _P]),
             "refh_caustic_query": (C.c_int, [_P, _P, C.c_int64, C.c_int, _P]),
+            "refh_minirt": (_P, [_P]), "refh_scene_ptr": (_P, [_P]),
+            "refh_viewport_ptr": (_P, [_P]), "refh_shader_data": (_P, [_P]),
+            "refh_gpu_structs": (_P, [_P]), "refh_sample_counters": (C.c_int, [_P, _P]),
+            "refh_gpu_counts": (C.c_int, [_P, _P]),
+            "refh_calc_one_sample": (None, [_P, C.c_double, C.c_double, C.c_int]),
         }
         for k, (r, a) in sig.items():
             f = getattr(lib, k)

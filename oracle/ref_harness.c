@@ -732,3 +732,61 @@ int	refh_caustic_query(void *hv, const double *pts, int64_t n, int k,
 	}
 	return (0);
 }
+
+/* Accessors for driving the miniRT drop-in adapter on the harness's own
+ * t_minirt (tests call the adapter's entry points with these pointers). */
+void	*refh_minirt(void *hv)
+{
+	return (((t_refh *)hv)->m);
+}
+
+void	*refh_scene_ptr(void *hv)
+{
+	return (&((t_refh *)hv)->m->scene);
+}
+
+void	*refh_viewport_ptr(void *hv)
+{
+	return (&((t_refh *)hv)->m->viewport);
+}
+
+void	*refh_shader_data(void *hv)
+{
+	return (&((t_refh *)hv)->m->shaders_data);
+}
+
+void	*refh_gpu_structs(void *hv)
+{
+	return (&((t_refh *)hv)->m->shaders_data.scene);
+}
+
+int	refh_sample_counters(void *hv, int *out3)
+{
+	t_minirt	*m;
+
+	m = ((t_refh *)hv)->m;
+	out3[0] = m->screen.sample;
+	out3[1] = m->screen.sample_total_anim;
+	out3[2] = m->screen.last_sample_am;
+	return (0);
+}
+
+int	refh_gpu_counts(void *hv, int *out6)
+{
+	t_gpu_structs	*g;
+
+	g = &((t_refh *)hv)->m->shaders_data.scene;
+	out6[0] = g->valid;
+	out6[1] = g->spheres_am;
+	out6[2] = g->planes_am;
+	out6[3] = g->triangles_am;
+	out6[4] = g->lights_am;
+	out6[5] = g->mat_am;
+	return (0);
+}
+
+/* The reference's own calc_one_sample with an explicit offset. */
+void	refh_calc_one_sample(void *hv, double ox, double oy, int max_bounces)
+{
+	calc_one_sample(((t_refh *)hv)->m, (t_vec3){ox, oy, 0}, max_bounces);
+}

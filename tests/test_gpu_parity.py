@@ -339,3 +339,26 @@ def test_autotuner_picks_a_working_form(mrt, oracle, mg):
     ctx.render(4, seed=5, form=mrt.FORM_AUTO)
     b, _ = ctx.read_accum()
     assert (np.abs(a - b).max(axis=2) <= 1e-4 * np.maximum(np.abs(a).max(axis=2), 1e-2)).mean() >= 0.99
+
+
+def test_batch_matches_individual_renders(mrt, oracle, scenes):
+    """Several scenes of uneven size in one launch: each accumulator equals
+    its own single-scene render on the same streams."""
+    specs = [scenes.make_c0(0, 40, 30), scenes.make_c1(3, 32, 24, freq=6, sky=(32, 16)),
+             scenes.make_c2(2, 24, 16, grid=12, photons=2000), scenes.make_c0(5, 16, 48)]
+    ctxs = []
+    for sc in specs:
+        c = mrt.Context(sc.width, sc.height)
+        c.build(oracle.canonical_scene(sc))
+        ctxs.append(c)
+    params = [dict(spp=4 + i, seed=11 + i, max_bounces=0) for i in range(len(ctxs))]
+    st = mrt.render_batch(ctxs, params)
+    assert st.kernel_launches == 1 and st.paths == sum(sc.width * sc.height * (4 + i)
+                                                       for i, sc in enumerate(specs))
+    batch = [c.read_accum() for c in ctxs]
+    for i, c in enumerate(ctxs):
+        assert batch[i][1] == params[i]["spp"]
+        c.clear()
+        c.render(params[i]["spp"], seed=params[i]["seed"])
+        single, _ = c.read_accum()
+        np.testing.assert_allclose(batch[i][0], single, rtol=1e-4, atol=1e-5)
