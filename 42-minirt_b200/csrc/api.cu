@@ -133,7 +133,6 @@ struct mrt_ctx {
   int bvh_depth = 0;
   int auto_form = MRT_FORM_MEGAKERNEL;   // choice of the autotuner for this scene
   int auto_block = 0, auto_capacity = 0, auto_sort = 0;
-  int plain_megakernel = 0;              // 1: one path per thread, no regeneration
 };
 
 namespace {
@@ -760,7 +759,7 @@ extern "C" int mrt_render(mrt_ctx* c, const mrt_render_params* p, mrt_render_sta
   if (!c->has_scene) return set_err(MRT_ERR_INVALID, "no scene: call mrt_scene_build first");
   if (p->spp < 0 || p->sample_base < 0) return set_err(MRT_ERR_INVALID, "negative spp / sample_base");
   if (p->render_mode < 0 || p->render_mode > 2) return set_err(MRT_ERR_INVALID, "render_mode %d", p->render_mode);
-  if (p->form < 0 || p->form > 2) return set_err(MRT_ERR_INVALID, "form %d", p->form);
+  if (p->form < 0 || p->form > 3) return set_err(MRT_ERR_INVALID, "form %d", p->form);
   if (p->offset && p->spp != 1) return set_err(MRT_ERR_INVALID, "explicit offset needs spp == 1");
   if (p->block_size && (p->block_size % 32 || p->block_size > 256))
     return set_err(MRT_ERR_INVALID, "block_size %d", p->block_size);
@@ -800,7 +799,7 @@ extern "C" int mrt_render(mrt_ctx* c, const mrt_render_params* p, mrt_render_sta
     int spp_chunk = (int)std::max<uint64_t>(1, max_paths / std::max<uint64_t>(npix, 1));
     // the persistent, regenerating megakernel for path tracing; the plain
     // one-path-per-thread launch for the debug modes and when counting
-    const bool regen = p->render_mode == 0 && !c->plain_megakernel;
+    const bool regen = p->render_mode == 0 && form != MRT_FORM_MEGAKERNEL_PLAIN;
     for (int s = 0; s < p->spp; s += spp_chunk) {
       int k = std::min(spp_chunk, p->spp - s);
       L.sample_base = (uint32_t)(p->sample_base + s);

@@ -29,7 +29,7 @@ STATUS_NAMES = {
     -7: "MRT_ERR_NO_DEVICE", -8: "MRT_ERR_STACK",
 }
 
-FORM_MEGAKERNEL, FORM_WAVEFRONT, FORM_AUTO = 0, 1, 2
+FORM_MEGAKERNEL, FORM_WAVEFRONT, FORM_AUTO, FORM_MEGAKERNEL_PLAIN = 0, 1, 2, 3
 JITTER_SHARED, JITTER_PIXEL = 0, 1
 LIGHT_POINT, LIGHT_DIRECTIONAL = 0, 1
 
@@ -273,7 +273,8 @@ class Context:
         """Times the forms / launch shapes, keeps the fastest for FORM_AUTO."""
         r = TuneResult()
         check(self.lib.mrt_tune(self.h, spp, seed, C.byref(r)), "mrt_tune")
-        names = {FORM_MEGAKERNEL: "megakernel", FORM_WAVEFRONT: "wavefront"}
+        names = {FORM_MEGAKERNEL: "megakernel", FORM_WAVEFRONT: "wavefront",
+                 FORM_MEGAKERNEL_PLAIN: "megakernel_plain"}
         return [dict(form=names[e.form], block_size=e.block_size, queue_capacity=e.queue_capacity,
                      sort_threshold=e.sort_threshold, mpaths_s=e.mpaths_s, best=(i == r.best))
                 for i, e in enumerate(r.entry[:r.n])]

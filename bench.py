@@ -8,8 +8,14 @@ benchmark scene). One step = one pass over the frame at --spp-per-step
 samples per pixel (16 steps = the 256 spp render).
 
   value       device time (CUDA events on the library's stream) of the timed
-              steps, inputs resident in HBM; the best of the two forms
-              (plain megakernel, wavefront), both reported under "forms".
+              steps, inputs resident in HBM; the best of the forms (plain
+              one-path-per-thread megakernel, persistent regenerating
+              megakernel, wavefront), each reported under "forms".
+  relmse      time to relMSE <= 1e-3: relMSE(N) = mean((img-ref)^2/(ref^2+0.01))
+              is measured at 16 and 256 spp against an independent --ref-spp
+              render; relMSE = c/N (unbiased estimator, independent
+              reference noise c/ref_spp), so N* = c/1e-3 and the time per
+              form is N* x pixels / Mpaths/s.
   e2e         the same render through the C-ABI a reference host calls:
               per step a camera upload, the render and a device->host read of
               the frame accumulated into a pinned double buffer
@@ -53,7 +59,9 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c1")
     ap.add_argument("--spp-per-step", type=int, default=16)
-    ap.add_argument("--forms", default="megakernel,wavefront")
+    ap.add_argument("--forms", default="megakernel_plain,megakernel,wavefront")
+    ap.add_argument("--no-relmse", action="store_true")
+    ap.add_argument("--ref-spp", type=int, default=1024)
     ap.add_argument("--cpu-seconds", type=float, default=8.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     return ap.parse_args()
@@ -133,6 +141,43 @@ def run_reference_arm(a) -> None:
     print(json.dumps(line), flush=True)
 
 
+def rel_mse(img: np.ndarray, ref: np.ndarray) -> float:
+    return float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
+
+
+def convergence(ctx, sc, spp_step: int, ref_spp: int, forms: dict, fid: int) -> dict:
+    """Time to relMSE <= 1e-3 per form from the measured 1/N law."""
+    ctx.clear()
+    done = 0
+    while done < ref_spp:
+        k = min(64, ref_spp - done)
+        ctx.render(k, seed=777, sample_base=done, form=fid)
+        done += k
+    ref, n = ctx.read_accum()
+    ref = ref / n
+    pts = {}
+    for n_spp in (16, 256):
+        ctx.clear()
+        done = 0
+        while done < n_spp:
+            k = min(spp_step, n_spp - done)
+            ctx.render(k, seed=31, sample_base=done, form=fid)
+            done += k
+        img, n = ctx.read_accum()
+        pts[n_spp] = rel_mse(img / n, ref)
+    c = (pts[16] - pts[256]) / (1 / 16 - 1 / 256)
+    c = max(c, 1e-12)
+    n_star = c / 1e-3
+    npix = sc.width * sc.height
+    out = {"relmse_16spp": pts[16], "relmse_256spp": pts[256], "ref_spp": ref_spp,
+           "c": c, "spp_to_1e-3": n_star, "relmse_definition": "mean((x-r)^2/(r^2+0.01))"}
+    for name, f in forms.items():
+        if "value" in f:
+            out[f"time_to_1e-3_s_{name}"] = n_star * npix / (f["value"] * 1e6)
+    ctx.clear()
+    return out
+
+
 def workload_config(a, sc) -> dict:
     return {"workload": f"{a.config}: 1920x1080, 256 spp, depth 12, 1,310,720-triangle displaced "
                         "geodesic sphere, 16 materials, 2048x1024 RGBE sky with importance sampling"
@@ -147,6 +192,7 @@ def main() -> int:
     if a.impl == "reference":
         run_reference_arm(a)
         return 0
+    import distributed as D
     import mrt
     import scenes
 
@@ -188,7 +234,8 @@ def main() -> int:
             dist.barrier()
 
     forms = {}
-    form_ids = {"megakernel": mrt.FORM_MEGAKERNEL, "wavefront": mrt.FORM_WAVEFRONT}
+    form_ids = {"megakernel": mrt.FORM_MEGAKERNEL, "wavefront": mrt.FORM_WAVEFRONT,
+                "megakernel_plain": mrt.FORM_MEGAKERNEL_PLAIN}
     clocks = Clocks(local)
     launches_total = 0
     best = None
@@ -205,7 +252,7 @@ def main() -> int:
         barrier()
         ms = 0.0
         launches = 0
-        base = rank * a.steps * spp
+        base, _ = D.shard_samples(a.steps * spp * world, world, rank)
         for s in range(a.steps):
             st = ctx.render(spp, seed=1, sample_base=base + s * spp, form=fid)
             ms += st.ms
@@ -249,8 +296,12 @@ def main() -> int:
         e2e_s = float(t.item())
         # the frames of all ranks summed on rank 0 (one NCCL reduce)
         frame = torch.from_numpy(host.astype(np.float32)).cuda(local)
-        dist.reduce(frame, dst=0)
+        D.reduce_frame(frame, dist)
     e2e = paths_per_step * a.steps * world / e2e_s / 1e6
+
+    relmse = None
+    if not a.no_relmse and world == 1:
+        relmse = convergence(ctx, sc, spp, a.ref_spp, forms, form_ids[best])
 
     f = forms[best]
     achieved = bpp * (paths_per_step / max(f["launches"] / a.steps, 1)) / (f["launch_ms"] / 1000.0) / 1e9
@@ -273,6 +324,8 @@ def main() -> int:
         "clocks": clk,
         "scene_build_s": build_s,
     }
+    if relmse is not None:
+        line["relmse"] = relmse
     if cpu is not None:
         line["cpu_baseline"] = {"value": cpu["mpaths_s"], "unit": UNIT, "cores": cpu["procs"],
                                 "kind": "reference", "sample": cpu["sample"]}

@@ -205,9 +205,10 @@ typedef struct mrt_scene_desc
 
 typedef enum mrt_form
 {
-	MRT_FORM_MEGAKERNEL = 0,   /* one thread = one path, all bounces */
-	MRT_FORM_WAVEFRONT = 1,    /* per-bounce queues, material-sorted shading */
-	MRT_FORM_AUTO = 2          /* autotuned choice for this scene */
+	MRT_FORM_MEGAKERNEL = 0,       /* persistent megakernel, lanes regenerate paths */
+	MRT_FORM_WAVEFRONT = 1,        /* per-bounce queues, material-sorted shading */
+	MRT_FORM_AUTO = 2,             /* autotuned choice for this scene */
+	MRT_FORM_MEGAKERNEL_PLAIN = 3  /* one thread = one path, all bounces (baseline form) */
 }	mrt_form;
 
 typedef enum mrt_jitter
