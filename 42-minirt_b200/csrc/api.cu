@@ -97,8 +97,30 @@ int wf_render(WfHost* H, const SceneView& v, const LaunchParams& L, int spp, int
               int sort_threshold, int use_graph, float4* frame, int* status, cudaStream_t st,
               unsigned* launches, const char** err);
 
+// Device state of the differentiable forward / backward (mrt_forward,
+// mrt_backward), sized for the current scene.
+struct DiffState {
+  int M = 0, EW = 0, EH = 0;
+  bool tables = false;                 // HDRI NEE tables are rebuilt from theta
+  DevBuf<float> theta, grad, img, dimg;
+  DevBuf<MaterialD> mats;
+  DevBuf<float4> accum, grid, rec0, rec1, state;
+  DevBuf<TapeEntry> tape;
+  DevBuf<int2> aux;
+  DevBuf<float> pdf, cm, cc;
+  DevBuf<double> gray, raw, rowcdf, scal, cdfh;
+  void release() {
+    theta.release(); grad.release(); img.release(); dimg.release(); mats.release();
+    accum.release(); grid.release(); rec0.release(); rec1.release(); aux.release();
+    state.release(); tape.release();
+    pdf.release(); cm.release(); cc.release();
+    gray.release(); raw.release(); rowcdf.release(); scal.release(); cdfh.release();
+  }
+};
+
 struct mrt_ctx {
   int device = 0;
+  DiffState* diff = nullptr;
   WfHost* wf = nullptr;
   int W = 0, H = 0;
   cudaStream_t stream = nullptr;
@@ -337,6 +359,7 @@ void mrt_destroy(mrt_ctx* c) {
   c->ph_pos.release(); c->ph_pow.release(); c->ph_pos_raw.release(); c->ph_pow_raw.release();
   c->cell_start.release(); c->cell_of.release(); c->ph_count.release();
   wf_destroy(c->wf);
+  if (c->diff) { c->diff->release(); delete c->diff; }
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -458,6 +481,12 @@ extern "C" int mrt_scene_build(mrt_ctx* c, const mrt_scene_desc* d) {
       (d->n_planes && !d->planes) || (d->n_meshes && !d->meshes) || (d->n_lights && !d->lights))
     return set_err(MRT_ERR_INVALID, "null element array with a non-zero count");
   c->has_scene = false;
+  if (c->diff) {
+    cudaStreamSynchronize(c->stream);
+    c->diff->release();
+    delete c->diff;
+    c->diff = nullptr;
+  }
   SceneView v{};
   v.width = c->W;
   v.height = c->H;
@@ -1153,4 +1182,276 @@ extern "C" int mrt_caustic_query(mrt_ctx* c, const double* pts3, int64_t n, int3
   CK(cudaFreeAsync(dout, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return MRT_OK;
+}
+
+// ------------------------------------------------- differentiable rendering
+
+namespace {
+
+// Direction and radiance texel of every (row index iv, column index iu) the
+// inverse-CDF tables can return: v = iv / (H-1), u = iu / (W-1) as floats,
+// then calc_inverse_transform_sampling_dir (get_dir.c:29-41) and the texel
+// get_background_color reads for that direction (background.c:15-70), with
+// the same double-precision libm calls as env_records.
+void env_grid(int W, int H, std::vector<float4>& grid) {
+  grid.assign((size_t)W * H, make_float4(0.f, 1.f, 0.f, 0.f));
+  auto work = [&](int y0, int y1) {
+    for (int iv = y0; iv < y1; ++iv) {
+      const double v = (double)(float)((double)iv / (double)(H - 1));
+      const float theta = (float)((v - 0.5) * kPiD);
+      const double th = (double)theta;
+      for (int iu = 0; iu < W; ++iu) {
+        const double u = (double)(float)((double)iu / (double)(W - 1));
+        const float phi = (float)((0.5 - u) * 2 * kPiD);
+        const double ph = (double)phi;
+        const V3 dir = {std::cos(th) * std::cos(ph), std::sin(th), std::cos(th) * std::sin(ph)};
+        const V3 un = unitv(dir);
+        const double vv = 0.5 + std::asin(un.y) / kPiD;
+        const double uu = 0.5 - std::atan2(un.z, un.x) / (2.0 * kPiD);
+        int x = (int)(uu * (W - 1)), yy = (int)(vv * (H - 1));
+        x = std::min(std::max(x, 0), W - 1);
+        yy = std::min(std::max(yy, 0), H - 1);
+        grid[(size_t)iv * W + iu] =
+            make_float4((float)dir.x, (float)dir.y, (float)dir.z, int_bits_as_float(yy * W + x));
+      }
+    }
+  };
+  const int nt = std::max(1, std::min((int)std::thread::hardware_concurrency(), 32));
+  std::vector<std::thread> pool;
+  for (int t = 0; t < nt; ++t) pool.emplace_back(work, H * t / nt, H * (t + 1) / nt);
+  for (auto& th : pool) th.join();
+}
+
+int64_t diff_count(const mrt_ctx* c, int64_t counts[4]) {
+  const int64_t M = c->view.n_mats;
+  const int64_t T = c->view.has_env ? (int64_t)c->view.env_w * c->view.env_h : 0;
+  const int64_t k[4] = {3 * M, M, M, 3 * T};
+  if (counts)
+    for (int i = 0; i < 4; ++i) counts[i] = k[i];
+  return k[0] + k[1] + k[2] + k[3];
+}
+
+int diff_check(mrt_ctx* c, const float* theta, const mrt_render_params* p) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!c->has_scene) return set_err(MRT_ERR_INVALID, "no scene: call mrt_scene_build first");
+  if (!theta || !p) return set_err(MRT_ERR_INVALID, "null theta / params");
+  if (p->spp <= 0 || p->sample_base < 0) return set_err(MRT_ERR_INVALID, "spp must be > 0, sample_base >= 0");
+  const int mb = p->max_bounces > 0 ? p->max_bounces : c->view.max_bounces;
+  if (mb < 1 || mb > kMaxTape)
+    return set_err(MRT_ERR_INVALID, "differentiable paths take 1..%d bounces, not %d", kMaxTape, mb);
+  if (c->view.n_mats > kDiffMaxMats)
+    return set_err(MRT_ERR_INVALID, "%d materials: the adjoint handles at most %d", c->view.n_mats,
+                   kDiffMaxMats);
+  if (c->view.has_env && c->view.env_inv_gamma != 1.0f)
+    return set_err(MRT_ERR_INVALID, "a differentiable sky needs a linear HDR (gamma 1)");
+  return MRT_OK;
+}
+
+// Upload theta and rebuild the materials, sky tables and NEE records from
+// it; v receives the scene view the forward and the replay trace.
+int diff_prepare(mrt_ctx* c, const float* theta, SceneView& v) {
+  cudaStream_t st = c->stream;
+  if (!c->diff) c->diff = new DiffState();
+  DiffState& D = *c->diff;
+  int64_t counts[4];
+  const int64_t n = diff_count(c, counts);
+  const int M = c->view.n_mats;
+  const int W = c->view.has_env ? c->view.env_w : 0, H = c->view.has_env ? c->view.env_h : 0;
+  const size_t npix = (size_t)c->W * c->H;
+  if (D.theta.n != (size_t)std::max<int64_t>(n, 1) || D.M != M || D.EW != W || D.EH != H) {
+    D.release();
+    D.M = M; D.EW = W; D.EH = H;
+    D.tables = c->view.env_nee && W >= 2 && H >= 2;
+    CK(D.theta.alloc(std::max<int64_t>(n, 1)));
+    CK(D.grad.alloc(n + 1));   // + d loss / d column average
+    CK(D.img.alloc(3 * npix));
+    CK(D.dimg.alloc(3 * npix));
+    CK(D.accum.alloc(npix));
+    CK(D.mats.alloc(std::max(M, 1)));
+    if (D.tables) {
+      const size_t t = (size_t)W * H, no = (size_t)(H - 1) * W;
+      std::vector<float4> grid;
+      env_grid(W, H, grid);
+      CK(D.grid.upload(grid.data(), grid.size(), st));
+      CK(D.rec0.alloc(no)); CK(D.rec1.alloc(no)); CK(D.aux.alloc(no));
+      CK(D.pdf.alloc(t)); CK(D.cm.alloc(H)); CK(D.cc.alloc(t));
+      CK(D.gray.alloc(t)); CK(D.raw.alloc(H)); CK(D.rowcdf.alloc(t)); CK(D.scal.alloc(8)); CK(D.cdfh.alloc(H));
+    }
+  }
+  if (n) CK(cudaMemcpyAsync(D.theta.p, theta, sizeof(float) * n, cudaMemcpyDefault, st));
+  CK(launch_diff_mats(c->mats.p, D.theta.p, M, D.mats.p, st));
+  v = c->view;
+  v.mats = D.mats.p;
+  const float* sky = D.theta.p + 5 * (size_t)M;
+  if (c->view.has_env) v.sky_rgb = sky;
+  if (D.tables) {
+    EnvBuild E{};
+    E.rgb = sky;
+    E.W = W;
+    E.H = H;
+    E.exposure_zero = 1;
+    E.gray = D.gray.p; E.raw = D.raw.p; E.row_cdf = D.rowcdf.p; E.scal = D.scal.p; E.cdf_h = D.cdfh.p;
+    E.pdf_joint = D.pdf.p; E.cdf_m_inv = D.cm.p; E.cdf_c_inv = D.cc.p;
+    E.out_prob = nullptr;
+    CK(launch_env_tables(E, st));
+    DiffEnvRecords R{D.cm.p, D.cc.p, D.pdf.p, D.grid.p, sky, W, H, D.rec0.p, D.rec1.p, D.aux.p};
+    CK(launch_diff_env_records(R, st));
+    v.env_rec0 = D.rec0.p;
+    v.env_rec1 = D.rec1.p;
+    v.pdf_joint = D.pdf.p;
+    v.cdf_m_inv = D.cm.p;
+    v.cdf_c_inv = D.cc.p;
+    v.alias = nullptr;
+    v.env_lookup = 1;
+  }
+  return MRT_OK;
+}
+
+int diff_finish(mrt_ctx* c, mrt_render_stats* stats, uint64_t paths, int launches) {
+  CK(cudaEventRecord(c->ev1, c->stream));
+  CK(cudaEventSynchronize(c->ev1));
+  int status = 0;
+  int rc = read_status(c, &status);
+  if (rc) return rc;
+  if (stats) {
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    *stats = mrt_render_stats{};
+    stats->ms = ms;
+    stats->paths = paths;
+    stats->kernel_launches = (uint32_t)launches;
+    stats->status = status;
+  }
+  if (status & ST_STACK) return set_err(MRT_ERR_STACK, "traversal stack overflow (status 0x%x)", status);
+  if (status & ST_BUDGET) return set_err(MRT_ERR_BUDGET, "traversal iteration budget exhausted (status 0x%x)", status);
+  if (status) return set_err(MRT_ERR_ABORTED, "device status 0x%x", status);
+  return MRT_OK;
+}
+
+}  // namespace
+
+extern "C" int64_t mrt_diff_layout(mrt_ctx* c, int64_t counts[4]) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!c->has_scene) return set_err(MRT_ERR_INVALID, "no scene: call mrt_scene_build first");
+  return diff_count(c, counts);
+}
+
+extern "C" int mrt_diff_get_params(mrt_ctx* c, float* theta) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!c->has_scene) return set_err(MRT_ERR_INVALID, "no scene: call mrt_scene_build first");
+  if (!theta) return set_err(MRT_ERR_INVALID, "null theta");
+  int64_t counts[4];
+  diff_count(c, counts);
+  const int M = c->view.n_mats;
+  std::vector<MaterialD> mats(std::max(M, 1));
+  if (M) CK(cudaMemcpy(mats.data(), c->mats.p, sizeof(MaterialD) * M, cudaMemcpyDeviceToHost));
+  std::vector<float> h((size_t)5 * M);
+  for (int m = 0; m < M; ++m) {
+    for (int k = 0; k < 3; ++k) h[3 * m + k] = mats[m].color[k];
+    h[3 * M + m] = mats[m].roughness;
+    h[4 * M + m] = mats[m].emission_strength;
+  }
+  if (M) CK(cudaMemcpyAsync(theta, h.data(), sizeof(float) * h.size(), cudaMemcpyDefault, c->stream));
+  if (counts[3]) {
+    float* d = nullptr;
+    CK(cudaMallocAsync(&d, sizeof(float) * counts[3], c->stream));
+    cudaError_t e = launch_diff_sky_init(c->view, d, c->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(theta + 5 * (size_t)M, d, sizeof(float) * counts[3], cudaMemcpyDefault, c->stream);
+    cudaFreeAsync(d, c->stream);
+    CK(e);
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  return MRT_OK;
+}
+
+extern "C" int mrt_forward(mrt_ctx* c, const float* theta, const mrt_render_params* p, float* image,
+                           mrt_render_stats* stats) {
+  int rc = diff_check(c, theta, p);
+  if (rc) return rc;
+  if (!image) return set_err(MRT_ERR_INVALID, "null image");
+  CK(cudaEventRecord(c->ev0, c->stream));
+  SceneView v;
+  rc = diff_prepare(c, theta, v);
+  if (rc) return rc;
+  DiffState& D = *c->diff;
+  const uint64_t npix = (uint64_t)c->W * c->H;
+  CK(cudaMemsetAsync(c->status.p, 0, sizeof(int), c->stream));
+  CK(cudaMemsetAsync(D.accum.p, 0, D.accum.bytes(), c->stream));
+  LaunchParams L{};
+  L.seed = p->seed;
+  L.max_bounces = p->max_bounces > 0 ? p->max_bounces : v.max_bounces;
+  L.jitter = p->jitter;
+  const int spp_chunk = (int)std::max<uint64_t>(1, (1ull << 26) / std::max<uint64_t>(npix, 1));
+  int launches = 0;
+  for (int s = 0; s < p->spp; s += spp_chunk) {
+    const int k = std::min(spp_chunk, p->spp - s);
+    L.sample_base = (uint32_t)(p->sample_base + s);
+    L.n_paths = npix * (uint64_t)k;
+    CK(launch_megakernel_regen(v, L, D.accum.p, c->status.p, c->counters.p + 7, 0, 0, c->stream));
+    launches++;
+  }
+  CK(launch_diff_image(D.accum.p, D.img.p, (int)npix, 1.0f / (float)p->spp, c->stream));
+  CK(cudaMemcpyAsync(image, D.img.p, sizeof(float) * 3 * npix, cudaMemcpyDefault, c->stream));
+  return diff_finish(c, stats, npix * (uint64_t)p->spp, launches + 1);
+}
+
+extern "C" int mrt_backward(mrt_ctx* c, const float* theta, const mrt_render_params* p,
+                            const float* grad_image, float* grad_theta, mrt_render_stats* stats) {
+  int rc = diff_check(c, theta, p);
+  if (rc) return rc;
+  if (!grad_image || !grad_theta) return set_err(MRT_ERR_INVALID, "null grad_image / grad_theta");
+  CK(cudaEventRecord(c->ev0, c->stream));
+  SceneView v;
+  rc = diff_prepare(c, theta, v);
+  if (rc) return rc;
+  DiffState& D = *c->diff;
+  int64_t counts[4];
+  const int64_t n = diff_count(c, counts);
+  const uint64_t npix = (uint64_t)c->W * c->H;
+  CK(cudaMemsetAsync(c->status.p, 0, sizeof(int), c->stream));
+  CK(cudaMemcpyAsync(D.dimg.p, grad_image, sizeof(float) * 3 * npix, cudaMemcpyDefault, c->stream));
+  CK(cudaMemsetAsync(D.grad.p, 0, D.grad.bytes(), c->stream));
+  AdjointArgs A{};
+  A.n_paths = npix * (uint64_t)p->spp;
+  A.seed = p->seed;
+  A.sample_base = (uint32_t)p->sample_base;
+  A.max_bounces = p->max_bounces > 0 ? p->max_bounces : v.max_bounces;
+  A.jitter = p->jitter;
+  A.n_mats = D.M;
+  A.n_texels = D.tables ? D.EW * D.EH : 0;
+  A.inv_spp = 1.0f / (float)p->spp;
+  A.pdf_dgray = 255.0f;
+  A.col = D.tables ? D.scal.p : nullptr;
+  A.dimg = D.dimg.p;
+  A.env_aux = D.tables ? D.aux.p : nullptr;
+  A.g_mats = D.grad.p;
+  A.g_sky = D.grad.p + 5 * (size_t)D.M;
+  A.g_col = D.grad.p + n;
+  // samples per chunk: the tape (80 B per bounce) stays within a budget of
+  // device memory, at most 16 GiB or a quarter of what is free
+  size_t free_b = 0, total_b = 0;
+  CK(cudaMemGetInfo(&free_b, &total_b));
+  const size_t have = D.tape.bytes() + D.state.bytes();
+  const size_t budget = std::min<size_t>(16ull << 30, (free_b + have) / 4);
+  const size_t per_sample = npix * ((size_t)A.max_bounces * sizeof(TapeEntry) + 4 * sizeof(float4));
+  const int spp_chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)p->spp, budget / per_sample));
+  const size_t paths_chunk = npix * (size_t)spp_chunk;
+  if (D.tape.n < paths_chunk * A.max_bounces) CK(D.tape.alloc(paths_chunk * A.max_bounces));
+  if (D.state.n < 4 * paths_chunk) CK(D.state.alloc(4 * paths_chunk));
+  int launches = 0;
+  for (int s0 = 0; s0 < p->spp; s0 += spp_chunk) {
+    const int k = std::min(spp_chunk, p->spp - s0);
+    AdjointArgs Ac = A;
+    Ac.n_paths = npix * (uint64_t)k;
+    Ac.sample_base = (uint32_t)(p->sample_base + s0);
+    CK(launch_adjoint_chunk(v, Ac, D.tape.p, D.state.p, c->counters.p + 7, c->status.p, c->stream));
+    launches += 1 + A.max_bounces;
+  }
+  CK(launch_diff_sky_mean(A, c->stream));
+  if (n) CK(cudaMemcpyAsync(grad_theta, D.grad.p, sizeof(float) * n, cudaMemcpyDefault, c->stream));
+  return diff_finish(c, stats, A.n_paths, launches + (A.n_texels ? 1 : 0));
 }

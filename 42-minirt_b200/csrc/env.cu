@@ -24,6 +24,12 @@ __global__ void grey_kernel(EnvBuild E) {
   size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   size_t n = (size_t)E.W * E.H;
   if (i >= n) return;
+  if (E.rgb) {
+    const double r = __dmul_rn((double)E.rgb[3 * i], 255.0), g = __dmul_rn((double)E.rgb[3 * i + 1], 255.0),
+                 b = __dmul_rn((double)E.rgb[3 * i + 2], 255.0);
+    E.gray[i] = __dadd_rn(__dadd_rn(__dmul_rn(0.2126, r), __dmul_rn(0.7152, g)), __dmul_rn(0.0722, b));
+    return;
+  }
   uint32_t px = E.rgbe[i];
   int e = (int)(px >> 24);
   double scale = ldexp(1.0, e - 128);
@@ -155,6 +161,7 @@ cudaError_t launch_env_tables(const EnvBuild& E, cudaStream_t st) {
   conditional_cdf_kernel<<<(E.H + 63) / 64, 64, 0, st>>>(E);
   conditional_inv_kernel<<<(unsigned)((n + b - 1) / b), b, 0, st>>>(E);
   const size_t no = (size_t)(E.H - 1) * E.W;
+  if (!E.out_prob) return cudaGetLastError();
   outcome_kernel<<<(unsigned)((no + b - 1) / b), b, 0, st>>>(E);
   return cudaGetLastError();
 }

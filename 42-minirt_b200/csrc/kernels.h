@@ -63,6 +63,8 @@ cudaError_t launch_accum_to_rgb(const float4* accum, float* rgb, int n, cudaStre
 // outcome probabilities / records of the two-step sampler ((H-1)*W entries).
 struct EnvBuild {
   const uint32_t* rgbe;
+  const float* rgb;        // when set: linear float RGB per texel instead of rgbe
+                           // (grey = 0.2126*255r + 0.7152*255g + 0.0722*255b)
   int W, H;
   double exposure_scale;   // powf(2, exposure) widened, used when exposure != 0
   int exposure_zero;
@@ -75,9 +77,66 @@ struct EnvBuild {
   float* pdf_joint;
   float* cdf_m_inv;
   float* cdf_c_inv;
-  double* out_prob;        // (H-1)*W
+  double* out_prob;        // (H-1)*W, or null to skip the outcome probabilities
 };
 cudaError_t launch_env_tables(const EnvBuild& E, cudaStream_t st);
+
+// Differentiable rendering (adjoint.cu).
+constexpr int kMaxTape = 16;       // bounces a differentiable path may take
+constexpr int kDiffMaxMats = 1024; // materials (shared-memory gradient accumulators)
+
+struct DiffEnvRecords {
+  const float* cdf_m_inv;  // H
+  const float* cdf_c_inv;  // W*H
+  const float* pdf_joint;  // W*H
+  const float4* grid;      // W*H: direction .xyz and texel (int bits) per (row, column) index
+  const float* sky;        // W*H*3 linear radiance
+  int W, H;
+  float4* rec0;            // (H-1)*W outputs
+  float4* rec1;
+  int2* aux;               // (radiance texel, pdf_joint index)
+};
+
+struct AdjointArgs {
+  uint64_t n_paths;
+  uint64_t seed;
+  uint32_t sample_base;
+  int max_bounces;         // <= kMaxTape
+  int jitter;
+  int n_mats;
+  int n_texels;
+  float inv_spp;
+  float pdf_dgray;         // d grey / d (lum-weighted channel): 255
+  const double* col;       // column average of the grey values (device)
+  const float* dimg;       // d loss / d image, W*H*3
+  const int2* env_aux;
+  float* g_mats;           // [albedo M*3 | roughness M | emission M]
+  float* g_sky;            // W*H*3
+  float* g_col;            // one float
+};
+
+// Tape of the backward: one entry per bounce, tape[k * n_paths + path].
+struct __align__(16) TapeEntry {   // 80 B
+  float4 o_t;          // ray origin, hit distance (root choice for spheres)
+  float4 d_ra;         // ray direction as traced (not normalised), sampler random 1
+  float4 P_rb;         // path power before shading, sampler random 2
+  float4 T;            // direct-light + caustic term of default_mat (detached)
+  int4 meta;           // primitive, material, flags, HDRI NEE outcome
+};
+
+cudaError_t launch_diff_mats(const MaterialD* base, const float* theta, int M, MaterialD* out,
+                             cudaStream_t st);
+cudaError_t launch_diff_env_records(const DiffEnvRecords& E, cudaStream_t st);
+cudaError_t launch_diff_image(const float4* accum, float* img, int npix, float inv_spp, cudaStream_t st);
+cudaError_t launch_diff_sky_init(const SceneView& S, float* out, cudaStream_t st);
+// Backward of the paths [sample_base, sample_base + n_paths / W*H) of one
+// chunk: replay writing the tape (n_paths * max_bounces entries) and the
+// per-path state (4 float4 per path), then one reverse launch per bounce
+// level. Gradients accumulate into A.g_*.
+cudaError_t launch_adjoint_chunk(const SceneView& S, const AdjointArgs& A, TapeEntry* tape, float4* state,
+                                 unsigned long long* work, int* status, cudaStream_t st);
+// The dense term of the pdf gradient (after all chunks).
+cudaError_t launch_diff_sky_mean(const AdjointArgs& A, cudaStream_t st);
 
 // Photons (photon.cu)
 struct PhotonEmit {

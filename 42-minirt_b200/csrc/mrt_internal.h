@@ -110,6 +110,7 @@ struct SceneView {
   int env_exposure_zero;
   float env_inv_gamma;   // 1/gamma, 1 = linear
   int has_env;           // sky texture present
+  const float* sky_rgb;  // when set: linear sky radiance per texel (W*H*3), used instead of rgbe
   int env_nee;           // importance-sampling tables present
   const float2* alias;   // (prob, alias as int bits), n_env_outcomes entries
   const float4* env_rec0;  // per outcome: direction .xyz, pdf

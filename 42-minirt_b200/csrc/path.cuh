@@ -197,6 +197,22 @@ __device__ __forceinline__ bool bounce(const SceneView& S, PathState& P, int& de
   return depth_left > 0;
 }
 
+// Pixel of the lin-th path of a sample: 8x4 tiles so that a warp traces
+// neighbouring primary rays.
+__device__ __forceinline__ uint32_t tile_pixel(uint32_t lin, int W, int H) {
+  // 8x4 tiles in row-major tile order; ragged edge tiles fall back to row-major
+  const uint32_t tw = 8, th = 4;
+  const uint32_t tiles_x = (W + tw - 1) / tw;
+  const uint32_t full_h = (H / th) * th;
+  const uint32_t full_rows_pixels = full_h * W;
+  if (lin < full_rows_pixels && (W % tw) == 0) {
+    uint32_t tile = lin / (tw * th), in = lin % (tw * th);
+    uint32_t tx = tile % tiles_x, ty = tile / tiles_x;
+    return (ty * th + in / tw) * W + tx * tw + in % tw;
+  }
+  return lin;
+}
+
 // Sub-pixel offset of a sample: shared by every pixel of the sample
 // (draw_pixels, render.c:33) or per pixel, from the path's own stream.
 __device__ __forceinline__ void sample_offset(uint64_t seed, uint32_t sample, int jitter, Rng& rng,

@@ -11,20 +11,6 @@
 
 namespace mrt {
 
-__device__ __forceinline__ uint32_t tile_pixel(uint32_t lin, int W, int H) {
-  // 8x4 tiles in row-major tile order; ragged edge tiles fall back to row-major
-  const uint32_t tw = 8, th = 4;
-  const uint32_t tiles_x = (W + tw - 1) / tw;
-  const uint32_t full_h = (H / th) * th;
-  const uint32_t full_rows_pixels = full_h * W;
-  if (lin < full_rows_pixels && (W % tw) == 0) {
-    uint32_t tile = lin / (tw * th), in = lin % (tw * th);
-    uint32_t tx = tile % tiles_x, ty = tile / tiles_x;
-    return (ty * th + in / tw) * W + tx * tw + in % tw;
-  }
-  return lin;
-}
-
 template <bool kCount, int kBlock>
 __global__ void __launch_bounds__(kBlock) megakernel(SceneView S, LaunchParams L, float4* accum,
                                                    int* depth, int* status,

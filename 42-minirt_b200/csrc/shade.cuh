@@ -38,16 +38,30 @@ __device__ __forceinline__ float3 sky_texel(const SceneView& S, int x, int y) {
   return c;
 }
 
-// get_background_color[_clamp] (background.c:15-84).
-__device__ __forceinline__ float3 background(const SceneView& S, float3 d, bool clamp) {
-  if (!S.has_env) return f3(S.amb_const[0], S.amb_const[1], S.amb_const[2]);
+// Texel (x, y) of direction d: the spherical mapping of get_background_color
+// (background.c:15-70).
+__device__ __forceinline__ void sky_xy(const SceneView& S, float3 d, int& x, int& y) {
   d = unit(d);
   float v = 0.5f + asinf(fminf(fmaxf(d.y, -1.f), 1.f)) / (float)MRT_PI_D;
   float u = 0.5f - atan2f(d.z, d.x) / (float)(2.0 * MRT_PI_D);
-  int x = (int)(u * (S.env_w - 1)), y = (int)(v * (S.env_h - 1));
+  x = (int)(u * (S.env_w - 1));
+  y = (int)(v * (S.env_h - 1));
   x = min(max(x, 0), S.env_w - 1);
   y = min(max(y, 0), S.env_h - 1);
-  float3 c = sky_texel(S, x, y);
+}
+
+// get_background_color[_clamp] (background.c:15-84).
+__device__ __forceinline__ float3 background(const SceneView& S, float3 d, bool clamp) {
+  if (!S.has_env) return f3(S.amb_const[0], S.amb_const[1], S.amb_const[2]);
+  int x, y;
+  sky_xy(S, d, x, y);
+  float3 c;
+  if (S.sky_rgb) {
+    const float* t = S.sky_rgb + 3 * ((size_t)y * S.env_w + x);
+    c = f3(t[0], t[1], t[2]);
+  } else {
+    c = sky_texel(S, x, y);
+  }
   if (clamp) c = f3(fminf(fmaxf(c.x, 0.f), 16.f), fminf(fmaxf(c.y, 0.f), 16.f), fminf(fmaxf(c.z, 0.f), 16.f));
   return c;
 }

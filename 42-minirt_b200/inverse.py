@@ -1,0 +1,108 @@
+"""Inverse rendering over the differentiable entry points (mrt_forward /
+mrt_backward): a torch.autograd.Function wrapper and a projected Adam fit.
+
+The parameters are the float shadows of the reference's material and sky
+fields, in the layout of mrt_diff_layout:
+[albedo M*3 | roughness M | emission M | sky H*W*3]. Tensors stay on the
+context's GPU; the library reads and writes them through their device
+pointers, so a step costs one forward and one backward launch sequence.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+import mrt
+
+
+def _torch():
+    import torch
+    return torch
+
+
+class RenderFunction:
+    """torch.autograd.Function contract: apply(theta, ctx, spp, seed,
+    sample_base) -> image (H, W, 3); backward replays the same paths."""
+
+    _fn = None
+
+    @classmethod
+    def get(cls):
+        if cls._fn is None:
+            torch = _torch()
+
+            class _Render(torch.autograd.Function):
+                @staticmethod
+                def forward(fctx, theta, ctx, spp, seed, sample_base):
+                    theta = theta.detach().contiguous()
+                    img = torch.empty((ctx.height, ctx.width, 3), dtype=torch.float32, device=theta.device)
+                    ctx.forward(theta, spp=spp, seed=seed, sample_base=sample_base, out=img)
+                    fctx.save_for_backward(theta)
+                    fctx.render = (ctx, spp, seed, sample_base)
+                    return img
+
+                @staticmethod
+                def backward(fctx, grad_img):
+                    (theta,) = fctx.saved_tensors
+                    ctx, spp, seed, sample_base = fctx.render
+                    g = torch.empty_like(theta)
+                    ctx.backward(theta, grad_img.contiguous(), spp=spp, seed=seed,
+                                 sample_base=sample_base, out=g)
+                    return g, None, None, None, None
+
+            cls._fn = _Render
+        return cls._fn
+
+
+def render(theta, ctx: mrt.Context, spp: int, seed: int = 1, sample_base: int = 0):
+    """Differentiable render of theta (a float32 CUDA tensor)."""
+    return RenderFunction.get().apply(theta, ctx, spp, seed, sample_base)
+
+
+def bounds(layout: dict, device) -> tuple:
+    """Box the fit projects onto: albedo [0, 1], roughness [0.05, 1],
+    emission >= 0, sky >= 0."""
+    torch = _torch()
+    n = layout["total"]
+    lo = torch.zeros(n, device=device)
+    hi = torch.full((n,), float("inf"), device=device)
+    a, r = layout["albedo"], layout["roughness"]
+    hi[:a] = 1.0
+    lo[a:a + r] = 0.05
+    hi[a:a + r] = 1.0
+    return lo, hi
+
+
+def perturb(theta0: np.ndarray, layout: dict, rel: float, seed: int) -> np.ndarray:
+    """theta0 scaled by factors uniform in [1 - rel, 1 + rel] (seeded),
+    clipped to the box."""
+    rng = np.random.default_rng(seed)
+    t = theta0 * rng.uniform(1 - rel, 1 + rel, theta0.shape)
+    a, r = layout["albedo"], layout["roughness"]
+    t[:a] = np.clip(t[:a], 0, 1)
+    t[a:a + r] = np.clip(t[a:a + r], 0.05, 1)
+    return t.astype(np.float32)
+
+
+def fit(ctx: mrt.Context, theta_init, target, steps: int = 100, lr: float = 1e-2, spp: int = 64,
+        seed: int = 1000, callback=None):
+    """Projected Adam on the mean squared error between render(theta) and
+    target (an (H, W, 3) CUDA tensor); each step draws fresh samples
+    (sample_base = step * spp). Returns (theta, losses)."""
+    torch = _torch()
+    layout = ctx.diff_layout()
+    theta = torch.as_tensor(theta_init, dtype=torch.float32, device=target.device).clone().requires_grad_(True)
+    lo, hi = bounds(layout, target.device)
+    opt = torch.optim.Adam([theta], lr=lr)
+    losses = []
+    for step in range(steps):
+        opt.zero_grad(set_to_none=True)
+        img = render(theta, ctx, spp, seed, step * spp)
+        loss = torch.mean((img - target) ** 2)
+        loss.backward()
+        opt.step()
+        with torch.no_grad():
+            theta.copy_(torch.maximum(torch.minimum(theta, hi), lo))
+        losses.append(float(loss.detach()))
+        if callback:
+            callback(step, losses[-1])
+    return theta.detach(), losses

@@ -167,6 +167,10 @@ SIGNATURES = {
     "mrt_read_photons": (C.c_int, [_P, _P, _P, C.c_int64]),
     "mrt_set_photons": (C.c_int, [_P, _P, _P, C.c_int64]),
     "mrt_caustic_query": (C.c_int, [_P, _P, C.c_int64, C.c_int32, _P]),
+    "mrt_diff_layout": (C.c_int64, [_P, C.POINTER(C.c_int64)]),
+    "mrt_diff_get_params": (C.c_int, [_P, _P]),
+    "mrt_forward": (C.c_int, [_P, _P, C.POINTER(RenderParams), _P, C.POINTER(RenderStats)]),
+    "mrt_backward": (C.c_int, [_P, _P, C.POINTER(RenderParams), _P, _P, C.POINTER(RenderStats)]),
 }
 
 
@@ -220,6 +224,18 @@ def check(rc: int, what: str) -> None:
 
 def _ptr(a: np.ndarray | None):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _buf(a, what: str):
+    """Pointer of a contiguous float32 numpy array (host) or torch tensor
+    (host or this context's GPU): the differentiable entry points take both."""
+    if hasattr(a, "data_ptr"):
+        if str(a.dtype) != "torch.float32" or not a.is_contiguous():
+            raise MRTError(f"{what}: needs a contiguous float32 tensor")
+        return C.c_void_p(a.data_ptr())
+    if not (isinstance(a, np.ndarray) and a.dtype == np.float32 and a.flags.c_contiguous):
+        raise MRTError(f"{what}: needs a C-contiguous float32 array")
+    return _ptr(a)
 
 
 class Context:
@@ -357,3 +373,52 @@ class Context:
         check(self.lib.mrt_caustic_query(self.h, _ptr(pts), len(pts), k, _ptr(out)),
               "mrt_caustic_query")
         return out
+
+    # -------------------------------------------- differentiable rendering
+
+    def diff_layout(self) -> dict:
+        """Sizes of the theta blocks: albedo (M*3), roughness (M), emission
+        (M), sky (H*W*3), in that order."""
+        c = (C.c_int64 * 4)()
+        n = self.lib.mrt_diff_layout(self.h, c)
+        if n < 0:
+            check(int(n), "mrt_diff_layout")
+        return {"albedo": c[0], "roughness": c[1], "emission": c[2], "sky": c[3], "total": int(n)}
+
+    def diff_params(self) -> np.ndarray:
+        """theta of the scene as built."""
+        out = np.zeros(self.diff_layout()["total"], np.float32)
+        check(self.lib.mrt_diff_get_params(self.h, _ptr(out)), "mrt_diff_get_params")
+        return out
+
+    @staticmethod
+    def _diff_params(spp, seed, sample_base, max_bounces, jitter) -> RenderParams:
+        return RenderParams(spp=spp, sample_base=sample_base, seed=seed, max_bounces=max_bounces,
+                            jitter=jitter)
+
+    def forward(self, theta, spp: int, seed: int = 1, sample_base: int = 0, max_bounces: int = 0,
+                jitter: int = JITTER_SHARED, out=None, stats: bool = False):
+        """Image (H, W, 3) float32, the mean of `spp` samples, rendered with
+        parameters theta. `out` may be a float32 numpy array or torch tensor
+        (host or device) of H*W*3 elements."""
+        if out is None:
+            out = np.zeros((self.height, self.width, 3), np.float32)
+        st = RenderStats()
+        p = self._diff_params(spp, seed, sample_base, max_bounces, jitter)
+        check(self.lib.mrt_forward(self.h, _buf(theta, "theta"), C.byref(p), _buf(out, "image"),
+                                   C.byref(st)), "mrt_forward")
+        return (out, st) if stats else out
+
+    def backward(self, theta, grad_image, spp: int, seed: int = 1, sample_base: int = 0,
+                 max_bounces: int = 0, jitter: int = JITTER_SHARED, out=None, stats: bool = False):
+        """d loss / d theta for d loss / d image, replaying the forward's paths
+        (same theta, spp, seed, sample_base, max_bounces, jitter)."""
+        if out is None:
+            out = np.zeros(self.diff_layout()["total"], np.float32)
+        st = RenderStats()
+        p = self._diff_params(spp, seed, sample_base, max_bounces, jitter)
+        check(self.lib.mrt_backward(self.h, _buf(theta, "theta"), C.byref(p),
+                                    _buf(grad_image, "grad_image"), _buf(out, "grad_theta"),
+                                    C.byref(st)), "mrt_backward")
+        return (out, st) if stats else out
+

@@ -388,10 +388,39 @@ def make_c1(seed: int = 1, width: int = 1920, height: int = 1080, spp: int = 256
     return sc
 
 
-def make_c4(seed: int = 4, width: int = 512, height: int = 512, spp: int = 64, depth: int = 8) -> Scene:
-    sc = make_c1(seed, width, height, spp, depth, freq=100, n_materials=32, sky=(512, 256))
+def make_c4(seed: int = 4, width: int = 512, height: int = 512, spp: int = 64, depth: int = 8,
+            freq: int = 100, n_materials: int = 32, sky=(512, 256)) -> Scene:
+    """Inverse-rendering scene: the c1 generator at 20*freq^2 triangles
+    (200,000 at freq 100) with 32 materials and a 512x256 sky. Roughness is
+    drawn in [0.05, 1] for every material (metal and glass sample GGX
+    directions with it), and one material in eight emits (white, strength
+    0.5..2); the others carry a white emission colour at strength 0, so
+    that emission has a gradient everywhere. Values are float32-exact."""
+    sc = make_c1(seed, width, height, spp, depth, freq=freq, n_materials=n_materials, sky=sky)
     sc.name = "c4"
+    rng = np.random.default_rng(seed + 1000)
+    for i, m in enumerate(sc.materials):
+        m["roughness"] = float(np.float32(rng.uniform(0.05, 1.0)))
+        m["emission_color"] = (255, 255, 255)
+        m["emission_strength"] = float(np.float32(rng.uniform(0.5, 2.0))) if i % 8 == 0 else 0.0
     return sc
+
+
+def diff_theta(scene: Scene) -> np.ndarray:
+    """theta of mrt_forward for a scene, computed on the host: colours / 255,
+    roughness, emission strength and the linear sky radiance decoded from
+    its RGBE texels (float32, as the renderer decodes them)."""
+    mats = scene.materials
+    alb = np.array([np.asarray(m.get("color", (0, 0, 0)), np.float64) / 255.0 for m in mats]).reshape(-1)
+    rough = np.array([min(max(m.get("roughness", 0.0), 0.0), 1.0) for m in mats])
+    emis = np.array([m.get("emission_strength", 0.0) for m in mats])
+    parts = [alb.astype(np.float32), rough.astype(np.float32), emis.astype(np.float32)]
+    if scene.hdr is not None:
+        rgbe = np.asarray(scene.hdr, np.uint8).reshape(-1, 4)
+        scale = np.ldexp(np.float32(1.0), rgbe[:, 3].astype(np.int32) - 128).astype(np.float32)
+        sky = (rgbe[:, :3].astype(np.float32) * scale[:, None]) / np.float32(255.0)
+        parts.append(sky.astype(np.float32).reshape(-1))
+    return np.concatenate(parts).astype(np.float32)
 
 
 # ------------------------------------------------------------------ c2

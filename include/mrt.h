@@ -375,6 +375,42 @@ MRT_API int			mrt_set_photons(mrt_ctx *ctx, const double *pos3, const double *po
 MRT_API int			mrt_caustic_query(mrt_ctx *ctx, const double *points3, int64_t n,
 				int32_t k, double *rgb_out);
 
+/* ------------------------------------------------ differentiable rendering
+ * (no counterpart in the reference, which renders only; the parameters are
+ * float shadows of its fields.)
+ *
+ * theta, M materials and a W x H sky, as one float array:
+ *   [albedo M*3 (t_mat.color_value / 255) | roughness M (roughness_value) |
+ *    emission strength M (emission_strength) |
+ *    sky radiance H*W*3 (what get_hdr_pixel_skybox returns, get_hdr_value.c:43)]
+ * The sky block is empty without an HDR sky; a differentiable sky must be
+ * linear (hdr gamma 1).
+ *
+ * The pair follows the torch.autograd.Function contract: mrt_forward(theta)
+ * returns the image (W*H*3 floats, the mean over params->spp samples);
+ * mrt_backward(theta, dL/dimage) returns dL/dtheta for the same theta and
+ * the same params (seed, sample_base, spp, max_bounces, jitter: the
+ * backward replays exactly the forward's paths). Fields of params other
+ * than those five are ignored; max_bounces must be <= 16. Array
+ * arguments may be host memory or device memory of the context's GPU.
+ * The forward is the production renderer (persistent megakernel) over
+ * materials, sky and HDRI sampling tables rebuilt from theta; the backward
+ * is the path-replay adjoint: the derivative for fixed random numbers,
+ * which central differences with common random numbers converge to as the
+ * step shrinks. Discrete choices (hit primitive, branch, visibility,
+ * inverse-CDF and nearest-texel lookups) carry no gradient. */
+
+/* counts[0..3] = albedo, roughness, emission and sky entries; returns the
+ * total (>= 0) or a negative mrt_status. */
+MRT_API int64_t		mrt_diff_layout(mrt_ctx *ctx, int64_t counts[4]);
+/* theta of the scene as built (colours / 255, roughness, emission, sky). */
+MRT_API int			mrt_diff_get_params(mrt_ctx *ctx, float *theta);
+MRT_API int			mrt_forward(mrt_ctx *ctx, const float *theta,
+				const mrt_render_params *params, float *image, mrt_render_stats *stats);
+MRT_API int			mrt_backward(mrt_ctx *ctx, const float *theta,
+				const mrt_render_params *params, const float *grad_image,
+				float *grad_theta, mrt_render_stats *stats);
+
 # ifdef __cplusplus
 }
 # endif

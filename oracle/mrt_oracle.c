@@ -259,6 +259,11 @@ struct ro_scene
 	ro_counters	cnt;
 	int			render_mode;
 	int			apply_mesh_transform;
+	/* differentiable-parameter overrides (ro_set_params) */
+	double		*albedo_d;          /* M*3, replaces color_value / 255 */
+	double		*sky_d;             /* W*H*3 linear radiance, replaces the RGBE sky */
+	double		*pdf_joint_d;       /* pdf_joint before its float store */
+	int			exact;              /* FP64 throughout (no float intermediates) */
 };
 
 static int	g_apply_mesh_transform = 1;
@@ -564,11 +569,15 @@ static int hit_sphere(ro_scene *s, prim_t *sp, const ray_t *r, hrec_t *rec)
 
 /* hit_triangle (hit_triangle.c:68-93): Moller-Trumbore with the reference's
  * float intermediates (t_moller f/u/v/t are float, structs.h:99-110). */
+static int hit_triangle_exact(ro_scene *s, prim_t *tr, const ray_t *r, hrec_t *rec);
+
 static int hit_triangle(ro_scene *s, prim_t *tr, const ray_t *r, hrec_t *rec)
 {
 	v3		e1, e2, h, sv, q, n;
 	float	a, f, u, v, t, w;
 
+	if (s->exact)
+		return hit_triangle_exact(s, tr, r, rec);
 	s->cnt.tri_tests++;
 	e1 = vsub(tr->p[1], tr->p[0]);
 	e2 = vsub(tr->p[2], tr->p[0]);
@@ -609,6 +618,50 @@ static int hit_triangle(ro_scene *s, prim_t *tr, const ray_t *r, hrec_t *rec)
 		rec->front_face = 1;
 	rec->u = (1.0f - u - v) * tr->uv[0][0] + u * tr->uv[1][0] + v * tr->uv[2][0];
 	rec->v = (1.0f - u - v) * tr->uv[0][1] + u * tr->uv[1][1] + v * tr->uv[2][1];
+	return 1;
+}
+
+/* The same test with every intermediate in double (exact mode). */
+static int hit_triangle_exact(ro_scene *s, prim_t *tr, const ray_t *r, hrec_t *rec)
+{
+	v3		e1, e2, h, sv, q, n;
+	double	a, f, u, v, t, w;
+
+	s->cnt.tri_tests++;
+	e1 = vsub(tr->p[1], tr->p[0]);
+	e2 = vsub(tr->p[2], tr->p[0]);
+	h = vcross(r->dir, e2);
+	a = vdot(e1, h);
+	if (s->one_sided == 1 ? a < 1e-6 : fabs(a) < 1e-6)
+		return 0;
+	f = 1.0 / a;
+	sv = vsub(r->orig, tr->p[0]);
+	u = f * vdot(sv, h);
+	if (u < 0.0 || u > 1.0)
+		return 0;
+	q = vcross(sv, e1);
+	v = f * vdot(r->dir, q);
+	if (v < 0.0 || u + v > 1.0)
+		return 0;
+	t = f * vdot(e2, q);
+	if (t < IT_MIN || t > IT_MAX)
+		return 0;
+	rec->t = t;
+	rec->point = ray_at(*r, t);
+	w = 1.0 - u - v;
+	n.x = w * tr->n[0].x + u * tr->n[1].x + v * tr->n[2].x;
+	n.y = w * tr->n[0].y + u * tr->n[1].y + v * tr->n[2].y;
+	n.z = w * tr->n[0].z + u * tr->n[1].z + v * tr->n[2].z;
+	rec->normal = vunit(n);
+	if (!s->one_sided && vdot(r->dir, rec->normal) > 0.0)
+	{
+		rec->front_face = 0;
+		rec->normal = vscale(rec->normal, -1.0);
+	}
+	else
+		rec->front_face = 1;
+	rec->u = w * tr->uv[0][0] + u * tr->uv[1][0] + v * tr->uv[2][0];
+	rec->v = w * tr->uv[0][1] + u * tr->uv[1][1] + v * tr->uv[2][1];
 	return 1;
 }
 
@@ -738,6 +791,8 @@ static fc hit_color(ro_scene *s, hrec_t *h)
 {
 	if (s->render_mode == 2)
 		return (fc){(h->normal.x + 1) * 0.5, (h->normal.z + 1) * 0.5, (h->normal.y + 1) * 0.5};
+	if (h->mat >= 0 && s->albedo_d)
+		return (fc){s->albedo_d[3 * h->mat], s->albedo_d[3 * h->mat + 1], s->albedo_d[3 * h->mat + 2]};
 	if (h->mat >= 0)
 		return c2f(s->mats[h->mat].c8);
 	return c2f(h->objcolor);
@@ -804,6 +859,12 @@ static fc hdr_pixel_sky(ro_scene *s, int x, int y)
 	double			exposure = s->hdr_exposure + s->amb_ratio - 1;
 	double			scale, g;
 
+	if (s->sky_d)
+	{
+		const double	*t = s->sky_d + 3 * ((size_t)y * s->hw + x);
+
+		return (fc){t[0], t[1], t[2]};
+	}
 	if (exposure == 0)
 		scale = ldexp(1.0, px[3] - 128);
 	else
@@ -840,6 +901,9 @@ static double grey_value(ro_scene *s, size_t i)          /* calc_pdf.c:16 */
 	const uint8_t	*p = s->rgbe + 4 * i;
 	double			scale;
 
+	if (s->sky_d)   /* linear sky: grey of the 0..255-scaled radiance */
+		return 0.2126 * (s->sky_d[3 * i] * 255.0) + 0.7152 * (s->sky_d[3 * i + 1] * 255.0)
+			+ 0.0722 * (s->sky_d[3 * i + 2] * 255.0);
 	if (s->hdr_exposure == 0)
 		scale = ldexp(1.0, p[3] - 128);
 	else
@@ -858,7 +922,12 @@ static void build_env_tables(ro_scene *s)
 	double	*cw = calloc(W, sizeof(double));
 	double	sum;
 
+	free(s->pdf_joint);
+	free(s->pdf_joint_d);
+	free(s->cdf_m_inv);
+	free(s->cdf_c_inv);
 	s->pdf_joint = calloc((size_t)W * H, sizeof(float));
+	s->pdf_joint_d = calloc((size_t)W * H, sizeof(double));
 	s->cdf_m_inv = calloc(H, sizeof(float));
 	s->cdf_c_inv = calloc((size_t)W * H, sizeof(float));
 	for (size_t i = 0; i < (size_t)W * H; i++)
@@ -875,7 +944,10 @@ static void build_env_tables(ro_scene *s)
 		sum += raw[i];
 	s->column_average = sum / H;
 	for (int i = 0; i < H * W; i++)
+	{
 		s->pdf_joint[i] = gray[i] / (s->column_average);
+		s->pdf_joint_d[i] = gray[i] / (s->column_average);
+	}
 	for (int i = 0; i < H; i++)
 		pm[i] = raw[i] / (s->column_average / 255);
 	for (int i = 0; i < H; i++)
@@ -1199,7 +1271,10 @@ static void metallic(rng_t *rg, ro_scene *s, ray_t *r, hrec_t *h, fc *power)
 		: h->normal;
 
 	r->dir = vunit(vsub(r->dir, vscale(m, 2 * vdot(r->dir, m))));
-	*power = fmul(*power, fresnel_color(ct, h->color));
+	if (s->exact)
+		*power = fmul(*power, fadd(h->color, fscale(fsub((fc){1.0, 1.0, 1.0}, h->color), pow(1 - ct, 5))));
+	else
+		*power = fmul(*power, fresnel_color(ct, h->color));
 }
 
 /* reflected_dielectric_color (dielectric.c:15-33). */
@@ -1384,6 +1459,21 @@ static void env_nee(rng_t *rg, ro_scene *s, ray_t *r, hrec_t *h, fc *power, fc *
 	r->dir = (v3){cos(theta) * cos(phi), sin(theta), cos(theta) * sin(phi)};
 	if (shadow_any(s, r, &th))
 		return ;
+	if (s->exact)
+	{
+		double	ctd = vdot(h->normal, r->dir);
+		double	pdfd = s->pdf_joint_d[(int)(vy * (s->hh - 1) * s->hw + vx * (s->hw - 1))];
+
+		if (pdfd <= 0)
+			return ;
+		rad = background(s, *r, 0);
+		if (h->mat >= 0)
+			rad = fscale(rad, s->mats[h->mat].ao);
+		rad = fscale(fmul(rad, *power), ctd / pdfd);
+		*acc = fadd(*acc, rad);
+		*power = fscale(*power, 1 - ctd);
+		return ;
+	}
 	ct = vdot(h->normal, r->dir);
 	pdf = s->pdf_joint[(int)(vy * (s->hh - 1) * s->hw + vx * (s->hw - 1))];
 	if (pdf <= 0)
@@ -1890,6 +1980,9 @@ void	ro_destroy(ro_scene *s)
 	free(s->planes);
 	free(s->lights);
 	free(s->rgbe_own);
+	free(s->albedo_d);
+	free(s->sky_d);
+	free(s->pdf_joint_d);
 	free(s->pdf_joint);
 	free(s->cdf_m_inv);
 	free(s->cdf_c_inv);
@@ -2152,4 +2245,43 @@ int	ro_trace_path_events(ro_scene *s, uint64_t seed, int32_t pixel, int32_t samp
 	rc = ro_trace_path_counter(s, seed, pixel, sample, jitter, rgb);
 	g_events = NULL;
 	return rc;
+}
+
+/* ------------------------------------------ differentiable parameters */
+
+int64_t	ro_param_count(ro_scene *s)
+{
+	int64_t	sky = s->rgbe ? (int64_t)s->hw * s->hh * 3 : 0;
+
+	return (int64_t)s->n_mats * 5 + sky;
+}
+
+int	ro_set_params(ro_scene *s, const double *theta, int64_t n, int exact)
+{
+	int	m, M = s->n_mats;
+
+	if (n != ro_param_count(s))
+		return -1;
+	free(s->albedo_d);
+	s->albedo_d = malloc(sizeof(double) * 3 * (M ? M : 1));
+	for (m = 0; m < M; m++)
+	{
+		s->albedo_d[3 * m] = theta[3 * m];
+		s->albedo_d[3 * m + 1] = theta[3 * m + 1];
+		s->albedo_d[3 * m + 2] = theta[3 * m + 2];
+		s->mats[m].roughness = theta[3 * M + m];
+		s->mats[m].emission_strength = theta[4 * M + m];
+	}
+	if (s->rgbe)
+	{
+		size_t	t = (size_t)s->hw * s->hh * 3;
+
+		free(s->sky_d);
+		s->sky_d = malloc(sizeof(double) * t);
+		memcpy(s->sky_d, theta + 5 * M, sizeof(double) * t);
+		if (s->pdf_joint && s->hw >= 2 && s->hh >= 2)
+			build_env_tables(s);
+	}
+	s->exact = exact;
+	return 0;
 }

@@ -106,6 +106,16 @@ void		ro_set_mesh_transform(int on);
 /* Triangle corner positions as intersected, 9 doubles per flat triangle. */
 int			ro_triangle_positions(ro_scene *s, double *out);
 
+/* Differentiable parameters, the layout of mrt_forward's theta:
+ * [albedo M*3 | roughness M | emission M | sky W*H*3]. ro_set_params
+ * replaces the scene's values (colours by the doubles given, the RGBE sky by
+ * linear radiance, HDRI tables rebuilt from it); exact = 1 also keeps every
+ * intermediate in double (triangle t/u/v, NEE cosine and pdf, Fresnel), so
+ * that central differences with a tiny step give the FP64 reference
+ * gradient. Returns -1 if n does not match ro_param_count. */
+int64_t		ro_param_count(ro_scene *s);
+int			ro_set_params(ro_scene *s, const double *theta, int64_t n, int exact);
+
 /* Counter-based RNG shared with the CUDA kernels (PCG32, XSH-RR output). */
 uint64_t	ro_path_seed(uint64_t seed, uint32_t pixel, uint32_t sample);
 float		ro_pcg_float(uint64_t *state);

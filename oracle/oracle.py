@@ -274,6 +274,8 @@ def rst_lib():
             "ro_set_mesh_transform": (None, [C.c_int]),
             "ro_triangle_positions": (C.c_int, [_P, _P]),
             "ro_counters_read": (C.c_int, [_P, _P]),
+            "ro_param_count": (C.c_int64, [_P]),
+            "ro_set_params": (C.c_int, [_P, _P, C.c_int64, C.c_int]),
         }
         for k, (r, a) in sig.items():
             f = getattr(lib, k)
@@ -383,6 +385,38 @@ class Restatement:
         out = np.zeros((len(pts), 3))
         self.lib.ro_caustic_query(self.h, _ptr(pts), len(pts), k, _ptr(out))
         return out
+
+    def param_count(self) -> int:
+        return int(self.lib.ro_param_count(self.h))
+
+    def set_params(self, theta, exact: bool = True) -> None:
+        """Differentiable parameters in mrt_forward's layout (albedo, roughness,
+        emission, linear sky); exact keeps every intermediate in double."""
+        theta = np.ascontiguousarray(theta, np.float64)
+        if self.lib.ro_set_params(self.h, _ptr(theta), len(theta), int(exact)) != 0:
+            raise ValueError(f"theta has {len(theta)} entries, the scene {self.param_count()}")
+
+    def linear_functional(self, theta, weights, seed: int, spp: int, pix, sample_base: int = 0,
+                          jitter: int = 0, exact: bool = True) -> float:
+        """sum(weights * mean-over-spp radiance) over the pixels `pix`
+        (counter RNG, the GPU's paths)."""
+        self.set_params(theta, exact)
+        acc, _ = self.render_counter(seed, spp, sample_base, jitter, pix)
+        return float(np.sum(np.asarray(weights, np.float64) * acc / spp))
+
+    def fd_gradient(self, theta, directions, weights, seed: int, spp: int, pix, h: float = 1e-6,
+                    sample_base: int = 0, jitter: int = 0) -> np.ndarray:
+        """FP64 reference gradient of linear_functional along each direction
+        (rows of `directions`): central differences with common random
+        numbers in exact mode, step h."""
+        theta = np.asarray(theta, np.float64)
+        out = []
+        for v in np.atleast_2d(directions):
+            fp = self.linear_functional(theta + h * v, weights, seed, spp, pix, sample_base, jitter)
+            fm = self.linear_functional(theta - h * v, weights, seed, spp, pix, sample_base, jitter)
+            out.append((fp - fm) / (2 * h))
+        self.set_params(theta, True)
+        return np.array(out)
 
 
 def pcg_stream(seed: int, pixel: int, sample: int, n: int) -> np.ndarray:
