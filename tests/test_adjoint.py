@@ -13,8 +13,9 @@ References:
  * FD-CRN on the GPU: h = 1e-3, common random numbers, the L2 loss against a
    perturbed target, for the parameters that move no path (albedo, emission,
    single sky texels): within 1%.
-Forward: bit-identical to the production render without a sky; with a sky
-the HDRI tables are rebuilt from float radiance, within 1e-6 of it.
+Forward: the production render (to the rounding of its float atomic pixel
+sums) without a sky; with a sky the HDRI tables are rebuilt from float
+radiance, within 1e-6 of it.
 """
 from __future__ import annotations
 
@@ -109,7 +110,9 @@ def test_forward_is_the_render_without_sky(mrt, scenes, oracle):
     ctx.clear()
     ctx.render(4, seed=3, form=mrt.FORM_MEGAKERNEL)
     acc, _ = ctx.read_accum()
-    np.testing.assert_array_equal(img, acc / 4.0)
+    # the same kernel and paths; pixels sum their paths with float atomics,
+    # so the order of the additions (and the last bit) may differ
+    np.testing.assert_allclose(img, acc / 4.0, rtol=1e-5, atol=1e-6)
 
 
 @gpu
@@ -218,13 +221,19 @@ def test_adjoint_matches_fd_crn(c4ctx):
     g = ctx.backward(th, (2 * (im0 - target)).astype(np.float32), spp=spp, seed=seed)
     idx = list(range(3 * M)) + [4 * M + m for m in range(M) if th[4 * M + m] > 0]
     idx += list(5 * M + np.argsort(-np.abs(g[5 * M:]))[:4])
+    fd = []
     for i in idx:
         h = 1e-3
         tp, tm = th.astype(np.float64), th.astype(np.float64)
         tp[i] += h
         tm[i] -= h
-        f = (loss(tp) - loss(tm)) / (2 * h)
-        assert abs(g[i] - f) <= 1e-2 * abs(f) + 1e-3, (i, g[i], f)
+        fd.append((loss(tp) - loss(tm)) / (2 * h))
+    fd = np.array(fd)
+    ad = g[idx].astype(np.float64)
+    # 1% of each entry, plus the float32 rounding noise of the rendered images
+    # in a 1e-3 step (about 1e-5 of the largest entry)
+    tol = 1e-2 * np.abs(fd) + 1e-5 * np.abs(fd).max()
+    assert np.all(np.abs(ad - fd) <= tol), list(zip(idx, ad, fd))
 
 
 @gpu
@@ -236,9 +245,11 @@ def test_autograd_contract_on_device(c4ctx):
     w = np.random.default_rng(4).uniform(0.5, 1.5, (64, 64, 3)).astype(np.float32)
     t = torch.tensor(th, device="cuda", requires_grad=True)
     img = inverse.render(t, ctx, spp=4, seed=11)
-    np.testing.assert_array_equal(img.detach().cpu().numpy(), ctx.forward(th, spp=4, seed=11))
+    # paths add into the pixels with float atomics: sums agree to rounding
+    np.testing.assert_allclose(img.detach().cpu().numpy(), ctx.forward(th, spp=4, seed=11), rtol=1e-5, atol=1e-6)
     (img * torch.tensor(w, device="cuda")).sum().backward()
-    np.testing.assert_allclose(t.grad.cpu().numpy(), ctx.backward(th, w, spp=4, seed=11), rtol=1e-5, atol=1e-6)
+    # gradients are sums of float atomics too: equal to their rounding
+    np.testing.assert_allclose(t.grad.cpu().numpy(), ctx.backward(th, w, spp=4, seed=11), rtol=1e-4, atol=1e-5)
 
 
 @gpu
