@@ -90,6 +90,11 @@ inline float int_bits_as_float(int i) {
 
 }  // namespace
 
+namespace mrt {
+// Sets mrt_last_error's message for entry points defined in other files.
+int set_error_message(int code, const char* msg) { return set_err(code, "%s", msg); }
+}  // namespace mrt
+
 struct WfHost;
 WfHost* wf_create();
 void wf_destroy(WfHost* H);

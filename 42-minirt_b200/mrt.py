@@ -167,6 +167,7 @@ SIGNATURES = {
     "mrt_read_photons": (C.c_int, [_P, _P, _P, C.c_int64]),
     "mrt_set_photons": (C.c_int, [_P, _P, _P, C.c_int64]),
     "mrt_caustic_query": (C.c_int, [_P, _P, C.c_int64, C.c_int32, _P]),
+    "mrt_env_tables_noalloc": (C.c_int, [C.c_int, _P, C.c_int32, C.c_int32, C.c_float, _P, _P, _P, _P]),
     "mrt_diff_layout": (C.c_int64, [_P, C.POINTER(C.c_int64)]),
     "mrt_diff_get_params": (C.c_int, [_P, _P]),
     "mrt_forward": (C.c_int, [_P, _P, C.POINTER(RenderParams), _P, C.POINTER(RenderStats)]),

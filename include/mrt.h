@@ -375,6 +375,40 @@ MRT_API int			mrt_set_photons(mrt_ctx *ctx, const double *pos3, const double *po
 MRT_API int			mrt_caustic_query(mrt_ctx *ctx, const double *points3, int64_t n,
 				int32_t k, double *rgb_out);
 
+/* ------------------------------------- table build without allocation
+ * No counterpart in the reference. The HDRI importance-sampling tables that
+ * mrt_scene_build makes (importance_sampling_manager.c:41; read them back with
+ * mrt_read_env_tables), built into buffers the caller owns, for hosts that
+ * cannot allocate GPU memory when they need the tables: a host whose device
+ * memory all comes from its own pre-sized arena or pool, or a loop that must
+ * never reach the allocator. This call allocates nothing: no cudaMalloc, no
+ * cudaFree, no allocating library routine.
+ *
+ * rgbe: width*height texels of 4 bytes (r, g, b, e), device memory,
+ * 4-byte aligned;
+ * hdr_exposure as in mrt_ambient; outputs as for mrt_read_env_tables
+ * (pdf_joint W*H, cdf_marginal_inverse H, cdf_conditional_inverse W*H
+ * floats), device memory. stream is a cudaStream_t (NULL: the legacy default
+ * stream); the call returns once the tables are written. Runs on `device`,
+ * restoring the caller's current device afterwards.
+ *
+ * Limits: 2 <= width, 2 <= height <= MRT_ENV_NOALLOC_MAX_ROWS and
+ * width*height <= MRT_ENV_NOALLOC_MAX_TEXELS (512x512 or 1024x256);
+ * larger skies get MRT_ERR_INVALID with the limit in mrt_last_error(). The
+ * build's scratch (about 4 MiB of doubles) is a fixed array in the library
+ * that each GPU holds from the library's load until the process exits. The
+ * first call on a device looks up that array's device address (set-up done
+ * once per device); make that first call before any stream capture. All
+ * calls on a device share the array, so calls that overlap on the GPU (from
+ * several host threads or streams at once) race and must be serialised by
+ * the caller. Every scratch value a call reads it has written itself, so
+ * what an earlier call left there does not matter. */
+# define MRT_ENV_NOALLOC_MAX_TEXELS 262144
+# define MRT_ENV_NOALLOC_MAX_ROWS 4096
+MRT_API int			mrt_env_tables_noalloc(int device, const uint8_t *rgbe, int32_t width,
+				int32_t height, float hdr_exposure, float *pdf_joint,
+				float *cdf_marginal_inverse, float *cdf_conditional_inverse, void *stream);
+
 /* ------------------------------------------------ differentiable rendering
  * (no counterpart in the reference, which renders only; the parameters are
  * float shadows of its fields.)
