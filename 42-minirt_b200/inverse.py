@@ -21,7 +21,10 @@ def _torch():
 
 class RenderFunction:
     """torch.autograd.Function contract: apply(theta, ctx, spp, seed,
-    sample_base) -> image (H, W, 3); backward replays the same paths."""
+    sample_base, grad_sample_base) -> image (H, W, 3). The backward replays
+    the paths of samples [grad_sample_base, grad_sample_base + spp): the
+    forward's own paths when it equals sample_base, independent ones
+    otherwise (decorrelated gradients, see fit)."""
 
     _fn = None
 
@@ -32,12 +35,12 @@ class RenderFunction:
 
             class _Render(torch.autograd.Function):
                 @staticmethod
-                def forward(fctx, theta, ctx, spp, seed, sample_base):
+                def forward(fctx, theta, ctx, spp, seed, sample_base, grad_sample_base):
                     theta = theta.detach().contiguous()
                     img = torch.empty((ctx.height, ctx.width, 3), dtype=torch.float32, device=theta.device)
                     ctx.forward(theta, spp=spp, seed=seed, sample_base=sample_base, out=img)
                     fctx.save_for_backward(theta)
-                    fctx.render = (ctx, spp, seed, sample_base)
+                    fctx.render = (ctx, spp, seed, grad_sample_base)
                     return img
 
                 @staticmethod
@@ -47,15 +50,17 @@ class RenderFunction:
                     g = torch.empty_like(theta)
                     ctx.backward(theta, grad_img.contiguous(), spp=spp, seed=seed,
                                  sample_base=sample_base, out=g)
-                    return g, None, None, None, None
+                    return g, None, None, None, None, None
 
             cls._fn = _Render
         return cls._fn
 
 
-def render(theta, ctx: mrt.Context, spp: int, seed: int = 1, sample_base: int = 0):
+def render(theta, ctx: mrt.Context, spp: int, seed: int = 1, sample_base: int = 0,
+           grad_sample_base: int | None = None):
     """Differentiable render of theta (a float32 CUDA tensor)."""
-    return RenderFunction.get().apply(theta, ctx, spp, seed, sample_base)
+    gsb = sample_base if grad_sample_base is None else grad_sample_base
+    return RenderFunction.get().apply(theta, ctx, spp, seed, sample_base, gsb)
 
 
 def bounds(layout: dict, device) -> tuple:
@@ -84,10 +89,14 @@ def perturb(theta0: np.ndarray, layout: dict, rel: float, seed: int) -> np.ndarr
 
 
 def fit(ctx: mrt.Context, theta_init, target, steps: int = 100, lr: float = 1e-2, spp: int = 64,
-        seed: int = 1000, callback=None):
+        seed: int = 1000, decorrelate: bool = True, callback=None):
     """Projected Adam on the mean squared error between render(theta) and
-    target (an (H, W, 3) CUDA tensor); each step draws fresh samples
-    (sample_base = step * spp). Returns (theta, losses)."""
+    target (an (H, W, 3) CUDA tensor); each step draws fresh samples. With
+    decorrelate, the gradient replays samples independent of those of the
+    image that sets the residual: E[2 (I_a - T) dI_b] is the gradient of
+    |E I - T|^2, while the same samples on both sides add 2 Cov(I, dI),
+    which pulls the parameters towards less noisy images. Returns
+    (theta, losses)."""
     torch = _torch()
     layout = ctx.diff_layout()
     theta = torch.as_tensor(theta_init, dtype=torch.float32, device=target.device).clone().requires_grad_(True)
@@ -96,7 +105,8 @@ def fit(ctx: mrt.Context, theta_init, target, steps: int = 100, lr: float = 1e-2
     losses = []
     for step in range(steps):
         opt.zero_grad(set_to_none=True)
-        img = render(theta, ctx, spp, seed, step * spp)
+        base = 2 * step * spp
+        img = render(theta, ctx, spp, seed, base, base + spp if decorrelate else base)
         loss = torch.mean((img - target) ** 2)
         loss.backward()
         opt.step()

@@ -25,6 +25,12 @@ samples per pixel (16 steps = the 256 spp render).
               against the measured HBM copy bandwidth.
   cpu_baseline the reference's own CPU code (compiled from its sources) on
               this host's cores, timed in a separate process.
+  adjoint     the differentiable workload (512x512, 64 spp, depth 8,
+              200,000-triangle sphere, 32 materials, 512x256 sky):
+              device time of mrt_forward and mrt_backward (path-replay
+              adjoint) and their ratio, then 100 projected Adam steps
+              (lr 1e-2, 64 spp each) from the scene's parameters towards a
+              1024-spp target rendered at parameters perturbed by +-20%.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 Under torchrun each rank renders its own sample range (weak scaling); the
@@ -64,6 +70,11 @@ def parse():
     ap.add_argument("--ref-spp", type=int, default=1024)
     ap.add_argument("--cpu-seconds", type=float, default=8.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adam-steps", type=int, default=100)
+    ap.add_argument("--only-adjoint", action="store_true",
+                    help="run only the differentiable workload and print its figures (profiling aid)")
+    ap.add_argument("--adjoint-res", type=int, default=512)
     return ap.parse_args()
 
 
@@ -178,6 +189,54 @@ def convergence(ctx, sc, spp_step: int, ref_spp: int, forms: dict, fid: int) -> 
     return out
 
 
+def adjoint_bench(device: int, adam_steps: int, res: int = 512) -> dict:
+    """Forward / backward cost and an Adam fit on the differentiable workload."""
+    import mrt
+    import scenes
+    sc = scenes.make_c4(width=res, height=res)
+    ctx = mrt.Context(sc.width, sc.height, device=device)
+    ctx.build(sc)
+    th = ctx.diff_params()
+    spp = 64
+    w = np.random.default_rng(0).uniform(0.5, 1.5, (sc.height, sc.width, 3)).astype(np.float32)
+    fwd, bwd = [], []
+    for i in range(4):
+        _, sf = ctx.forward(th, spp=spp, seed=1 + i, stats=True)
+        _, sb = ctx.backward(th, w, spp=spp, seed=1 + i, stats=True)
+        if i:                                   # the first pair is warm-up
+            fwd.append(sf.ms)
+            bwd.append(sb.ms)
+    paths = sc.width * sc.height * spp
+    out = {"workload": f"c4: {res}x{res}, 64 spp, depth 8, 200,000-triangle displaced sphere, "
+                       "32 materials, 512x256 RGBE sky",
+           "forward_ms": statistics.median(fwd), "backward_ms": statistics.median(bwd),
+           "backward_over_forward": statistics.median(bwd) / statistics.median(fwd),
+           "forward_mpaths_s": paths / statistics.median(fwd) / 1e3,
+           "backward_mpaths_s": paths / statistics.median(bwd) / 1e3}
+    if adam_steps > 0:
+        try:
+            import torch
+            import inverse
+        except ImportError:
+            return out
+        lay = ctx.diff_layout()
+        target_theta = inverse.perturb(th, lay, 0.2, seed=4)
+        target = torch.tensor(ctx.forward(target_theta, spp=1024, seed=4242), device=f"cuda:{device}")
+        t0 = time.perf_counter()
+        fit, losses = inverse.fit(ctx, th, target, steps=adam_steps, lr=1e-2, spp=spp)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+        fit = fit.cpu().numpy()
+        nm = 5 * (lay["albedo"] // 3)
+        err0 = float(np.abs(th[:nm] - target_theta[:nm]).mean())
+        err1 = float(np.abs(fit[:nm] - target_theta[:nm]).mean())
+        out["adam"] = {"steps": adam_steps, "lr": 1e-2, "spp": spp, "loss_first": losses[0],
+                       "loss_last": float(np.mean(losses[-5:])), "wall_s": wall,
+                       "material_param_mae_start": err0, "material_param_mae_end": err1}
+    ctx.close()
+    return out
+
+
 def workload_config(a, sc) -> dict:
     return {"workload": f"{a.config}: 1920x1080, 256 spp, depth 12, 1,310,720-triangle displaced "
                         "geodesic sphere, 16 materials, 2048x1024 RGBE sky with importance sampling"
@@ -191,6 +250,9 @@ def main() -> int:
     a = parse()
     if a.impl == "reference":
         run_reference_arm(a)
+        return 0
+    if a.only_adjoint:
+        print(json.dumps({"adjoint": adjoint_bench(0, a.adam_steps, a.adjoint_res)}), flush=True)
         return 0
     import distributed as D
     import mrt
@@ -302,6 +364,9 @@ def main() -> int:
     relmse = None
     if not a.no_relmse and world == 1:
         relmse = convergence(ctx, sc, spp, a.ref_spp, forms, form_ids[best])
+    adjoint = None
+    if not a.no_adjoint and world == 1:
+        adjoint = adjoint_bench(local, a.adam_steps)
 
     f = forms[best]
     achieved = bpp * (paths_per_step / max(f["launches"] / a.steps, 1)) / (f["launch_ms"] / 1000.0) / 1e9
@@ -326,6 +391,8 @@ def main() -> int:
     }
     if relmse is not None:
         line["relmse"] = relmse
+    if adjoint is not None:
+        line["adjoint"] = adjoint
     if cpu is not None:
         line["cpu_baseline"] = {"value": cpu["mpaths_s"], "unit": UNIT, "cores": cpu["procs"],
                                 "kind": "reference", "sample": cpu["sample"]}
