@@ -155,6 +155,7 @@ struct mrt_ctx {
   uint64_t photons_per_light = 0;
   int64_t n_photons = 0;
   mrt_caustic caustic{};
+  int photon_pass = 0;                   // progressive mode: pass of the current photon map
   SceneView view{};
   size_t scene_bytes = 0;
   int bvh_depth = 0;
@@ -753,6 +754,10 @@ extern "C" int mrt_scene_build(mrt_ctx* c, const mrt_scene_desc* d) {
     c->view.inv_norm = (float)(1.0 / d->caustic.norm_factor);
     c->view.caustic_mode = d->caustic.mode;
     c->view.fixed_radius2 = (float)d->caustic.radius;
+    if (d->caustic.mode == 1 && d->caustic.passes > 1 &&
+        (d->caustic.spp_per_pass < 0 || !(d->caustic.shrink > 0.0 && d->caustic.shrink <= 1.0)))
+      return set_err(MRT_ERR_INVALID, "progressive caustics need spp_per_pass >= 0 and shrink in (0, 1]");
+    c->photon_pass = 0;
     int rc2 = emit_photons(c, 0, d->caustic.radius);
     if (rc2) return rc2;
   }
@@ -777,6 +782,27 @@ extern "C" int mrt_set_camera(mrt_ctx* c, const mrt_camera* cam, double ior_all,
 
 // ---------------------------------------------------------------- render
 
+// Progressive photon mapping (caustic mode 1, the configuration's extension
+// of the reference's single kNN pass): sample s renders with photon pass
+// min(s / spp_per_pass, passes - 1); pass q is emitted from its own streams
+// and gathered within radius * shrink^(2q) (radius is compared against
+// squared distances, so the gather radius shrinks by `shrink` per pass).
+static int pass_of(const mrt_ctx* c, int64_t sample) {
+  const mrt_caustic& k = c->caustic;
+  if (!k.enable || k.mode != 1 || k.passes <= 1 || k.spp_per_pass <= 0) return 0;
+  return (int)std::min<int64_t>(sample / k.spp_per_pass, k.passes - 1);
+}
+
+static int ensure_photon_pass(mrt_ctx* c, int q) {
+  if (q == c->photon_pass) return MRT_OK;
+  const double r2 = c->caustic.radius * std::pow(c->caustic.shrink, 2.0 * q);
+  c->view.fixed_radius2 = (float)r2;
+  const int rc = emit_photons(c, (uint32_t)q, r2);
+  if (rc) return rc;
+  c->photon_pass = q;
+  return MRT_OK;
+}
+
 static int read_status(mrt_ctx* c, int* out) {
   int s = 0;
   CK(cudaMemcpyAsync(&s, c->status.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -798,6 +824,38 @@ extern "C" int mrt_render(mrt_ctx* c, const mrt_render_params* p, mrt_render_sta
   if (p->block_size && (p->block_size % 32 || p->block_size > 256))
     return set_err(MRT_ERR_INVALID, "block_size %d", p->block_size);
   if (p->env_sampler < 0 || p->env_sampler > 1) return set_err(MRT_ERR_INVALID, "env_sampler %d", p->env_sampler);
+  if (p->render_mode == 0 && p->spp > 0 && pass_of(c, (int64_t)p->sample_base + p->spp - 1) > 0) {
+    const int q0 = pass_of(c, p->sample_base), q1 = pass_of(c, (int64_t)p->sample_base + p->spp - 1);
+    if (q0 != q1) {   // one call per photon pass
+      mrt_render_stats total{};
+      int64_t s = p->sample_base;
+      const int64_t end = (int64_t)p->sample_base + p->spp;
+      while (s < end) {
+        const int q = pass_of(c, s);
+        const int64_t seg_end = q == c->caustic.passes - 1
+                                    ? end : std::min<int64_t>(end, (int64_t)(q + 1) * c->caustic.spp_per_pass);
+        mrt_render_params sub = *p;
+        sub.sample_base = (int32_t)s;
+        sub.spp = (int32_t)(seg_end - s);
+        mrt_render_stats st{};
+        rc = mrt_render(c, &sub, &st);
+        if (rc) return rc;
+        total.ms += st.ms;
+        total.paths += st.paths;
+        total.segments += st.segments;
+        total.shadow_rays += st.shadow_rays;
+        total.kernel_launches += st.kernel_launches;
+        total.status |= st.status;
+        s = seg_end;
+      }
+      if (stats) *stats = total;
+      return MRT_OK;
+    }
+  }
+  if (p->render_mode == 0 && p->spp > 0) {
+    rc = ensure_photon_pass(c, pass_of(c, p->sample_base));
+    if (rc) return rc;
+  }
   SceneView v = c->view;
   v.env_lookup = p->env_sampler;
   const uint64_t npix = (uint64_t)c->W * c->H;

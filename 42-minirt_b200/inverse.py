@@ -21,10 +21,10 @@ def _torch():
 
 class RenderFunction:
     """torch.autograd.Function contract: apply(theta, ctx, spp, seed,
-    sample_base, grad_sample_base) -> image (H, W, 3). The backward replays
-    the paths of samples [grad_sample_base, grad_sample_base + spp): the
-    forward's own paths when it equals sample_base, independent ones
-    otherwise (decorrelated gradients, see fit)."""
+    sample_base, grad_sample_base, grad_spp) -> image (H, W, 3). The backward
+    replays the paths of samples [grad_sample_base, grad_sample_base +
+    grad_spp): the forward's own paths when both equal the forward's,
+    independent ones otherwise (decorrelated gradients, see fit)."""
 
     _fn = None
 
@@ -35,12 +35,12 @@ class RenderFunction:
 
             class _Render(torch.autograd.Function):
                 @staticmethod
-                def forward(fctx, theta, ctx, spp, seed, sample_base, grad_sample_base):
+                def forward(fctx, theta, ctx, spp, seed, sample_base, grad_sample_base, grad_spp):
                     theta = theta.detach().contiguous()
                     img = torch.empty((ctx.height, ctx.width, 3), dtype=torch.float32, device=theta.device)
                     ctx.forward(theta, spp=spp, seed=seed, sample_base=sample_base, out=img)
                     fctx.save_for_backward(theta)
-                    fctx.render = (ctx, spp, seed, grad_sample_base)
+                    fctx.render = (ctx, grad_spp, seed, grad_sample_base)
                     return img
 
                 @staticmethod
@@ -50,29 +50,30 @@ class RenderFunction:
                     g = torch.empty_like(theta)
                     ctx.backward(theta, grad_img.contiguous(), spp=spp, seed=seed,
                                  sample_base=sample_base, out=g)
-                    return g, None, None, None, None, None
+                    return g, None, None, None, None, None, None
 
             cls._fn = _Render
         return cls._fn
 
 
 def render(theta, ctx: mrt.Context, spp: int, seed: int = 1, sample_base: int = 0,
-           grad_sample_base: int | None = None):
-    """Differentiable render of theta (a float32 CUDA tensor)."""
+           grad_sample_base: int | None = None, grad_spp: int | None = None):
+    """Differentiable render of theta (a float32 CUDA tensor). The backward
+    replays grad_spp samples from grad_sample_base (default: the forward's)."""
     gsb = sample_base if grad_sample_base is None else grad_sample_base
-    return RenderFunction.get().apply(theta, ctx, spp, seed, sample_base, gsb)
+    gspp = spp if grad_spp is None else grad_spp
+    return RenderFunction.get().apply(theta, ctx, spp, seed, sample_base, gsb, gspp)
 
 
 def bounds(layout: dict, device) -> tuple:
-    """Box the fit projects onto: albedo [0, 1], roughness [0.05, 1],
-    emission >= 0, sky >= 0."""
+    """Box the fit projects onto: albedo [0, 1], roughness [0, 1] (the
+    reference clamps both to that range), emission >= 0, sky >= 0."""
     torch = _torch()
     n = layout["total"]
     lo = torch.zeros(n, device=device)
     hi = torch.full((n,), float("inf"), device=device)
     a, r = layout["albedo"], layout["roughness"]
     hi[:a] = 1.0
-    lo[a:a + r] = 0.05
     hi[a:a + r] = 1.0
     return lo, hi
 
@@ -89,29 +90,42 @@ def perturb(theta0: np.ndarray, layout: dict, rel: float, seed: int) -> np.ndarr
 
 
 def fit(ctx: mrt.Context, theta_init, target, steps: int = 100, lr: float = 1e-2, spp: int = 64,
-        seed: int = 1000, decorrelate: bool = True, callback=None):
+        seed: int = 1000, decorrelate: bool = True, mask=None, residual_spp: int | None = None,
+        lr_decay: bool = False, callback=None):
     """Projected Adam on the mean squared error between render(theta) and
     target (an (H, W, 3) CUDA tensor); each step draws fresh samples. With
     decorrelate, the gradient replays samples independent of those of the
     image that sets the residual: E[2 (I_a - T) dI_b] is the gradient of
     |E I - T|^2, while the same samples on both sides add 2 Cov(I, dI),
-    which pulls the parameters towards less noisy images. Returns
-    (theta, losses)."""
+    which pulls the parameters towards less noisy images. mask (0/1 per
+    entry of theta) restricts the fit to a subset. residual_spp (decorrelated
+    only) renders the image that sets the residual with more samples than
+    the gradient replays (a forward costs about half a backward); lr_decay
+    anneals the rate along a cosine to 1% of lr. Returns (theta, losses)."""
     torch = _torch()
     layout = ctx.diff_layout()
     theta = torch.as_tensor(theta_init, dtype=torch.float32, device=target.device).clone().requires_grad_(True)
     lo, hi = bounds(layout, target.device)
     opt = torch.optim.Adam([theta], lr=lr)
+    keep = None if mask is None else torch.as_tensor(mask, dtype=torch.float32, device=target.device)
     losses = []
+    rspp = spp if (residual_spp is None or not decorrelate) else residual_spp
+    stride = rspp + spp
     for step in range(steps):
+        if lr_decay:
+            for grp in opt.param_groups:
+                grp["lr"] = lr * (0.01 + 0.99 * 0.5 * (1 + np.cos(np.pi * step / max(steps - 1, 1))))
         opt.zero_grad(set_to_none=True)
-        base = 2 * step * spp
-        img = render(theta, ctx, spp, seed, base, base + spp if decorrelate else base)
+        base = step * stride
+        img = render(theta, ctx, rspp, seed, base, base + rspp if decorrelate else base, spp)
         loss = torch.mean((img - target) ** 2)
         loss.backward()
+        if keep is not None:
+            theta.grad.mul_(keep)
         opt.step()
         with torch.no_grad():
-            theta.copy_(torch.maximum(torch.minimum(theta, hi), lo))
+            boxed = torch.maximum(torch.minimum(theta, hi), lo)
+            theta.copy_(boxed if keep is None else torch.where(keep > 0, boxed, theta))
         losses.append(float(loss.detach()))
         if callback:
             callback(step, losses[-1])

@@ -20,7 +20,7 @@ HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "libmrt.so"
 MINIRT_LIB_PATH = HERE / "libmrt_minirt.so"
 
-MRT_ABI_VERSION = 1
+MRT_ABI_VERSION = 2
 
 MRT_OK = 0
 STATUS_NAMES = {
@@ -85,7 +85,8 @@ class Caustic(C.Structure):
     _fields_ = [("enable", C.c_int32), ("passes", C.c_int32),
                 ("photons_per_light", C.c_uint64), ("radius", C.c_double),
                 ("norm_factor", C.c_double), ("shrink", C.c_double),
-                ("knn", C.c_int32), ("mode", C.c_int32)]
+                ("knn", C.c_int32), ("mode", C.c_int32), ("spp_per_pass", C.c_int32),
+                ("pad_", C.c_int32)]
 
 
 class SceneDesc(C.Structure):

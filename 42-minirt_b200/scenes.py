@@ -113,6 +113,7 @@ class Scene:
             d.caustic.shrink = c.get("shrink", 0.9)
             d.caustic.knn = c.get("k", 15)
             d.caustic.mode = c.get("mode", 0)
+            d.caustic.spp_per_pass = c.get("spp_per_pass", 0)
         mats = (mrt.Material * max(1, len(self.materials)))()
         for i, m in enumerate(self.materials):
             mats[i].color[:] = m["color"]
@@ -453,7 +454,8 @@ def heightfield(n: int, size: float, y0: float, seed: int, amplitude: float = 0.
 
 
 def make_c2(seed: int = 2, width: int = 1280, height: int = 720, spp: int = 128, depth: int = 10,
-            grid: int = 512, photons: int = 2_000_000, passes: int = 1, mode: int = 0) -> Scene:
+            grid: int = 512, photons: int = 2_000_000, passes: int = 1, mode: int = 0,
+            spp_per_pass: int = 0) -> Scene:
     pos = (0.0, 3.2, 6.5)
     sc = Scene("c2", width, height, spp, depth,
                camera=dict(position=pos, orientation=look_at(pos, (0, 0.6, 0)), fov=60), seed=seed)
@@ -468,7 +470,7 @@ def make_c2(seed: int = 2, width: int = 1280, height: int = 720, spp: int = 128,
                           color=(255, 255, 255)))
     sc.ambient_ratio, sc.ambient_color = 0.0, (0, 0, 0)
     sc.caustic = dict(photons=photons, radius=0.02, norm=1.0, k=15, passes=passes,
-                      shrink=0.9, mode=mode)
+                      shrink=0.9, mode=mode, spp_per_pass=spp_per_pass)
     return sc
 
 
@@ -507,4 +509,12 @@ def make_c3_scene(spec: dict, sky_cache: dict | None = None) -> Scene:
     return sc
 
 
-CONFIGS = {"c0": make_c0, "c1": make_c1, "c2": make_c2, "c4": make_c4}
+def make_c2_progressive(**kw) -> Scene:
+    """c2's extension mode: 16 photon passes of 2 M photons, 8 spp each
+    (128 spp), fixed-radius gather shrinking by 0.9 per pass."""
+    sc = make_c2(passes=16, mode=1, spp_per_pass=8, **kw)
+    sc.name = "c2p"
+    return sc
+
+
+CONFIGS = {"c0": make_c0, "c1": make_c1, "c2": make_c2, "c2p": make_c2_progressive, "c4": make_c4}

@@ -36,7 +36,7 @@
 extern "C" {
 # endif
 
-# define MRT_ABI_VERSION 1
+# define MRT_ABI_VERSION 2
 
 # if defined(__GNUC__)
 #  define MRT_API __attribute__((visibility("default")))
@@ -174,6 +174,12 @@ typedef struct mrt_caustic
 	double		shrink;          /* progressive mode radius factor per pass */
 	int32_t		knn;             /* k nearest (reference: 15, material_default.c:81) */
 	int32_t		mode;            /* 0 = kNN parity mode, 1 = fixed-radius progressive */
+	int32_t		spp_per_pass;    /* progressive mode (mode 1, passes > 1): sample s uses
+	                              * photon pass min(s / spp_per_pass, passes - 1), emitted
+	                              * from its own streams, gathered within radius
+	                              * radius * shrink^(2 pass) (radius is compared against
+	                              * squared distances); 0 = one pass */
+	int32_t		pad_;
 }	mrt_caustic;
 
 typedef struct mrt_scene_desc

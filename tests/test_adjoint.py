@@ -265,13 +265,31 @@ def test_invalid_arguments(c4ctx, mrt):
 
 
 @gpu
-def test_adam_fit_reduces_the_loss(c4ctx):
+def test_adam_fit_recovers_albedo(mrt, scenes, oracle):
+    """100 projected Adam steps (lr 1e-2; gradients of 32 spp decorrelated
+    from a 128-spp residual) on the albedos alone move a +-20% albedo
+    perturbation of the materials the camera sees towards the target (c0
+    scene: spheres under an emissive sphere light). Each step's gradient has
+    a signal-to-noise ratio of 0.1-0.5 per entry, which bounds the recovery."""
     torch = pytest.importorskip("torch")
     import inverse
-    sc, ctx = c4ctx
+    sc = scenes.make_c0(width=96, height=72, spp=16, depth=8)
+    ctx = mrt.Context(96, 72)
+    ctx.build(oracle.canonical_scene(sc))
     th = ctx.diff_params()
-    lay = ctx.diff_layout()
-    target_theta = inverse.perturb(th, lay, 0.2, seed=7)
-    target = torch.tensor(ctx.forward(target_theta, spp=256, seed=77), device="cuda")
-    _, losses = inverse.fit(ctx, th, target, steps=100, lr=1e-2, spp=8)
-    assert np.mean(losses[-10:]) < 0.5 * np.mean(losses[:3])
+    M = len(sc.materials)
+    rng = np.random.default_rng(7)
+    target_theta = th.copy()
+    target_theta[:3 * M] = np.clip(th[:3 * M] * rng.uniform(0.8, 1.2, 3 * M), 0, 1)
+    target = ctx.forward(target_theta, spp=512, seed=77)
+    mask = np.zeros_like(th)
+    mask[:3 * M] = 1
+    fit, _ = inverse.fit(ctx, th, torch.tensor(target, device="cuda"), steps=100, lr=1e-2, spp=32,
+                         residual_spp=128, mask=mask)
+    fit = fit.cpu().numpy()
+    assert np.array_equal(fit[3 * M:], th[3 * M:])
+    g0 = ctx.backward(th, np.ones((72, 96, 3), np.float32), spp=16)
+    seen = np.abs(g0[:3 * M]) > 1e-2 * np.abs(g0[:3 * M]).max()
+    err0 = np.abs(th[:3 * M] - target_theta[:3 * M])[seen].mean()
+    err1 = np.abs(fit[:3 * M] - target_theta[:3 * M])[seen].mean()
+    assert err1 < 0.7 * err0, (err0, err1)
