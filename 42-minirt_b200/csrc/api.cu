@@ -150,7 +150,7 @@ struct mrt_ctx {
   DevBuf<float2> alias;
   DevBuf<float4> env_rec0, env_rec1;
   DevBuf<float4> ph_pos, ph_pow, ph_pos_raw, ph_pow_raw;
-  DevBuf<uint32_t> cell_start, cell_of;
+  DevBuf<float4> ph_nodes;
   DevBuf<unsigned int> ph_count;
   uint64_t photons_per_light = 0;
   int64_t n_photons = 0;
@@ -363,7 +363,7 @@ void mrt_destroy(mrt_ctx* c) {
   c->rgbe.release(); c->pdf_joint.release(); c->cdf_m.release(); c->cdf_c.release();
   c->alias.release(); c->env_rec0.release(); c->env_rec1.release();
   c->ph_pos.release(); c->ph_pow.release(); c->ph_pos_raw.release(); c->ph_pow_raw.release();
-  c->cell_start.release(); c->cell_of.release(); c->ph_count.release();
+  c->ph_nodes.release(); c->ph_count.release();
   wf_destroy(c->wf);
   if (c->diff) { c->diff->release(); delete c->diff; }
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -376,65 +376,31 @@ void mrt_destroy(mrt_ctx* c) {
 
 // ------------------------------------------------------- photon map build
 
-static int build_grid(mrt_ctx* c, double radius2) {
+// Photon map over the emitted photons: Morton order + linear BVH.
+static int build_photon_map(mrt_ctx* c) {
   SceneView& v = c->view;
   const uint32_t n = (uint32_t)c->n_photons;
-  std::vector<float4> pos(n);
-  if (n) {
-    CK(cudaMemcpyAsync(pos.data(), c->ph_pos_raw.p, sizeof(float4) * n, cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-  }
-  float mn[3] = {0, 0, 0}, mx[3] = {0, 0, 0};
-  for (uint32_t i = 0; i < n; ++i) {
-    const float p[3] = {pos[i].x, pos[i].y, pos[i].z};
-    for (int k = 0; k < 3; ++k) {
-      if (i == 0 || p[k] < mn[k]) mn[k] = p[k];
-      if (i == 0 || p[k] > mx[k]) mx[k] = p[k];
-    }
-  }
-  double r = std::sqrt(std::max(radius2, 1e-12));
-  double ext = std::max({(double)mx[0] - mn[0], (double)mx[1] - mn[1], (double)mx[2] - mn[2], 1e-6});
-  double cell = std::max(r, ext / 1024.0) * 1.0001;
-  int dim[3];
-  for (;;) {
-    uint64_t tot = 1;
-    for (int k = 0; k < 3; ++k) {
-      dim[k] = std::max(1, (int)std::ceil(((double)mx[k] - mn[k]) / cell) + 1);
-      tot *= (uint64_t)dim[k];
-    }
-    if (tot <= (1u << 24)) break;
-    cell *= 1.25;
-  }
-  const uint32_t n_cells = (uint32_t)((uint64_t)dim[0] * dim[1] * dim[2]);
-  CK(c->cell_start.alloc((size_t)n_cells + 1));
-  CK(c->cell_of.alloc(std::max<size_t>(n, 1)));
   CK(c->ph_pos.alloc(std::max<size_t>(n, 1)));
   CK(c->ph_pow.alloc(std::max<size_t>(n, 1)));
-  GridBuild G{};
-  G.pos_in = c->ph_pos_raw.p;
-  G.pow_in = c->ph_pow_raw.p;
-  G.n = n;
-  G.pos_out = c->ph_pos.p;
-  G.pow_out = c->ph_pow.p;
-  G.cell_of = c->cell_of.p;
-  G.cell_start = c->cell_start.p;
-  G.n_cells = n_cells;
-  for (int k = 0; k < 3; ++k) { G.grid_min[k] = mn[k]; G.dim[k] = dim[k]; }
-  G.inv_cell = (float)(1.0 / cell);
-  CK(launch_grid_build(G, c->stream));
+  CK(c->ph_nodes.alloc(4 * std::max<size_t>(n > 1 ? n - 1 : 1, 1)));
+  PhotonTree T{};
+  T.pos_in = c->ph_pos_raw.p;
+  T.pow_in = c->ph_pow_raw.p;
+  T.n = n;
+  T.pos_out = c->ph_pos.p;
+  T.pow_out = c->ph_pow.p;
+  T.nodes = c->ph_nodes.p;
+  CK(launch_photon_tree(T, c->stream));
   CK(cudaStreamSynchronize(c->stream));
-  for (int k = 0; k < 3; ++k) { v.grid_min[k] = mn[k]; v.grid_dim[k] = dim[k]; }
-  v.grid_inv_cell = (float)(1.0 / cell);
-  v.grid_cell = (float)cell;
   v.photon_pos = c->ph_pos.p;
   v.photon_pow = c->ph_pow.p;
-  v.cell_start = c->cell_start.p;
+  v.photon_nodes = c->ph_nodes.p;
   v.n_photons = (int)n;
   return MRT_OK;
 }
 
-// Emits the photons of `pass` and rebuilds the grid (caustic_manager.c:83).
-static int emit_photons(mrt_ctx* c, uint32_t pass, double radius2) {
+// Emits the photons of `pass` and rebuilds the photon map (caustic_manager.c:83).
+static int emit_photons(mrt_ctx* c, uint32_t pass) {
   SceneView& v = c->view;
   const uint64_t cap = c->photons_per_light * (uint64_t)c->n_point_lights;
   v.caustic = 0;   // emission traces without gathering
@@ -464,7 +430,7 @@ static int emit_photons(mrt_ctx* c, uint32_t pass, double radius2) {
   CK(cudaMemcpyAsync(&cnt, c->ph_count.p, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->n_photons = std::min<uint64_t>(cnt, cap);
-  int rc = build_grid(c, radius2);
+  int rc = build_photon_map(c);
   if (rc != MRT_OK) return rc;
   v.caustic = 1;
   return MRT_OK;
@@ -758,14 +724,14 @@ extern "C" int mrt_scene_build(mrt_ctx* c, const mrt_scene_desc* d) {
         (d->caustic.spp_per_pass < 0 || !(d->caustic.shrink > 0.0 && d->caustic.shrink <= 1.0)))
       return set_err(MRT_ERR_INVALID, "progressive caustics need spp_per_pass >= 0 and shrink in (0, 1]");
     c->photon_pass = 0;
-    int rc2 = emit_photons(c, 0, d->caustic.radius);
+    int rc2 = emit_photons(c, 0);
     if (rc2) return rc2;
   }
   CK(cudaStreamSynchronize(st));
   c->scene_bytes = c->nodes.bytes() + c->geom.bytes() + c->meta.bytes() + c->shade.bytes() +
                    c->planes.bytes() + c->mats.bytes() + c->lights.bytes() + c->rgbe.bytes() +
                    c->pdf_joint.bytes() + c->cdf_m.bytes() + c->cdf_c.bytes() + c->alias.bytes() +
-                   c->env_rec0.bytes() + c->env_rec1.bytes() + c->ph_pos.bytes() + c->ph_pow.bytes() + c->cell_start.bytes();
+                   c->env_rec0.bytes() + c->env_rec1.bytes() + c->ph_pos.bytes() + c->ph_pow.bytes() + c->ph_nodes.bytes();
   c->has_scene = true;
   return MRT_OK;
 }
@@ -797,7 +763,7 @@ static int ensure_photon_pass(mrt_ctx* c, int q) {
   if (q == c->photon_pass) return MRT_OK;
   const double r2 = c->caustic.radius * std::pow(c->caustic.shrink, 2.0 * q);
   c->view.fixed_radius2 = (float)r2;
-  const int rc = emit_photons(c, (uint32_t)q, r2);
+  const int rc = emit_photons(c, (uint32_t)q);
   if (rc) return rc;
   c->photon_pass = q;
   return MRT_OK;
@@ -1220,7 +1186,7 @@ extern "C" int mrt_set_photons(mrt_ctx* c, const double* pos3, const double* pow
   CK(c->ph_pos_raw.upload(a.data(), a.size(), c->stream));
   CK(c->ph_pow_raw.upload(b.data(), b.size(), c->stream));
   c->n_photons = n;
-  rc = build_grid(c, c->caustic.radius);
+  rc = build_photon_map(c);
   if (rc) return rc;
   c->view.caustic = 1;
   return MRT_OK;

@@ -1,21 +1,38 @@
-// caustic.cuh — photon-map radiance estimate on a uniform hash grid.
+// caustic.cuh — photon-map radiance estimate over the photon hierarchy.
 //
 // Reference: estimate_caustics_physically_based + calculate_caustic_radiance
 // (get_caustic.c:37-88) over a median kd-tree (kd_tree_find_near.c:93). The
 // estimate is non-zero only when the k-th nearest photon lies within
 // r_max^2 = caustic_radius (the option value is compared against squared
-// distances, get_caustic.c:45), so only photons inside r_max matter: the grid
-// has cells of side >= r_max and the 27 cells around the query hold every
-// candidate. The k nearest are kept in a register-resident sorted list.
+// distances, get_caustic.c:45), so only photons inside r_max matter.
+//
+// The photons are in Morton order with a linear BVH over them
+// (SceneView.photon_nodes). The kNN walk visits the nearer child first and
+// skips every node farther than the current k-th distance (or r_max until k
+// are found), keeping the k nearest in a register-resident sorted list. The
+// fixed-radius walk (the progressive mode) adds the summed power of a node
+// whose box lies entirely inside the sphere without visiting its photons.
 #pragma once
 #include "device_common.cuh"
 
 namespace mrt {
 
 constexpr int kKnnMax = 32;
+// A depth-first walk keeps at most one pending node per level; the radix
+// tree is at most 63 code bits + 32 index bits deep.
+constexpr int kPhotonStack = 100;
 
-__device__ __forceinline__ int grid_cell_index(const SceneView& S, int x, int y, int z) {
-  return (z * S.grid_dim[1] + y) * S.grid_dim[0] + x;
+__device__ __forceinline__ float node_dist2(const float4& lo, const float4& hi, float3 p) {
+  const float dx = fmaxf(fmaxf(lo.x - p.x, p.x - hi.x), 0.f);
+  const float dy = fmaxf(fmaxf(lo.y - p.y, p.y - hi.y), 0.f);
+  const float dz = fmaxf(fmaxf(lo.z - p.z, p.z - hi.z), 0.f);
+  return dx * dx + dy * dy + dz * dz;
+}
+__device__ __forceinline__ float node_far2(const float4& lo, const float4& hi, float3 p) {
+  const float dx = fmaxf(fabsf(p.x - lo.x), fabsf(p.x - hi.x));
+  const float dy = fmaxf(fabsf(p.y - lo.y), fabsf(p.y - hi.y));
+  const float dz = fmaxf(fabsf(p.z - lo.z), fabsf(p.z - hi.z));
+  return dx * dx + dy * dy + dz * dz;
 }
 
 // kNN mode: sum of the k nearest photon powers / (pi r_k^2) / norm when the
@@ -24,55 +41,99 @@ __device__ __forceinline__ int grid_cell_index(const SceneView& S, int x, int y,
 __device__ __forceinline__ float3 caustic_estimate(const SceneView& S, float3 p) {
   if (!S.caustic || S.n_photons == 0) return f3(0.f, 0.f, 0.f);
   const float r2max = S.caustic_mode ? S.fixed_radius2 : S.caustic_radius2;
-  int cx = (int)floorf((p.x - S.grid_min[0]) * S.grid_inv_cell);
-  int cy = (int)floorf((p.y - S.grid_min[1]) * S.grid_inv_cell);
-  int cz = (int)floorf((p.z - S.grid_min[2]) * S.grid_inv_cell);
-  if (cx < -1 || cy < -1 || cz < -1 || cx > S.grid_dim[0] || cy > S.grid_dim[1] || cz > S.grid_dim[2])
-    return f3(0.f, 0.f, 0.f);
+  const int n = S.n_photons;
+  int stack[kPhotonStack];
+  int sp = 0;
+  // children of the node being expanded (a single photon is its own root)
+  int kids[2] = {n == 1 ? ~0 : 0, n == 1 ? ~0 : 0};
+  int n_kids = n == 1 ? 1 : 0;
+  if (n > 1) stack[sp++] = 0;
+  int guard = 2 * n + 8;                  // every node is visited at most once
   if (S.caustic_mode) {
     float3 sum = f3(0.f, 0.f, 0.f);
-    for (int z = max(cz - 1, 0); z <= min(cz + 1, S.grid_dim[2] - 1); ++z)
-      for (int y = max(cy - 1, 0); y <= min(cy + 1, S.grid_dim[1] - 1); ++y)
-        for (int x = max(cx - 1, 0); x <= min(cx + 1, S.grid_dim[0] - 1); ++x) {
-          int c = grid_cell_index(S, x, y, z);
-          uint32_t b = __ldg(S.cell_start + c), e = __ldg(S.cell_start + c + 1);
-          for (uint32_t i = b; i < e; ++i) {
-            float4 q = __ldg(S.photon_pos + i);
-            float dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
-            if (dx * dx + dy * dy + dz * dz <= r2max) {
-              float4 w = __ldg(S.photon_pow + i);
-              sum = sum + f3(w.x, w.y, w.z);
-            }
-          }
+    while ((sp > 0 || n_kids > 0) && --guard > 0) {
+      if (n_kids == 0) {
+        const int nd = stack[--sp];
+        const float4 lo = __ldg(S.photon_nodes + 4 * nd), hi = __ldg(S.photon_nodes + 4 * nd + 1);
+        if (node_dist2(lo, hi, p) > r2max) continue;
+        if (node_far2(lo, hi, p) <= r2max) {
+          const float4 w = __ldg(S.photon_nodes + 4 * nd + 2);
+          sum = sum + f3(w.x, w.y, w.z);
+          continue;
         }
-    float area = 3.14159265358979f * r2max;
+        const float4 ch = __ldg(S.photon_nodes + 4 * nd + 3);
+        kids[0] = __float_as_int(ch.x);
+        kids[1] = __float_as_int(ch.y);
+        n_kids = 2;
+      }
+      const int c = kids[--n_kids];
+      if (c < 0) {
+        const float4 q = __ldg(S.photon_pos + ~c);
+        const float dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
+        if (dx * dx + dy * dy + dz * dz <= r2max) {
+          const float4 w = __ldg(S.photon_pow + ~c);
+          sum = sum + f3(w.x, w.y, w.z);
+        }
+      } else if (sp < kPhotonStack) {
+        stack[sp++] = c;
+      }
+    }
+    const float area = 3.14159265358979f * r2max;
     return sum * (S.inv_norm / area);
   }
   const int k = S.knn;
   float bd[kKnnMax];
   int bi[kKnnMax];
   int cnt = 0;
-  for (int z = max(cz - 1, 0); z <= min(cz + 1, S.grid_dim[2] - 1); ++z)
-    for (int y = max(cy - 1, 0); y <= min(cy + 1, S.grid_dim[1] - 1); ++y)
-      for (int x = max(cx - 1, 0); x <= min(cx + 1, S.grid_dim[0] - 1); ++x) {
-        int c = grid_cell_index(S, x, y, z);
-        uint32_t b = __ldg(S.cell_start + c), e = __ldg(S.cell_start + c + 1);
-        for (uint32_t i = b; i < e; ++i) {
-          float4 q = __ldg(S.photon_pos + i);
-          float dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
-          float d2 = dx * dx + dy * dy + dz * dz;
-          if (d2 > r2max) continue;
-          if (cnt == k && d2 >= bd[k - 1]) continue;
-          int j = cnt < k ? cnt++ : k - 1;
-          while (j > 0 && bd[j - 1] > d2) {
-            bd[j] = bd[j - 1];
-            bi[j] = bi[j - 1];
-            --j;
-          }
-          bd[j] = d2;
-          bi[j] = (int)i;
+  while ((sp > 0 || n_kids > 0) && --guard > 0) {
+    float bound = cnt == k ? fminf(r2max, bd[k - 1]) : r2max;
+    if (n_kids == 0) {
+      const int nd = stack[--sp];
+      const float4 lo = __ldg(S.photon_nodes + 4 * nd), hi = __ldg(S.photon_nodes + 4 * nd + 1);
+      if (node_dist2(lo, hi, p) > bound) continue;
+      const float4 ch = __ldg(S.photon_nodes + 4 * nd + 3);
+      kids[0] = __float_as_int(ch.x);
+      kids[1] = __float_as_int(ch.y);
+      n_kids = 2;
+      // photons first; internal children pushed farther first
+      int in[2], m = 0;
+      float din[2];
+      for (int t = 0; t < 2; ++t) {
+        const int c = kids[t];
+        if (c >= 0) {
+          din[m] = node_dist2(__ldg(S.photon_nodes + 4 * c), __ldg(S.photon_nodes + 4 * c + 1), p);
+          in[m++] = c;
         }
       }
+      if (m == 2 && din[0] < din[1]) {
+        const int ti = in[0]; in[0] = in[1]; in[1] = ti;
+        const float td = din[0]; din[0] = din[1]; din[1] = td;
+      }
+      for (int t = 0; t < m; ++t)
+        if (din[t] <= bound && sp < kPhotonStack) stack[sp++] = in[t];
+      // keep only the photon children for the loop below
+      int np = 0;
+      for (int t = 0; t < 2; ++t)
+        if (kids[t] < 0) kids[np++] = kids[t];
+      n_kids = np;
+      continue;
+    }
+    const int c = kids[--n_kids];
+    const int i = ~c;
+    const float4 q = __ldg(S.photon_pos + i);
+    const float dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
+    const float d2 = dx * dx + dy * dy + dz * dz;
+    if (d2 > r2max) continue;
+    if (cnt == k && d2 >= bd[k - 1]) continue;
+    int j = cnt < k ? cnt++ : k - 1;
+    while (j > 0 && bd[j - 1] > d2) {
+      bd[j] = bd[j - 1];
+      bi[j] = bi[j - 1];
+      --j;
+    }
+    bd[j] = d2;
+    bi[j] = i;
+  }
   if (cnt < k) return f3(0.f, 0.f, 0.f);
   float r2 = bd[k - 1];
   float area = 3.14159265358979f * r2;

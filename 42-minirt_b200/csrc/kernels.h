@@ -152,21 +152,18 @@ struct PhotonEmit {
 };
 cudaError_t launch_photon_emit(const SceneView& S, const PhotonEmit& P, int* status, cudaStream_t st);
 
-struct GridBuild {
+// Photon map (photon.cu): sorts the photons by the 63-bit Morton code of
+// their position (CUB radix sort of (code, index), deterministic) and builds
+// the linear BVH of SceneView.photon_nodes over them.
+struct PhotonTree {
   const float4* pos_in;
   const float4* pow_in;
   uint32_t n;
-  float4* pos_out;
-  float4* pow_out;
-  uint32_t* cell_of;         // n
-  uint32_t* cell_start;      // n_cells + 1
-  uint32_t* cursor;          // n_cells
-  uint32_t n_cells;
-  float grid_min[3];
-  float inv_cell;
-  int dim[3];
+  float4* pos_out;           // n
+  float4* pow_out;           // n
+  float4* nodes;             // 4 * max(n - 1, 1)
 };
-cudaError_t launch_grid_build(const GridBuild& G, cudaStream_t st);
+cudaError_t launch_photon_tree(const PhotonTree& T, cudaStream_t st);
 
 struct CausticQuery {
   const double* pts;

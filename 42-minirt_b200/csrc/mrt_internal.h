@@ -14,6 +14,8 @@
 //   shade   : 64 B per triangle in leaf order: (n0, u0) (n1, u1) (n2, u2)
 //             (v0, v1, v2, -). Read once per closest hit.
 //   planes  : 2 float4 + int4 per plane.
+//   photons : position / power float4 pairs in Morton order plus a linear
+//             BVH over them (4 float4 per internal node).
 //   env     : RGBE texels as uint32; for importance sampling an alias table
 //             (float prob, int alias) over the outcomes of the reference's
 //             two-step lookup and two float4 records per outcome
@@ -125,13 +127,14 @@ struct SceneView {
   int knn;
   float caustic_radius2; // compared against the k-th squared distance (get_caustic.c:45)
   float inv_norm;        // 1 / norm_factor
-  const float4* photon_pos;    // sorted by cell
+  const float4* photon_pos;    // in Morton order of their positions
   const float4* photon_pow;
-  const uint32_t* cell_start;  // grid cells, cell_start[c]..cell_start[c+1]
-  float grid_min[3];
-  float grid_inv_cell;
-  int grid_dim[3];
-  float grid_cell;
+  // Linear BVH over the Morton-ordered photons (Karras 2012): n - 1 internal
+  // nodes, node 0 the root, each split at the highest Morton bit that
+  // differs within its range; 4 float4 per node: (min.xyz, -), (max.xyz, -),
+  // (summed power.rgb, -), (left, right as int bits, -, -) where a child
+  // >= 0 is an internal node and ~i is photon i.
+  const float4* photon_nodes;
   int caustic_mode;      // 0 kNN, 1 fixed radius
   float fixed_radius2;
   int n_photons;

@@ -1,4 +1,4 @@
-// photon.cu — photon emission and the uniform-grid photon map.
+// photon.cu — photon emission and the photon map.
 //
 // Emission follows caustic_manager / emit_photon_from_one_light /
 // trace_single_photon_path / material_manager_v3_phothon
@@ -9,8 +9,21 @@
 // specular bounce preceded it (`return depth != 0`). One thread per photon,
 // warp-aggregated append into the photon buffer.
 //
-// The grid sorts photons by cell (CUB radix sort of (cell, index), so the
-// order is deterministic) and records each cell's start.
+// The map sorts the photons by the 63-bit Morton code of their position in
+// the photons' bounding box (21 bits per axis: a few stray photons land
+// hundreds of metres from the caustics, and a coarser code would leave the
+// caustics in a handful of cells; CUB radix sort of (code, index), so the
+// order is deterministic) and builds a linear BVH over them (Karras,
+// "Maximizing parallelism in the construction of BVHs, octrees, and k-d
+// trees", HPG 2012): internal node i covers a Morton range and splits it at
+// its highest differing bit, so every node is a spatial cell of the code's
+// implicit octree; boxes and power sums are filled bottom-up, the second
+// child to finish completing its parent. A uniform grid was the first form:
+// the caustics of configuration 2 are clustered (the densest 10 cm of floor
+// holds ~180x the median) and the stray photons stretched its cells, so
+// every gather scanned thousands of photons. The hierarchy adapts: a kNN
+// gather prunes by its k-th distance, a fixed-radius gather adds whole nodes
+// that lie inside the sphere.
 #include <cub/device/device_radix_sort.cuh>
 
 #include "kernels.h"
@@ -110,35 +123,146 @@ __global__ void photon_emit_kernel(SceneView S, PhotonEmit E, int* status) {
   }
 }
 
-__global__ void cell_of_kernel(GridBuild G, uint32_t* idx) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= G.n) return;
-  float4 p = G.pos_in[i];
-  int x = min(max((int)floorf((p.x - G.grid_min[0]) * G.inv_cell), 0), G.dim[0] - 1);
-  int y = min(max((int)floorf((p.y - G.grid_min[1]) * G.inv_cell), 0), G.dim[1] - 1);
-  int z = min(max((int)floorf((p.z - G.grid_min[2]) * G.inv_cell), 0), G.dim[2] - 1);
-  G.cell_of[i] = (uint32_t)((z * G.dim[1] + y) * G.dim[0] + x);
+// Float min / max through int atomics: the order-preserving map of a float
+// to an int (negative values have their magnitude bits flipped).
+__device__ __forceinline__ int ordered(float f) {
+  const int i = __float_as_int(f);
+  return i >= 0 ? i : i ^ 0x7fffffff;
+}
+__device__ __forceinline__ float unordered(int i) { return __int_as_float(i >= 0 ? i : i ^ 0x7fffffff); }
+
+// bounds[0..2] min, [3..5] max as ordered ints (initialised by the host).
+__global__ void photon_bounds_kernel(PhotonTree T, int* bounds) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+  if (i < T.n) {
+    const float4 p = T.pos_in[i];
+    mn[0] = mx[0] = p.x;
+    mn[1] = mx[1] = p.y;
+    mn[2] = mx[2] = p.z;
+  }
+  for (int k = 0; k < 3; ++k)
+    for (int off = 16; off > 0; off >>= 1) {
+      mn[k] = fminf(mn[k], __shfl_down_sync(0xffffffffu, mn[k], off));
+      mx[k] = fmaxf(mx[k], __shfl_down_sync(0xffffffffu, mx[k], off));
+    }
+  if ((threadIdx.x & 31) == 0 && mn[0] <= mx[0])
+    for (int k = 0; k < 3; ++k) {
+      atomicMin(bounds + k, ordered(mn[k]));
+      atomicMax(bounds + 3 + k, ordered(mx[k]));
+    }
+}
+
+// Spreads the low 21 bits of v to every third bit.
+__device__ __forceinline__ uint64_t spread3(uint64_t v) {
+  v &= 0x1fffffull;
+  v = (v | (v << 32)) & 0x1f00000000ffffull;
+  v = (v | (v << 16)) & 0x1f0000ff0000ffull;
+  v = (v | (v << 8)) & 0x100f00f00f00f00full;
+  v = (v | (v << 4)) & 0x10c30c30c30c30c3ull;
+  v = (v | (v << 2)) & 0x1249249249249249ull;
+  return v;
+}
+
+__global__ void morton_kernel(PhotonTree T, const int* bounds, uint64_t* code, uint32_t* idx) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= T.n) return;
+  const float4 p = T.pos_in[i];
+  const float q[3] = {p.x, p.y, p.z};
+  // one scale for the three axes (cubic cells): photons on a plane have a
+  // near-zero extent across it, and scaling that axis by its own extent
+  // would give float noise the top bits of the code
+  double ext = 0.0;
+  for (int k = 0; k < 3; ++k) ext = fmax(ext, (double)unordered(bounds[3 + k]) - (double)unordered(bounds[k]));
+  uint64_t c[3];
+  for (int k = 0; k < 3; ++k) {
+    const double u = ext > 0.0 ? ((double)q[k] - (double)unordered(bounds[k])) / ext : 0.0;
+    c[k] = (uint64_t)min(max((long long)(u * 2097151.0), 0ll), 2097151ll);
+  }
+  code[i] = (spread3(c[0]) << 2) | (spread3(c[1]) << 1) | spread3(c[2]);
   idx[i] = i;
 }
 
-__global__ void gather_kernel(GridBuild G, const uint32_t* sorted_cell, const uint32_t* sorted_idx) {
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= G.n) return;
-  uint32_t s = sorted_idx[i];
-  G.pos_out[i] = G.pos_in[s];
-  G.pow_out[i] = G.pow_in[s];
-  uint32_t c = sorted_cell[i];
-  if (i == 0 || sorted_cell[i - 1] != c) {
-    uint32_t prev = i == 0 ? 0 : sorted_cell[i - 1] + 1;
-    for (uint32_t k = prev; k <= c; ++k) G.cell_start[k] = i;
-  }
-  if (i == G.n - 1)
-    for (uint32_t k = c + 1; k <= G.n_cells; ++k) G.cell_start[k] = G.n;
+__global__ void photon_gather_kernel(PhotonTree T, const uint32_t* sorted_idx) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= T.n) return;
+  const uint32_t s = sorted_idx[i];
+  T.pos_out[i] = T.pos_in[s];
+  T.pow_out[i] = T.pow_in[s];
 }
 
-__global__ void empty_grid_kernel(GridBuild G) {
-  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k <= G.n_cells) G.cell_start[k] = 0;
+// Length of the common prefix of the keys of photons i and j (index as a
+// tie-break for equal codes); -1 outside [0, n).
+__device__ __forceinline__ int common_prefix(const uint64_t* code, int n, int i, int j) {
+  if (j < 0 || j >= n) return -1;
+  const uint64_t a = code[i], b = code[j];
+  if (a != b) return __clzll((long long)(a ^ b));
+  return 64 + __clz((int)((uint32_t)i ^ (uint32_t)j));
+}
+
+// Internal node i of the radix tree: its range, split and children.
+__global__ void lbvh_internal_kernel(PhotonTree T, const uint64_t* code, int* parent_node, int* parent_leaf) {
+  const int n = (int)T.n;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n - 1) return;
+  const int d = common_prefix(code, n, i, i + 1) - common_prefix(code, n, i, i - 1) >= 0 ? 1 : -1;
+  const int dmin = common_prefix(code, n, i, i - d);
+  int lmax = 2;
+  while (common_prefix(code, n, i, i + lmax * d) > dmin) lmax *= 2;   // bounded by the range end
+  int l = 0;
+  for (int t = lmax / 2; t >= 1; t /= 2)
+    if (common_prefix(code, n, i, i + (l + t) * d) > dmin) l += t;
+  const int j = i + l * d;
+  const int dnode = common_prefix(code, n, i, j);
+  int s = 0;
+  for (int div = 2;; div *= 2) {
+    const int t = (l + div - 1) / div;
+    if (common_prefix(code, n, i, i + (s + t) * d) > dnode) s += t;
+    if (t <= 1) break;
+  }
+  const int g = i + s * d + min(d, 0);
+  const int lo = min(i, j), hi = max(i, j);
+  const int left = lo == g ? ~g : g;
+  const int right = hi == g + 1 ? ~(g + 1) : g + 1;
+  T.nodes[4 * (size_t)i + 3] = make_float4(__int_as_float(left), __int_as_float(right), 0.f, 0.f);
+  if (left >= 0) parent_node[left] = i; else parent_leaf[~left] = i;
+  if (right >= 0) parent_node[right] = i; else parent_leaf[~right] = i;
+  if (i == 0) parent_node[0] = -1;
+}
+
+__device__ __forceinline__ void child_box(const PhotonTree& T, int c, float3& lo, float3& hi, float3& pw) {
+  if (c < 0) {
+    const float4 p = __ldcg(T.pos_out + ~c), w = __ldcg(T.pow_out + ~c);
+    lo = hi = f3(p.x, p.y, p.z);
+    pw = f3(w.x, w.y, w.z);
+  } else {
+    const float4 a = __ldcg(T.nodes + 4 * (size_t)c), b = __ldcg(T.nodes + 4 * (size_t)c + 1),
+                 w = __ldcg(T.nodes + 4 * (size_t)c + 2);
+    lo = f3(a.x, a.y, a.z);
+    hi = f3(b.x, b.y, b.z);
+    pw = f3(w.x, w.y, w.z);
+  }
+}
+
+// Bottom-up boxes: one thread per photon walks to the root; at each node the
+// first child to arrive stops, the second fills the node.
+__global__ void lbvh_bounds_kernel(PhotonTree T, const int* parent_node, const int* parent_leaf,
+                                   unsigned* arrived) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= (int)T.n) return;
+  int node = parent_leaf[j];
+  for (int guard = 0; node >= 0 && guard < 64 + (int)T.n; ++guard) {
+    __threadfence();
+    if (atomicAdd(arrived + node, 1u) == 0u) return;
+    const float4 ch = __ldcg(T.nodes + 4 * (size_t)node + 3);
+    float3 la, ha, pa, lb, hb, pb;
+    child_box(T, __float_as_int(ch.x), la, ha, pa);
+    child_box(T, __float_as_int(ch.y), lb, hb, pb);
+    T.nodes[4 * (size_t)node] = make_float4(fminf(la.x, lb.x), fminf(la.y, lb.y), fminf(la.z, lb.z), 0.f);
+    T.nodes[4 * (size_t)node + 1] = make_float4(fmaxf(ha.x, hb.x), fmaxf(ha.y, hb.y), fmaxf(ha.z, hb.z), 0.f);
+    T.nodes[4 * (size_t)node + 2] = make_float4(pa.x + pb.x, pa.y + pb.y, pa.z + pb.z, 0.f);
+    node = parent_node[node];
+  }
 }
 
 __global__ void caustic_query_kernel(SceneView S, CausticQuery Q) {
@@ -161,30 +285,51 @@ cudaError_t launch_photon_emit(const SceneView& S, const PhotonEmit& P, int* sta
   return cudaGetLastError();
 }
 
-// Scratch: cell_of (n), idx (n), sorted cell (n), sorted idx (n), CUB temp.
-cudaError_t launch_grid_build(const GridBuild& G, cudaStream_t st) {
-  if (G.n == 0) {
-    empty_grid_kernel<<<(G.n_cells + 256) / 256, 256, 0, st>>>(G);
-    return cudaGetLastError();
-  }
-  uint32_t *idx = nullptr, *scell = nullptr, *sidx = nullptr;
+// Scratch: bounds (6 ints), code (n, 64-bit), idx (n), sorted code, sorted idx
+// (n), CUB temp; stream-ordered allocations released at the end.
+cudaError_t launch_photon_tree(const PhotonTree& T, cudaStream_t st) {
+  if (T.n == 0) return cudaSuccess;
+  int* bounds = nullptr;
+  uint64_t *code = nullptr, *scode = nullptr;
+  uint32_t *idx = nullptr, *sidx = nullptr;
   void* tmp = nullptr;
   size_t tmp_bytes = 0;
   cudaError_t e;
-  if ((e = cudaMallocAsync(&idx, sizeof(uint32_t) * G.n, st)) != cudaSuccess) return e;
-  if ((e = cudaMallocAsync(&scell, sizeof(uint32_t) * G.n, st)) != cudaSuccess) return e;
-  if ((e = cudaMallocAsync(&sidx, sizeof(uint32_t) * G.n, st)) != cudaSuccess) return e;
+  if ((e = cudaMallocAsync(&bounds, sizeof(int) * 6, st)) != cudaSuccess) return e;
+  if ((e = cudaMallocAsync(&code, sizeof(uint64_t) * T.n, st)) != cudaSuccess) return e;
+  if ((e = cudaMallocAsync(&idx, sizeof(uint32_t) * T.n, st)) != cudaSuccess) return e;
+  if ((e = cudaMallocAsync(&scode, sizeof(uint64_t) * T.n, st)) != cudaSuccess) return e;
+  if ((e = cudaMallocAsync(&sidx, sizeof(uint32_t) * T.n, st)) != cudaSuccess) return e;
+  // ordered(+inf) for the minima, ordered(-inf) for the maxima
+  const int init[6] = {0x7f800000, 0x7f800000, 0x7f800000, (int)(0xff800000u ^ 0x7fffffffu),
+                       (int)(0xff800000u ^ 0x7fffffffu), (int)(0xff800000u ^ 0x7fffffffu)};
+  if ((e = cudaMemcpyAsync(bounds, init, sizeof(init), cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
   const unsigned b = 256;
-  cell_of_kernel<<<(G.n + b - 1) / b, b, 0, st>>>(G, idx);
-  int bits = 1;
-  while (bits < 32 && (1ull << bits) <= G.n_cells) ++bits;
-  cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, G.cell_of, scell, idx, sidx, (int)G.n, 0, bits, st);
+  const unsigned g = (T.n + b - 1) / b;
+  photon_bounds_kernel<<<g, b, 0, st>>>(T, bounds);
+  morton_kernel<<<g, b, 0, st>>>(T, bounds, code, idx);
+  cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, code, scode, idx, sidx, (int)T.n, 0, 63, st);
   if ((e = cudaMallocAsync(&tmp, tmp_bytes, st)) != cudaSuccess) return e;
-  cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, G.cell_of, scell, idx, sidx, (int)G.n, 0, bits, st);
-  gather_kernel<<<(G.n + b - 1) / b, b, 0, st>>>(G, scell, sidx);
+  cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, code, scode, idx, sidx, (int)T.n, 0, 63, st);
+  photon_gather_kernel<<<g, b, 0, st>>>(T, sidx);
+  if (T.n > 1) {
+    int *parent_node = nullptr, *parent_leaf = nullptr;
+    unsigned* arrived = nullptr;
+    if ((e = cudaMallocAsync(&parent_node, sizeof(int) * (T.n - 1), st)) != cudaSuccess) return e;
+    if ((e = cudaMallocAsync(&parent_leaf, sizeof(int) * T.n, st)) != cudaSuccess) return e;
+    if ((e = cudaMallocAsync(&arrived, sizeof(unsigned) * (T.n - 1), st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(arrived, 0, sizeof(unsigned) * (T.n - 1), st)) != cudaSuccess) return e;
+    lbvh_internal_kernel<<<(T.n - 1 + b - 1) / b, b, 0, st>>>(T, scode, parent_node, parent_leaf);
+    lbvh_bounds_kernel<<<g, b, 0, st>>>(T, parent_node, parent_leaf, arrived);
+    cudaFreeAsync(parent_node, st);
+    cudaFreeAsync(parent_leaf, st);
+    cudaFreeAsync(arrived, st);
+  }
   cudaFreeAsync(tmp, st);
+  cudaFreeAsync(bounds, st);
+  cudaFreeAsync(code, st);
   cudaFreeAsync(idx, st);
-  cudaFreeAsync(scell, st);
+  cudaFreeAsync(scode, st);
   cudaFreeAsync(sidx, st);
   return cudaGetLastError();
 }
