@@ -20,7 +20,7 @@ HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "libmrt.so"
 MINIRT_LIB_PATH = HERE / "libmrt_minirt.so"
 
-MRT_ABI_VERSION = 2
+MRT_ABI_VERSION = 3
 
 MRT_OK = 0
 STATUS_NAMES = {
@@ -53,6 +53,25 @@ class Sphere(C.Structure):
 class Plane(C.Structure):
     _fields_ = [("point", f64x3), ("normal", f64x3), ("material", C.c_int32),
                 ("color", u8x3), ("pad_", C.c_uint8)]
+
+
+class Cylinder(C.Structure):
+    _fields_ = [("position", f64x3), ("orientation", f64x3), ("diameter", C.c_double),
+                ("height", C.c_double), ("material", C.c_int32), ("material_top", C.c_int32),
+                ("material_bot", C.c_int32), ("color", u8x3), ("pad_", C.c_uint8)]
+
+
+class Cone(C.Structure):
+    _fields_ = [("position", f64x3), ("orientation", f64x3), ("diameter", C.c_double),
+                ("height", C.c_double), ("material", C.c_int32), ("material_top", C.c_int32),
+                ("color", u8x3), ("pad_", C.c_uint8 * 5)]
+
+
+class Hyperboloid(C.Structure):
+    _fields_ = [("position", f64x3), ("orientation", f64x3), ("a", C.c_double),
+                ("b", C.c_double), ("c", C.c_double), ("shape", C.c_double),
+                ("height", C.c_double), ("material", C.c_int32), ("color", u8x3),
+                ("pad_", C.c_uint8)]
 
 
 class Mesh(C.Structure):
@@ -100,7 +119,10 @@ class SceneDesc(C.Structure):
                 ("planes", C.POINTER(Plane)), ("n_planes", C.c_int32),
                 ("n_meshes", C.c_int32), ("meshes", C.POINTER(Mesh)),
                 ("lights", C.POINTER(Light)), ("n_lights", C.c_int32),
-                ("pad2_", C.c_int32)]
+                ("pad2_", C.c_int32),
+                ("cylinders", C.POINTER(Cylinder)), ("cones", C.POINTER(Cone)),
+                ("hyperboloids", C.POINTER(Hyperboloid)), ("n_cylinders", C.c_int32),
+                ("n_cones", C.c_int32), ("n_hyperboloids", C.c_int32), ("pad3_", C.c_int32)]
 
 
 class RenderParams(C.Structure):

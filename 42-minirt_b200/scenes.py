@@ -64,6 +64,9 @@ class Scene:
     planes: list = field(default_factory=list)    # (point, normal, material, color)
     meshes: list = field(default_factory=list)    # MeshData
     lights: list = field(default_factory=list)    # dicts
+    cylinders: list = field(default_factory=list)  # dicts: position, orientation, diameter, height, ...
+    cones: list = field(default_factory=list)      # dicts: position (apex), orientation, diameter, height
+    hyperboloids: list = field(default_factory=list)  # dicts: position, orientation, a, b, c, shape, height
     ambient_ratio: float = 0.0
     ambient_color: tuple = (0, 0, 0)
     hdr: np.ndarray | None = None                 # (H,W,4) uint8 RGBE
@@ -175,6 +178,35 @@ class Scene:
             li[i].shadow_sample = L.get("shadow_sample", 0)
         keep.append(li)
         d.lights, d.n_lights = li, len(self.lights)
+        cy = (mrt.Cylinder * max(1, len(self.cylinders)))()
+        for i, q in enumerate(self.cylinders):
+            cy[i].position[:] = q["position"]
+            cy[i].orientation[:] = q["orientation"]
+            cy[i].diameter, cy[i].height = q["diameter"], q["height"]
+            cy[i].material = q.get("material", -1)
+            cy[i].material_top = q.get("material_top", -1)
+            cy[i].material_bot = q.get("material_bot", -1)
+            cy[i].color[:] = q.get("color", (255, 255, 255))
+        co = (mrt.Cone * max(1, len(self.cones)))()
+        for i, q in enumerate(self.cones):
+            co[i].position[:] = q["position"]
+            co[i].orientation[:] = q["orientation"]
+            co[i].diameter, co[i].height = q["diameter"], q["height"]
+            co[i].material = q.get("material", -1)
+            co[i].material_top = q.get("material_top", -1)
+            co[i].color[:] = q.get("color", (255, 255, 255))
+        hb = (mrt.Hyperboloid * max(1, len(self.hyperboloids)))()
+        for i, q in enumerate(self.hyperboloids):
+            hb[i].position[:] = q["position"]
+            hb[i].orientation[:] = q["orientation"]
+            hb[i].a, hb[i].b, hb[i].c = q["a"], q["b"], q["c"]
+            hb[i].shape, hb[i].height = q["shape"], q["height"]
+            hb[i].material = q.get("material", -1)
+            hb[i].color[:] = q.get("color", (255, 255, 255))
+        keep += [cy, co, hb]
+        d.cylinders, d.n_cylinders = cy, len(self.cylinders)
+        d.cones, d.n_cones = co, len(self.cones)
+        d.hyperboloids, d.n_hyperboloids = hb, len(self.hyperboloids)
         self._keep = keep
         return d
 
@@ -514,6 +546,57 @@ def make_c2_progressive(**kw) -> Scene:
     (128 spp), fixed-radius gather shrinking by 0.9 per pass."""
     sc = make_c2(passes=16, mode=1, spp_per_pass=8, **kw)
     sc.name = "c2p"
+    return sc
+
+
+def _unit(v) -> tuple:
+    v = np.asarray(v, float)
+    return tuple(v / np.linalg.norm(v))
+
+
+def make_quadrics(seed: int = 5, width: int = 320, height: int = 240, spp: int = 64,
+                  depth: int = 8) -> Scene:
+    """Cylinders, cones and hyperboloids (t_cylinder / t_cone / t_hyperboloid)
+    over a ground plane: an upright cylinder with a metal top cap, a tilted
+    glass cylinder with a lambertian bottom cap, an inverted cone with a metal
+    cap, a tilted cone, a one-sheet and a two-sheet hyperboloid, an emissive
+    sphere, a glass sphere and a point light under a blue-grey ambient sky.
+    Orientations are unit vectors, as the reference's parser leaves them
+    (parse_elements.c:28)."""
+    rng = np.random.default_rng(seed)
+    aspect = width / height
+    sc = Scene("quadrics", width, height, spp, depth,
+               camera=dict(position=(0.0, 3.0, 12.0), orientation=look_at((0, 3, 12), (0, 1, 0)),
+                           fov=hfov_from_vfov(45.0, aspect)), seed=seed)
+
+    def mat(**m):
+        sc.materials.append(m)
+        return len(sc.materials) - 1
+
+    ground = mat(color=(200, 200, 190), metallic=0.0, ior=0.0)
+    sc.planes.append(((0.0, 0.0, 0.0), (0.0, 1.0, 0.0), ground, (200, 200, 190)))
+    lam = [mat(**_material_mix(rng, "lambertian")) for _ in range(4)]
+    metal = [mat(**_material_mix(rng, "metal")) for _ in range(2)]
+    glass = mat(**_material_mix(rng, "dielectric"))
+    sc.cylinders.append(dict(position=(-3.0, 1.0, 0.0), orientation=(0.0, 1.0, 0.0), diameter=1.6,
+                             height=2.0, material=lam[0], material_top=metal[0], color=(255, 255, 255)))
+    sc.cylinders.append(dict(position=(2.5, 1.2, -1.0), orientation=_unit((1.0, 0.6, 0.3)), diameter=1.0,
+                             height=2.5, material=glass, material_bot=lam[1], color=(255, 255, 255)))
+    sc.cones.append(dict(position=(0.0, 2.5, -2.0), orientation=(0.0, -1.0, 0.0), diameter=2.0,
+                         height=2.0, material=lam[2], material_top=metal[1], color=(255, 255, 255)))
+    sc.cones.append(dict(position=(-1.2, 0.2, 2.5), orientation=_unit((0.3, 1.0, 0.2)), diameter=1.2,
+                         height=1.5, material=lam[3], color=(255, 255, 255)))
+    sc.hyperboloids.append(dict(position=(3.5, 1.5, 2.0), orientation=(0.0, 1.0, 0.0), a=0.5, b=0.7,
+                                c=1.0, shape=1.0, height=3.0, material=lam[1], color=(255, 255, 255)))
+    sc.hyperboloids.append(dict(position=(-4.0, 2.0, -3.0), orientation=_unit((0.2, 1.0, 0.1)), a=0.6,
+                                b=0.6, c=0.8, shape=-1.0, height=3.0, material=metal[0],
+                                color=(255, 255, 255)))
+    light = mat(color=(0, 0, 0), metallic=0.0, ior=0.0, emission_strength=8.0,
+                emission_color=(255, 240, 220))
+    sc.spheres.append(((0.0, 7.0, 2.0), 0.8, light, (0, 0, 0)))
+    sc.spheres.append(((1.0, 0.6, 3.0), 0.6, glass, (255, 255, 255)))
+    sc.lights.append(dict(position=(2.0, 6.0, 6.0), brightness=0.6, color=(255, 255, 255)))
+    sc.ambient_ratio, sc.ambient_color = 0.2, (120, 140, 200)
     return sc
 
 

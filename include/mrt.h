@@ -36,7 +36,7 @@
 extern "C" {
 # endif
 
-# define MRT_ABI_VERSION 2
+# define MRT_ABI_VERSION 3
 
 # if defined(__GNUC__)
 #  define MRT_API __attribute__((visibility("default")))
@@ -96,6 +96,52 @@ typedef struct mrt_plane
 	uint8_t	color[3];
 	uint8_t	pad_;
 }	mrt_plane;
+
+/* t_cylinder (scene_structs.h:196-206): centred on position, axis along
+ * orientation (unit, as parse_elements.c:28 leaves it), caps at
+ * position +- height/2 * orientation. */
+typedef struct mrt_cylinder
+{
+	double	position[3];
+	double	orientation[3];
+	double	diameter;
+	double	height;
+	int32_t	material;          /* < 0: none (the object's colour) */
+	int32_t	material_top;      /* < 0: material */
+	int32_t	material_bot;      /* < 0: material */
+	uint8_t	color[3];
+	uint8_t	pad_;
+}	mrt_cylinder;
+
+/* t_cone (scene_structs.h:185-194): position is the apex, the cap of the
+ * given diameter lies at apex + height * orientation. */
+typedef struct mrt_cone
+{
+	double	position[3];
+	double	orientation[3];
+	double	diameter;
+	double	height;
+	int32_t	material;
+	int32_t	material_top;      /* < 0: material */
+	uint8_t	color[3];
+	uint8_t	pad_[5];
+}	mrt_cone;
+
+/* t_hyperboloid (scene_structs.h:154-165): x^2/a^2 + y^2/b^2 - z^2/c^2 =
+ * shape in the frame of its orientation, clipped to |z| <= height / 2. */
+typedef struct mrt_hyperboloid
+{
+	double	position[3];
+	double	orientation[3];
+	double	a;
+	double	b;
+	double	c;
+	double	shape;
+	double	height;
+	int32_t	material;
+	uint8_t	color[3];
+	uint8_t	pad_;
+}	mrt_hyperboloid;
 
 /* Triangle mesh (t_custom_object + t_triangle/t_vertex, scene_structs.h:208-252).
  * Indexed: positions/normals per vertex, 3 indices per triangle. indices may
@@ -205,6 +251,15 @@ typedef struct mrt_scene_desc
 	const mrt_light		*lights;
 	int32_t				n_lights;
 	int32_t				pad2_;
+	/* Objects of the BVH are numbered (flat prim ids) spheres, cylinders,
+	 * cones, hyperboloids, then mesh triangles, then planes. */
+	const mrt_cylinder		*cylinders;
+	const mrt_cone			*cones;
+	const mrt_hyperboloid	*hyperboloids;
+	int32_t				n_cylinders;
+	int32_t				n_cones;
+	int32_t				n_hyperboloids;
+	int32_t				pad3_;
 }	mrt_scene_desc;
 
 /* ------------------------------------------------------------- rendering */

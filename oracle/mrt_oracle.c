@@ -67,6 +67,7 @@ static inline fc fmul(fc a, fc b) { return (fc){a.r * b.r, a.g * b.g, a.b * b.b}
 static inline fc fscale(fc a, double c) { return (fc){a.r * c, a.g * c, a.b * c}; }
 static inline fc c2f(const uint8_t *c) { return (fc){c[0] / 255.0, c[1] / 255.0, c[2] / 255.0}; }
 static inline double clamp01(double v) { return v < 0 ? 0 : (v > 1 ? 1 : v); } /* clamp_int.c:39 */
+static inline int mat_or_none(int32_t m, int n) { return (m >= 0 && m < n) ? m : -1; }
 static inline double clampv(double v, double lo, double hi)               /* clamp_double.c:15 */
 {
 	if (v <= lo)
@@ -170,7 +171,7 @@ typedef struct
 	fc		emission_color;
 }	mat_t;
 
-enum { PT_SPHERE = 0, PT_TRI = 1 };
+enum { PT_SPHERE = 0, PT_TRI = 1, PT_CYL = 2, PT_CONE = 3, PT_HYP = 4 };
 
 typedef struct
 {
@@ -178,8 +179,12 @@ typedef struct
 	int		flat;
 	int		mat;
 	uint8_t	color[3];
-	v3		center;            /* sphere centre or triangle centroid */
+	v3		center;            /* sphere centre, triangle centroid, quadric position */
 	double	radius, r2;
+	v3		ori;               /* quadric orientation as given */
+	double	diam, height;      /* cylinder, cone */
+	double	qa, qb, qc, shape; /* hyperboloid (height in `height`) */
+	int		mat_top, mat_bot;  /* cylinder / cone cap materials, -1 none */
 	v3		p[3], n[3];
 	double	uv[3][2];
 }	prim_t;
@@ -383,13 +388,48 @@ static void qsort_axis_(uint32_t *arr, double lo, double hi, ro_scene *s, int ax
 	}
 }
 
-static void prim_bounds(prim_t *p, v3 *mn, v3 *mx)     /* bvh_obj_bounds.c:16,96 */
+/* extents of a disc of radius r with unit normal a, added to [p0, p1]
+ * (compute_cylinder_bounds, bvh_obj_bounds.c:41-60) */
+static void disc_bounds(v3 p0, v3 p1, v3 a, double r, v3 *mn, v3 *mx)
+{
+	v3	e = {r * sqrt(1.0 - a.x * a.x), r * sqrt(1.0 - a.y * a.y), r * sqrt(1.0 - a.z * a.z)};
+
+	*mn = vsub(vmin(p0, p1), e);
+	*mx = vadd(vmax(p0, p1), e);
+}
+
+static void prim_bounds(prim_t *p, v3 *mn, v3 *mx)     /* bvh_obj_bounds.c:16-96 */
 {
 	if (p->type == PT_SPHERE)
 	{
 		v3 r = {p->radius, p->radius, p->radius};
 		*mn = vsub(p->center, r);
 		*mx = vadd(p->center, r);
+		return ;
+	}
+	if (p->type == PT_CYL)
+	{
+		v3	a = vunit(p->ori);
+		v3	half = vscale(a, p->height * 0.5);
+
+		disc_bounds(vsub(p->center, half), vadd(p->center, half), a, p->diam * 0.5, mn, mx);
+		return ;
+	}
+	if (p->type == PT_CONE)
+	{
+		v3	a = vunit(p->ori);
+
+		disc_bounds(p->center, vadd(p->center, vscale(a, p->height)), a, p->diam * 0.5, mn, mx);
+		return ;
+	}
+	if (p->type == PT_HYP)
+	{
+		v3		a = vunit(p->ori);
+		v3		half = vscale(a, p->height * 0.5);
+		double	rmax = fmax(p->qa, p->qb) * sqrt(p->shape
+				+ ((p->height * 0.5) * (p->height * 0.5)) / (p->qc * p->qc));
+
+		disc_bounds(vsub(p->center, half), vadd(p->center, half), a, rmax, mn, mx);
 		return ;
 	}
 	*mn = vmin(p->p[0], vmin(p->p[1], p->p[2]));
@@ -665,6 +705,297 @@ static int hit_triangle_exact(ro_scene *s, prim_t *tr, const ray_t *r, hrec_t *r
 	return 1;
 }
 
+/* ------------------------------------------------------------ quadrics */
+
+/* solve_quadratic (quadratique.c:17) */
+static int solve_q(double a, double b, double c, double *t0, double *t1)
+{
+	double	disc = b * b - 4.0 * a * c;
+	double	sq, den;
+
+	if (disc < 0.0)
+		return (0);
+	den = 2.0 * a;
+	sq = sqrt(disc);
+	*t0 = (-b - sq) / den;
+	*t1 = (-b + sq) / den;
+	return (1);
+}
+
+/* valid_t (valid_t.c:16) */
+static int valid_root(double t0, double t1, double *th)
+{
+	*th = t0;
+	if (*th < IT_MIN || *th > IT_MAX)
+	{
+		*th = t1;
+		if (*th < IT_MIN || *th > IT_MAX)
+			return (0);
+	}
+	return (1);
+}
+
+/* set_normal_face (normal.c:16) */
+static v3 face(const ray_t *r, v3 n, hrec_t *rec)
+{
+	if (vdot(r->dir, n) < 0)
+	{
+		rec->front_face = 1;
+		return (n);
+	}
+	rec->front_face = 0;
+	return (vneg(n));
+}
+
+/* texture coordinates of the quadrics (cylinder_uv.c:16-58,
+ * hit_cone.c:14-52, hit_hyperboloid.c:14-34): the material's scale tiles
+ * them as for spheres */
+static void uv_tile(ro_scene *s, int mat, hrec_t *rec)
+{
+	double	ip;
+
+	if (mat >= 0 && s->mats[mat].scale != 1)
+	{
+		rec->u *= s->mats[mat].scale;
+		rec->v *= s->mats[mat].scale;
+		rec->u = modf(rec->u, &ip);
+		rec->v = modf(rec->v, &ip);
+	}
+}
+
+static v3 uv_right(v3 ori)
+{
+	if (fabs(ori.y) < 0.99)
+		return (vunit(vcross((v3){0, 1, 0}, ori)));
+	return (vunit(vcross((v3){1, 0, 0}, ori)));
+}
+
+static double uv_angle(v3 rel, v3 ori)
+{
+	v3	right = uv_right(ori);
+
+	return (clamp01((atan2(vdot(rel, vcross(ori, right)), vdot(rel, right)) + PI_D) / (2.0 * PI_D)));
+}
+
+static void uv_cap(hrec_t *rec, v3 centre, v3 ori, double diam)
+{
+	v3	right = uv_right(ori);
+	v3	rel = vsub(rec->point, centre);
+
+	rec->u = clamp01((vdot(rel, right) / diam) + 0.5);
+	rec->v = clamp01((vdot(rel, vcross(ori, right)) / diam) + 0.5);
+}
+
+/* one cap of hit_cylinder (hit_cylinder.c:39-99); normal n as given */
+static int cyl_cap(const ray_t *r, v3 c, v3 ori, double rad, v3 n, hrec_t *rec)
+{
+	double	den = vdot(r->dir, ori);
+	double	t;
+	v3		hp;
+
+	if (fabs(den) < 1e-6)
+		return (0);
+	t = -vdot(vsub(r->orig, c), ori) / den;
+	if (t < IT_MIN || t > IT_MAX)
+		return (0);
+	hp = ray_at(*r, t);
+	if (vlen(vsub(hp, c)) > rad)
+		return (0);
+	rec->t = t;
+	rec->point = hp;
+	rec->normal = n;
+	rec->front_face = (vdot(r->dir, rec->normal) < 0);
+	return (1);
+}
+
+/* hit_cylinder (hit_cylinder.c:110-134) with handle_cylinder_hit (:15-37)
+ * and the cap materials of update_hit_cylinder (hit_obj.c:16-32) */
+static int hit_cylinder(ro_scene *s, prim_t *p, const ray_t *r, hrec_t *rec)
+{
+	v3		ori = p->ori;
+	v3		axis, oc, pt, base;
+	double	dd, oo, t0, t1, th, proj, rad = p->diam * 0.5;
+	int		hit_any = 0;
+	hrec_t	tmp;
+
+	if (ori.x == 0 && ori.y == 0 && ori.z == 0)
+		ori.y = 1;
+	axis = vunit(ori);
+	oc = vsub(r->orig, p->center);
+	dd = vdot(r->dir, ori);
+	oo = vdot(oc, ori);
+	if (solve_q(vdot(r->dir, r->dir) - dd * dd, 2.0 * (vdot(r->dir, oc) - dd * oo),
+			vdot(oc, oc) - oo * oo - rad * rad, &t0, &t1) && valid_root(t0, t1, &th))
+	{
+		pt = ray_at(*r, th);
+		base = vsub(p->center, vscale(axis, p->height * 0.5));
+		proj = vdot(vsub(pt, base), axis);
+		if (!(proj < 0.0 || proj > p->height))
+		{
+			v3	out = vunit(vsub(vsub(pt, base), vscale(axis, proj)));
+
+			rec->t = th;
+			rec->point = pt;
+			rec->normal = face(r, out, rec);
+			rec->mat = p->mat;
+			rec->u = uv_angle(vsub(pt, p->center), ori);
+			rec->v = clamp01((vdot(vsub(pt, p->center), ori) / p->height) + 0.5);
+			uv_tile(s, rec->mat, rec);
+			hit_any = 1;
+		}
+	}
+	memset(&tmp, 0, sizeof(tmp));
+	if (cyl_cap(r, vsub(p->center, vscale(axis, p->height * 0.5)), ori, rad, vneg(ori), &tmp)
+		&& (!hit_any || tmp.t < rec->t))
+	{
+		tmp.mat = p->mat_bot >= 0 ? p->mat_bot : p->mat;
+		uv_cap(&tmp, vadd(p->center, vscale(ori, p->height * 0.5 * -1)), ori, p->diam);
+		uv_tile(s, tmp.mat, &tmp);
+		*rec = tmp;
+		hit_any = 1;
+	}
+	memset(&tmp, 0, sizeof(tmp));
+	if (cyl_cap(r, vadd(p->center, vscale(axis, p->height * 0.5)), ori, rad, ori, &tmp)
+		&& (!hit_any || tmp.t < rec->t))
+	{
+		tmp.mat = p->mat_top >= 0 ? p->mat_top : p->mat;
+		uv_cap(&tmp, vadd(p->center, vscale(ori, p->height * 0.5 * 1)), ori, p->diam);
+		uv_tile(s, tmp.mat, &tmp);
+		*rec = tmp;
+		hit_any = 1;
+	}
+	if (!hit_any)
+		return (0);
+	rec->front_face = (vdot(r->dir, rec->normal) < 0);
+	rec->normal = face(r, rec->normal, rec);
+	return (1);
+}
+
+/* hit_cone (hit_cone.c:108-129) with handle_cone_hit (:54-75), cone_cap
+ * (:77-106) and update_hit_cone (hit_obj.c:34-47) */
+static int hit_cone(ro_scene *s, prim_t *p, const ray_t *r, hrec_t *rec)
+{
+	v3		ori = p->ori;
+	v3		axis, oc, pt, n, cap;
+	double	k, dd, oo, t0, t1, th, proj, den, t, q;
+
+	if (ori.x == 0 && ori.y == 0 && ori.z == 0)
+		ori.y = 1;
+	k = pow((p->diam * 0.5) / p->height, 2);
+	oc = vsub(r->orig, p->center);
+	dd = vdot(r->dir, ori);
+	oo = vdot(oc, ori);
+	if (!solve_q(vdot(r->dir, r->dir) - (1.0 + k) * dd * dd, 2.0 * (vdot(r->dir, oc) - (1.0 + k) * dd * oo),
+			vdot(oc, oc) - (1.0 + k) * oo * oo, &t0, &t1) || !valid_root(t0, t1, &th))
+		return (0);
+	axis = vunit(ori);
+	pt = ray_at(*r, th);
+	proj = vdot(vsub(pt, p->center), axis);
+	if (!(proj < 0.0 || proj > p->height))
+	{
+		q = p->diam * 0.5 / p->height;
+		n = vunit(vsub(vsub(pt, p->center), vscale(axis, (1.0 + q * q) * proj)));
+		rec->t = th;
+		rec->point = pt;
+		rec->normal = face(r, n, rec);
+		rec->mat = p->mat;
+		rec->u = uv_angle(vsub(pt, p->center), ori);
+		rec->v = clamp01((vdot(vsub(pt, p->center), ori) / (p->height)));
+		uv_tile(s, rec->mat, rec);
+		return (1);
+	}
+	cap = vadd(p->center, vscale(axis, p->height));
+	den = vdot(r->dir, axis);
+	if (fabs(den) < 1e-6)
+		return (0);
+	t = vdot(vsub(cap, r->orig), axis) / den;
+	if (t < IT_MIN || t > IT_MAX)
+		return (0);
+	pt = ray_at(*r, t);
+	if (vlen(vsub(pt, cap)) > p->diam * 0.5)
+		return (0);
+	rec->t = t;
+	rec->point = pt;
+	rec->normal = axis;
+	rec->mat = p->mat_top >= 0 ? p->mat_top : p->mat;
+	uv_cap(rec, vadd(p->center, vscale(ori, p->height * 0.5)), ori, p->diam);
+	uv_tile(s, rec->mat, rec);
+	rec->front_face = (vdot(r->dir, rec->normal) < 0);
+	rec->normal = face(r, rec->normal, rec);
+	return (1);
+}
+
+/* hit_hyperboloid (hit_hyperboloid.c:80-104), init_hyperboloid_quadratic
+ * (quadratique_hyperboloid.c:15-63), compute_normal (hit_hyperboloid.c:36-52) */
+static int hyp_side(ro_scene *s, prim_t *p, const ray_t *r, double t, hrec_t *rec)
+{
+	v3		axis = vunit(p->ori);
+	v3		pt = ray_at(*r, t);
+	v3		to_p = vsub(pt, p->center);
+	v3		tmp, u, v, n;
+
+	if (!(fabs(vdot(to_p, axis)) <= p->height * 0.5))
+		return (0);
+	tmp = fabs(axis.y) < 0.99 ? (v3){0, 1, 0} : (v3){1, 0, 0};
+	u = vunit(vcross(tmp, axis));
+	v = vcross(axis, u);
+	n = vunit(vadd(vadd(vscale(u, 2.0 * vdot(to_p, u) / (p->qa * p->qa)),
+					vscale(v, 2.0 * vdot(to_p, v) / (p->qb * p->qb))),
+				vscale(axis, -2.0 * vdot(to_p, axis) / (p->qc * p->qc))));
+	rec->t = t;
+	rec->point = pt;
+	rec->normal = face(r, n, rec);
+	rec->front_face = vdot(r->dir, n) < 0;
+	rec->mat = p->mat;
+	rec->u = uv_angle(to_p, p->ori);
+	rec->v = clamp01((vdot(vsub(pt, p->center), p->ori) / (p->height * 0.5)) * 0.5 + 0.5);
+	uv_tile(s, p->mat, rec);
+	return (1);
+}
+
+static int hit_hyperboloid(ro_scene *s, prim_t *p, const ray_t *r, hrec_t *rec)
+{
+	v3		x, y, z, tmp, rel, ld, lo;
+	double	aa = p->qa * p->qa, bb = p->qb * p->qb, cc = p->qc * p->qc, t0, t1, imax = IT_MAX;
+	int		hit = 0;
+	prim_t	q = *p;
+
+	if (vlen2(q.ori) < 1e-6)
+		q.ori = (v3){0, 0, 1};
+	z = vunit(q.ori);
+	tmp = fabs(z.x) > 0.9 ? (v3){0, 1, 0} : (v3){1, 0, 0};
+	x = vunit(vcross(tmp, z));
+	y = vcross(z, x);
+	rel = vsub(r->orig, q.center);
+	ld = (v3){vdot(r->dir, x), vdot(r->dir, y), vdot(r->dir, z)};
+	lo = (v3){vdot(rel, x), vdot(rel, y), vdot(rel, z)};
+	if (!solve_q((ld.x * ld.x) / aa + (ld.y * ld.y) / bb - (ld.z * ld.z) / cc,
+			2.0 * ((ld.x * lo.x) / aa + (ld.y * lo.y) / bb - (ld.z * lo.z) / cc),
+			(lo.x * lo.x) / aa + (lo.y * lo.y) / bb - (lo.z * lo.z) / cc - q.shape, &t0, &t1))
+		return (0);
+	if (t0 > IT_MIN && t0 < imax && hyp_side(s, &q, r, t0, rec))
+	{
+		hit = 1;
+		imax = t0;
+	}
+	if (t1 > IT_MIN && t1 < imax && hyp_side(s, &q, r, t1, rec))
+		hit = 1;
+	return (hit);
+}
+
+static int hit_prim(ro_scene *s, prim_t *p, const ray_t *r, hrec_t *rec)
+{
+	if (p->type == PT_SPHERE)
+		return (hit_sphere(s, p, r, rec));
+	if (p->type == PT_TRI)
+		return (hit_triangle(s, p, r, rec));
+	if (p->type == PT_CYL)
+		return (hit_cylinder(s, p, r, rec));
+	if (p->type == PT_CONE)
+		return (hit_cone(s, p, r, rec));
+	return (hit_hyperboloid(s, p, r, rec));
+}
+
 /* hit_plane + get_uv_plane (hit_plane.c:18-71). */
 static int hit_plane(ro_scene *s, plane_t *p, const ray_t *r, hrec_t *rec)
 {
@@ -733,14 +1064,15 @@ static void bvh_closest(ro_scene *s, const ray_t *r, hrec_t *best, int *best_pos
 
 			s->cnt.prim_tests++;
 			memset(&tmp, 0, sizeof(tmp));
-			ok = p->type == PT_SPHERE ? hit_sphere(s, p, r, &tmp) : hit_triangle(s, p, r, &tmp);
+			ok = hit_prim(s, p, r, &tmp);
 			if (!ok || tmp.t >= 1000)
 				continue ;
 			if (!best->hit || tmp.t < best->t || (tmp.t == best->t && (int)nd->first < *best_pos))
 			{
 				tmp.hit = 1;
 				tmp.prim = s->prim_idx[nd->first];
-				tmp.mat = p->mat;
+				if (p->type == PT_SPHERE || p->type == PT_TRI)
+					tmp.mat = p->mat;
 				tmp.objcolor = p->color;
 				*best = tmp;
 				*best_pos = nd->first;
@@ -1844,10 +2176,11 @@ ro_scene	*ro_create(const mrt_scene_desc *d)
 		o->scale = m->scale;
 		o->emission_color = c2f(m->emission_color);
 	}
-	/* primitive order of bvh_make_lst (bvh_make_lst.c:46-65): spheres, then
-	 * one custom object per (mesh, material) in order of first appearance. */
+	/* primitive order of bvh_make_lst (bvh_make_lst.c:46-65) over the object
+	 * list spheres, cylinders, cones, hyperboloids, then one custom object
+	 * per (mesh, material) in order of first appearance. */
 	{
-		size_t	total = d->n_spheres;
+		size_t	total = d->n_spheres + (size_t)d->n_cylinders + d->n_cones + d->n_hyperboloids;
 
 		for (int i = 0; i < d->n_meshes; i++)
 			total += d->meshes[i].n_triangles;
@@ -1865,8 +2198,58 @@ ro_scene	*ro_create(const mrt_scene_desc *d)
 		p->radius = (d->spheres[i].radius * 2.0) * 0.5;
 		p->r2 = p->radius * p->radius;
 	}
+	for (int i = 0; i < d->n_cylinders; i++)
 	{
-		uint32_t	flat = d->n_spheres;
+		const mrt_cylinder	*c = &d->cylinders[i];
+		prim_t				*p = &s->prims[np++];
+
+		p->type = PT_CYL;
+		p->flat = d->n_spheres + i;
+		p->mat = mat_or_none(c->material, d->n_materials);
+		p->mat_top = mat_or_none(c->material_top, d->n_materials);
+		p->mat_bot = mat_or_none(c->material_bot, d->n_materials);
+		memcpy(p->color, c->color, 3);
+		p->center = a3(c->position);
+		p->ori = a3(c->orientation);
+		p->diam = c->diameter;
+		p->height = c->height;
+	}
+	for (int i = 0; i < d->n_cones; i++)
+	{
+		const mrt_cone	*c = &d->cones[i];
+		prim_t			*p = &s->prims[np++];
+
+		p->type = PT_CONE;
+		p->flat = d->n_spheres + d->n_cylinders + i;
+		p->mat = mat_or_none(c->material, d->n_materials);
+		p->mat_top = mat_or_none(c->material_top, d->n_materials);
+		p->mat_bot = -1;
+		memcpy(p->color, c->color, 3);
+		p->center = a3(c->position);
+		p->ori = a3(c->orientation);
+		p->diam = c->diameter;
+		p->height = c->height;
+	}
+	for (int i = 0; i < d->n_hyperboloids; i++)
+	{
+		const mrt_hyperboloid	*c = &d->hyperboloids[i];
+		prim_t					*p = &s->prims[np++];
+
+		p->type = PT_HYP;
+		p->flat = d->n_spheres + d->n_cylinders + d->n_cones + i;
+		p->mat = mat_or_none(c->material, d->n_materials);
+		p->mat_top = p->mat_bot = -1;
+		memcpy(p->color, c->color, 3);
+		p->center = a3(c->position);
+		p->ori = a3(c->orientation);
+		p->qa = c->a;
+		p->qb = c->b;
+		p->qc = c->c;
+		p->shape = c->shape;
+		p->height = c->height;
+	}
+	{
+		uint32_t	flat = d->n_spheres + d->n_cylinders + d->n_cones + d->n_hyperboloids;
 
 		for (int mi = 0; mi < d->n_meshes; mi++)
 		{

@@ -40,6 +40,7 @@ typedef struct s_refh
 	t_minirt			*m;
 	int					n_spheres;
 	int					n_tris;
+	int					tri_base;     /* flat id of the first triangle */
 	int					n_planes;
 	int					*elem_flat;    /* element index -> flat prim id (spheres/planes) */
 	int					n_groups;
@@ -239,6 +240,7 @@ void	*refh_create(const mrt_scene_desc *d)
 	t_scene		*sc;
 	int			el;
 	int			ngroups;
+	int			nquad;
 	uint32_t	flat_base;
 
 	if (!d || d->abi_version != MRT_ABI_VERSION || d->render_width <= 0
@@ -257,9 +259,10 @@ void	*refh_create(const mrt_scene_desc *d)
 	for (int i = 0; i < d->n_meshes; i++)
 		ngroups += count_groups(&d->meshes[i]);
 	h->groups = calloc(ngroups + 1, sizeof(t_refh_mesh_group));
-	sc->elements = calloc(d->n_spheres + ngroups + d->n_planes + d->n_lights + 1,
+	nquad = d->n_cylinders + d->n_cones + d->n_hyperboloids;
+	sc->elements = calloc(d->n_spheres + nquad + ngroups + d->n_planes + d->n_lights + 1,
 			sizeof(t_object));
-	h->elem_flat = calloc(d->n_spheres + ngroups + d->n_planes + d->n_lights + 1,
+	h->elem_flat = calloc(d->n_spheres + nquad + ngroups + d->n_planes + d->n_lights + 1,
 			sizeof(int));
 	el = 0;
 	for (int i = 0; i < d->n_spheres; i++)
@@ -276,13 +279,64 @@ void	*refh_create(const mrt_scene_desc *d)
 		h->elem_flat[el++] = i;
 	}
 	h->n_spheres = d->n_spheres;
-	flat_base = d->n_spheres;
+	/* the element list is spheres, cylinders, cones, hyperboloids, meshes,
+	 * planes, lights: bvh_make_lst keeps that order for the BVH objects */
+	for (int i = 0; i < d->n_cylinders; i++)
+	{
+		const mrt_cylinder *c = &d->cylinders[i];
+		t_cylinder *o = calloc(1, sizeof(t_cylinder));
+		o->position = v3(c->position);
+		o->orientation = v3(c->orientation);
+		o->diameter = c->diameter;
+		o->height = c->height;
+		o->material = mat_ptr(sc, c->material);
+		o->material_top = mat_ptr(sc, c->material_top);
+		o->material_bot = mat_ptr(sc, c->material_bot);
+		o->color = c3(c->color);
+		sc->elements[el].object = o;
+		sc->elements[el].type = CYLINDER;
+		h->elem_flat[el++] = d->n_spheres + i;
+	}
+	for (int i = 0; i < d->n_cones; i++)
+	{
+		const mrt_cone *c = &d->cones[i];
+		t_cone *o = calloc(1, sizeof(t_cone));
+		o->position = v3(c->position);
+		o->orientation = v3(c->orientation);
+		o->diameter = c->diameter;
+		o->height = c->height;
+		o->material = mat_ptr(sc, c->material);
+		o->material_top = mat_ptr(sc, c->material_top);
+		o->color = c3(c->color);
+		sc->elements[el].object = o;
+		sc->elements[el].type = CONE;
+		h->elem_flat[el++] = d->n_spheres + d->n_cylinders + i;
+	}
+	for (int i = 0; i < d->n_hyperboloids; i++)
+	{
+		const mrt_hyperboloid *c = &d->hyperboloids[i];
+		t_hyperboloid *o = calloc(1, sizeof(t_hyperboloid));
+		o->position = v3(c->position);
+		o->orientation = v3(c->orientation);
+		o->a = c->a;
+		o->b = c->b;
+		o->c = c->c;
+		o->shape = c->shape;
+		o->height = c->height;
+		o->material = mat_ptr(sc, c->material);
+		o->color = c3(c->color);
+		sc->elements[el].object = o;
+		sc->elements[el].type = HYPERBOLOID;
+		h->elem_flat[el++] = d->n_spheres + d->n_cylinders + d->n_cones + i;
+	}
+	flat_base = d->n_spheres + nquad;
 	for (int i = 0; i < d->n_meshes; i++)
 	{
 		add_mesh_groups(h, &d->meshes[i], flat_base, &el);
 		flat_base += d->meshes[i].n_triangles;
 	}
-	h->n_tris = flat_base - d->n_spheres;
+	h->tri_base = d->n_spheres + nquad;
+	h->n_tris = flat_base - h->tri_base;
 	for (int i = 0; i < d->n_planes; i++)
 	{
 		t_plane *p = calloc(1, sizeof(t_plane));
@@ -571,7 +625,7 @@ int	refh_triangle_positions(void *hv, double *out)
 		t_custom_object *o = h->groups[g].obj;
 		for (size_t k = 0; k < o->triangle_count; k++)
 		{
-			double *p = out + 9 * (size_t)(h->groups[g].flat_tri[k] - h->n_spheres);
+			double *p = out + 9 * (size_t)(h->groups[g].flat_tri[k] - h->tri_base);
 			t_triangle *t = &o->triangles[k];
 			p[0] = t->v0.pos.x; p[1] = t->v0.pos.y; p[2] = t->v0.pos.z;
 			p[3] = t->v1.pos.x; p[4] = t->v1.pos.y; p[5] = t->v1.pos.z;

@@ -7,7 +7,7 @@ oracle/_ref/liboracle_ref.so, on small seeded scenes:
   * float_render after N samples of calc_one_sample with a fixed RNG state,
   * HDRI tables of make_importance_sampling_map,
   * the photon map of caustic_manager and kNN caustic estimates.
-Run here (where the reference is mounted):  python tests/golden/make_golden.py
+Run here (where the reference is mounted):  python tests/golden/make_golden.py [case ...]
 The GPU box has no reference; tests there read these files.
 """
 from __future__ import annotations
@@ -29,6 +29,7 @@ CASES = {
     "c0": dict(make=lambda: scenes.make_c0(0, 32, 24, depth=8), spp=4),
     "c1": dict(make=lambda: scenes.make_c1(1, 24, 16, depth=6, freq=12, sky=(48, 24)), spp=2),
     "c2": dict(make=lambda: scenes.make_c2(2, 24, 16, depth=6, grid=16, photons=3000), spp=2),
+    "q0": dict(make=lambda: scenes.make_quadrics(5, 32, 24, depth=6), spp=4),
 }
 
 
@@ -40,6 +41,8 @@ def scene_digest(sc) -> str:
         h.update(repr(s).encode())
     for p in sc.planes:
         h.update(repr(p).encode())
+    for q in sc.cylinders + sc.cones + sc.hyperboloids:
+        h.update(repr(sorted(q.items())).encode())
     for m in sc.meshes:
         for a in (m.positions, m.normals, m.indices, m.tri_material):
             if a is not None:
@@ -65,8 +68,10 @@ def rays_for(ref, n=4096, seed=0):
     return o, d
 
 
-def main():
+def main(names=None):
     for name, case in CASES.items():
+        if names and name not in names:
+            continue
         sc = case["make"]()
         oracle.ref_lib().refh_set_seed(4242)
         ref = oracle.RefOracle(sc)
@@ -97,4 +102,4 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -42,7 +42,8 @@ def test_library_loads_and_exports_every_declared_symbol(mrt):
 
 def test_ctypes_layouts_match_c(mrt):
     structs = {"mrt_material": mrt.Material, "mrt_sphere": mrt.Sphere, "mrt_plane": mrt.Plane,
-               "mrt_mesh": mrt.Mesh, "mrt_light": mrt.Light, "mrt_camera": mrt.Camera,
+               "mrt_mesh": mrt.Mesh, "mrt_cylinder": mrt.Cylinder, "mrt_cone": mrt.Cone,
+               "mrt_hyperboloid": mrt.Hyperboloid, "mrt_light": mrt.Light, "mrt_camera": mrt.Camera,
                "mrt_ambient": mrt.Ambient, "mrt_caustic": mrt.Caustic,
                "mrt_scene_desc": mrt.SceneDesc, "mrt_render_params": mrt.RenderParams,
                "mrt_render_stats": mrt.RenderStats, "mrt_ray": mrt.Ray, "mrt_hit": mrt.Hit,
@@ -52,6 +53,7 @@ def test_ctypes_layouts_match_c(mrt):
         src += f'  printf("{name} %zu\\n", sizeof({name}));\n'
     src += '  printf("off_scene_materials %zu\\n", offsetof(mrt_scene_desc, materials));\n'
     src += '  printf("off_scene_lights %zu\\n", offsetof(mrt_scene_desc, lights));\n'
+    src += '  printf("off_scene_hyperboloids %zu\\n", offsetof(mrt_scene_desc, hyperboloids));\n'
     src += "  return 0;}\n"
     with tempfile.TemporaryDirectory() as d:
         c = Path(d) / "sizes.c"
@@ -64,6 +66,7 @@ def test_ctypes_layouts_match_c(mrt):
         assert int(got[name]) == C.sizeof(cls), name
     assert int(got["off_scene_materials"]) == mrt.SceneDesc.materials.offset
     assert int(got["off_scene_lights"]) == mrt.SceneDesc.lights.offset
+    assert int(got["off_scene_hyperboloids"]) == mrt.SceneDesc.hyperboloids.offset
 
 
 def test_null_context_is_rejected_with_invalid(mrt):
