@@ -48,6 +48,7 @@
 // integers, light_manager.c:103) and the photon estimate (treated as a
 // constant field).
 #include <algorithm>
+#include <type_traits>
 
 #include "dual.cuh"
 #include "kernels.h"
@@ -66,6 +67,7 @@ enum TapeFlags : int {
   TF_EMIT = 8,
   TF_NEE = 16,         // HDRI NEE contributed (visible, pdf > 0)
   TF_GGX = 32,         // a GGX sample was drawn (roughness > 0)
+  TF_PART_SHIFT = 6,   // bits 6-7: part of a quadric hit (QuadricPart)
 };
 enum Branch : int { BR_DIFFUSE = 0, BR_METAL = 1, BR_REFLECT = 2, BR_REFRACT = 3 };
 
@@ -80,14 +82,66 @@ __device__ __forceinline__ V3T<D7> dunit(const V3T<D7>& a) {
 }
 __device__ __forceinline__ D7 dot_c(const V3T<D7>& a, float3 w) { return a.x * w.x + a.y * w.y + a.z * w.z; }
 
+// Outward normal of a quadric part at p (quadric_surf's formulas, before
+// facing): the lateral normals depend on p, the caps' do not.
+__device__ __forceinline__ V3T<D7> quadric_normal_dual(int type, int part, const float4& a, const float4& b,
+                                                       const float4& c, const V3T<D7>& p) {
+  const float3 pos = f3(a.x, a.y, a.z), ori = f3(b.x, b.y, b.z), axis = unit(ori);
+  if (type == PRIM_CYL) {
+    if (part == PART_TOP) return dv3(ori);
+    if (part == PART_BOTTOM) return dv3(-ori);
+    const V3T<D7> q = p - dv3(pos - axis * (c.x * 0.5f));
+    return dunit(q - dv3(axis) * dot_c(q, axis));
+  }
+  if (type == PRIM_CONE) {
+    if (part != PART_SIDE) return dv3(axis);
+    const float rr = b.w / c.x;
+    const V3T<D7> q = p - dv3(pos);
+    return dunit(q - dv3(axis) * (dot_c(q, axis) * (1.0f + rr * rr)));
+  }
+  const float3 tmp = fabsf(axis.y) < 0.99f ? f3(0.f, 1.f, 0.f) : f3(1.f, 0.f, 0.f);
+  const float3 u = unit(cross(tmp, axis));
+  const float3 v = cross(axis, u);
+  const V3T<D7> q = p - dv3(pos);
+  return dunit(dv3(u) * (dot_c(q, u) * (2.0f / (b.w * b.w))) + dv3(v) * (dot_c(q, v) * (2.0f / (c.x * c.x))) -
+               dv3(axis) * (dot_c(q, axis) * (2.0f / (c.y * c.y))));
+}
+
 // Hit point and shading normal of a known primitive for the ray (o, d):
-// make_surf's formulas with t (and u, v) recomputed from the ray.
-__device__ __forceinline__ void surf_dual(const SceneView& S, int prim, float t_rec, int front,
+// make_surf's formulas with t (and u, v) recomputed from the ray. For a
+// quadric, t follows the implicit surface F(o + t d) = 0 to first order:
+// dt = -N . (do + t dd) / (N . d) with N the normal at the recorded hit,
+// which is the derivative of t through the tangent plane there; the value
+// of t stays the recorded one.
+template <class V>
+__device__ __forceinline__ void surf_dual(const V& S, int prim, float t_rec, int flags,
                                           const V3T<D7>& o, const V3T<D7>& d, V3T<D7>& p, V3T<D7>& n) {
+  const int front = (flags & TF_FRONT) != 0;
   if (prim >= 0) {
     const float4* g = S.geom + 3 * (size_t)prim;
     const float4 a = __ldg(g), b = __ldg(g + 1);
-    if (__float_as_int(a.w) == PRIM_TRI) {
+    const int type = __float_as_int(a.w);
+    if constexpr (V::kQuadrics) {
+      if (type >= PRIM_CYL) {
+        const float4 c = __ldg(g + 2);
+        const int part = (flags >> TF_PART_SHIFT) & 3;
+        const float3 o0 = f3(o.x.v, o.y.v, o.z.v), d0 = f3(d.x.v, d.y.v, d.z.v);
+        const float3 p0 = o0 + d0 * t_rec;
+        const V3T<D7> n0 = quadric_normal_dual(type, part, a, b, c, dv3(p0));
+        const float3 N = f3(n0.x.v, n0.y.v, n0.z.v);
+        D7 t = dot_c(dv3(p0) - o, N) / dot_c(d, N);
+        t.v = t_rec;
+        p = o + d * t;
+        const V3T<D7> out = quadric_normal_dual(type, part, a, b, c, p);
+        // the cylinder's lateral normal faces the ray with front_face 1
+        const bool keep = (type == PRIM_CYL && part == PART_SIDE)
+                              ? (d.x.v * out.x.v + d.y.v * out.y.v + d.z.v * out.z.v) < 0.0f
+                              : front != 0;
+        n = keep ? out : -out;
+        return;
+      }
+    }
+    if (type == PRIM_TRI) {
       const float4 c = __ldg(g + 2);
       const V3T<D7> v0 = dv3(a.x, a.y, a.z), e1 = dv3(b.x, b.y, b.z), e2 = dv3(c.x, c.y, c.z);
       const V3T<D7> h = vcross(d, e2);
@@ -179,7 +233,8 @@ __device__ __forceinline__ void record_pair(const Rng& r, Rec& rec) {
 }
 
 // default_mat (material_default.c:71-92), recording.
-__device__ __forceinline__ void default_rec(const SceneView& S, PathState& P, const Surf& s, int* status,
+template <class V>
+__device__ __forceinline__ void default_rec(const V& S, PathState& P, const Surf& s, int* status,
                                             PathCounters& C, Rec& rec) {
   const float3 direct = compute_light(S, P.rng, s, status, C.shadow);
   const float3 total = direct + caustic_estimate(S, s.p);
@@ -231,7 +286,8 @@ __device__ __forceinline__ void refract_rec(const SceneView& S, const MaterialD&
 }
 
 // material_manager_v3 (path_trace.c:15-35) + dielectric_mat (dielectric.c:37-64).
-__device__ __forceinline__ void material_rec(const SceneView& S, PathState& P, const Surf& s, int* status,
+template <class V>
+__device__ __forceinline__ void material_rec(const V& S, PathState& P, const Surf& s, int* status,
                                              PathCounters& C, Rec& rec) {
   if (s.mat < 0) { default_rec(S, P, s, status, C, rec); return; }
   const MaterialD& M = S.mats[s.mat];
@@ -293,7 +349,8 @@ struct MatGrad {
 
 // One reverse step: the adjoint state (Pb, ob, db) after bounce k becomes
 // the state before it; gradients of the bounce's parameters are added.
-__device__ __forceinline__ void reverse_step(const SceneView& S, const AdjointArgs& A, MatGrad& G,
+template <class V>
+__device__ __forceinline__ void reverse_step(const V& S, const AdjointArgs& A, MatGrad& G,
                                              const TapeEntry& te, float3 g, float inv_col, float3& Pb,
                                              float3& ob, float3& db, float& gcol) {
   const float lw[3] = {0.2126f, 0.7152f, 0.0722f};
@@ -310,7 +367,7 @@ __device__ __forceinline__ void reverse_step(const SceneView& S, const AdjointAr
   const V3T<D7> o{D7::seed(te.o_t.x, 0), D7::seed(te.o_t.y, 1), D7::seed(te.o_t.z, 2)};
   const V3T<D7> d{D7::seed(te.d_ra.x, 3), D7::seed(te.d_ra.y, 4), D7::seed(te.d_ra.z, 5)};
   V3T<D7> p, n;
-  surf_dual(S, prim, te.o_t.w, (flags & TF_FRONT) != 0, o, d, p, n);
+  surf_dual(S, prim, te.o_t.w, flags, o, d, p, n);
   // phi = ob . p + db . next_direction + (scalar weights) . (cosines)
   D7 phi = dot_c(p, ob);
   float3 a = f3(0.f, 0.f, 0.f);   // radiance added per unit power: c_k = P_k * a
@@ -425,8 +482,8 @@ __device__ __forceinline__ void finish_path(const SceneView& S, const AdjointArg
 // Replay: the paths of the forward again (persistent, lanes regenerate
 // paths as in the regenerating megakernel), writing one tape entry per
 // bounce to tape[k * n_paths + path].
-template <int kBlock>
-__global__ void __launch_bounds__(kBlock) adj_replay_kernel(SceneView S, AdjointArgs A, TapeEntry* tape,
+template <int kBlock, class V>
+__global__ void __launch_bounds__(kBlock) adj_replay_kernel(V S, AdjointArgs A, TapeEntry* tape,
                                                             float4* state, int* status,
                                                             unsigned long long* work) {
   const uint32_t npix = (uint32_t)S.width * (uint32_t)S.height;
@@ -482,7 +539,10 @@ __global__ void __launch_bounds__(kBlock) adj_replay_kernel(SceneView S, Adjoint
         const Surf s = make_surf(S, h, P.o, P.d, 0);
         TapeEntry te;
         te.o_t = make_float4(P.o.x, P.o.y, P.o.z, h.t);
-        Rec rec{s.front ? (int)TF_FRONT : 0, 0.f, 0.f, -1, f3(0.f, 0.f, 0.f)};
+        int fl = s.front ? (int)TF_FRONT : 0;
+        if (V::kQuadrics && h.prim >= 0 && __ldg(S.meta + h.prim).z >= PRIM_CYL)
+          fl |= ((int)h.u) << TF_PART_SHIFT;
+        Rec rec{fl, 0.f, 0.f, -1, f3(0.f, 0.f, 0.f)};
         const float3 d0 = P.d, p0 = P.power;
         P.o = s.p;
         P.last_mat = s.mat;
@@ -504,8 +564,8 @@ __global__ void __launch_bounds__(kBlock) adj_replay_kernel(SceneView S, Adjoint
 }
 
 // Reverse sweep of bounce level k for every path that reached it.
-template <int kBlock>
-__global__ void __launch_bounds__(kBlock) adj_level_kernel(SceneView S, AdjointArgs A, const TapeEntry* tape,
+template <int kBlock, class V>
+__global__ void __launch_bounds__(kBlock) adj_level_kernel(V S, AdjointArgs A, const TapeEntry* tape,
                                                            float4* state, int k) {
   extern __shared__ float smem[];
   MatGrad G{smem, A.n_mats};
@@ -651,21 +711,24 @@ cudaError_t launch_adjoint_chunk(const SceneView& S, const AdjointArgs& A, TapeE
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaError_t e = cudaMemsetAsync(work, 0, sizeof(unsigned long long), st);
   if (e != cudaSuccess) return e;
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, adj_replay_kernel<kBlock>, kBlock, 0);
-  if (e != cudaSuccess) return e;
-  const uint64_t want = (A.n_paths + kBlock - 1) / kBlock;
-  unsigned grid = (unsigned)std::min<uint64_t>((uint64_t)sms * std::max(occ, 1), want);
-  adj_replay_kernel<kBlock><<<grid, kBlock, 0, st>>>(S, A, tape, state, status, work);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  const size_t smem = (size_t)5 * A.n_mats * sizeof(float);
-  e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, adj_level_kernel<kBlock>, kBlock, smem);
-  if (e != cudaSuccess) return e;
-  grid = (unsigned)std::min<uint64_t>((uint64_t)sms * std::max(occ, 1), want);
-  for (int k = A.max_bounces - 1; k >= 0; --k) {
-    adj_level_kernel<kBlock><<<grid, kBlock, smem, st>>>(S, A, tape, state, k);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-  }
-  return cudaSuccess;
+  return with_view(S, [&](const auto& v) -> cudaError_t {
+    using VT = std::decay_t<decltype(v)>;
+    cudaError_t e2 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, adj_replay_kernel<kBlock, VT>, kBlock, 0);
+    if (e2 != cudaSuccess) return e2;
+    const uint64_t want = (A.n_paths + kBlock - 1) / kBlock;
+    unsigned grid = (unsigned)std::min<uint64_t>((uint64_t)sms * std::max(occ, 1), want);
+    adj_replay_kernel<kBlock, VT><<<grid, kBlock, 0, st>>>(v, A, tape, state, status, work);
+    if ((e2 = cudaGetLastError()) != cudaSuccess) return e2;
+    const size_t smem = (size_t)5 * A.n_mats * sizeof(float);
+    e2 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, adj_level_kernel<kBlock, VT>, kBlock, smem);
+    if (e2 != cudaSuccess) return e2;
+    grid = (unsigned)std::min<uint64_t>((uint64_t)sms * std::max(occ, 1), want);
+    for (int k = A.max_bounces - 1; k >= 0; --k) {
+      adj_level_kernel<kBlock, VT><<<grid, kBlock, smem, st>>>(v, A, tape, state, k);
+      if ((e2 = cudaGetLastError()) != cudaSuccess) return e2;
+    }
+    return cudaSuccess;
+  });
 }
 
 cudaError_t launch_diff_sky_mean(const AdjointArgs& A, cudaStream_t st) {

@@ -447,10 +447,13 @@ extern "C" int mrt_scene_build(mrt_ctx* c, const mrt_scene_desc* d) {
   if (d->render_width != c->W || d->render_height != c->H)
     return set_err(MRT_ERR_INVALID, "scene size %dx%d does not match the context %dx%d",
                    d->render_width, d->render_height, c->W, c->H);
-  if (d->n_materials < 0 || d->n_spheres < 0 || d->n_planes < 0 || d->n_meshes < 0 || d->n_lights < 0)
+  if (d->n_materials < 0 || d->n_spheres < 0 || d->n_planes < 0 || d->n_meshes < 0 || d->n_lights < 0 ||
+      d->n_cylinders < 0 || d->n_cones < 0 || d->n_hyperboloids < 0)
     return set_err(MRT_ERR_INVALID, "negative element count");
   if ((d->n_materials && !d->materials) || (d->n_spheres && !d->spheres) ||
-      (d->n_planes && !d->planes) || (d->n_meshes && !d->meshes) || (d->n_lights && !d->lights))
+      (d->n_planes && !d->planes) || (d->n_meshes && !d->meshes) || (d->n_lights && !d->lights) ||
+      (d->n_cylinders && !d->cylinders) || (d->n_cones && !d->cones) ||
+      (d->n_hyperboloids && !d->hyperboloids))
     return set_err(MRT_ERR_INVALID, "null element array with a non-zero count");
   c->has_scene = false;
   if (c->diff) {
@@ -488,7 +491,8 @@ extern "C" int mrt_scene_build(mrt_ctx* c, const mrt_scene_desc* d) {
     o.alpha4 = (float)((rough * rough) * (rough * rough));
   }
 
-  // primitives: spheres then triangles (flat ids), double boxes -> float
+  // primitives in flat-id order: spheres, cylinders, cones, hyperboloids,
+  // triangles; double boxes -> float
   size_t n_tris = 0;
   for (int i = 0; i < d->n_meshes; ++i) {
     const mrt_mesh& me = d->meshes[i];
@@ -502,7 +506,9 @@ extern "C" int mrt_scene_build(mrt_ctx* c, const mrt_scene_desc* d) {
       return set_err(MRT_ERR_INVALID, "mesh %d has too few vertices for implicit indices", i);
     n_tris += me.n_triangles;
   }
-  const size_t n_prims = (size_t)d->n_spheres + n_tris;
+  const size_t q_cyl = (size_t)d->n_spheres, q_cone = q_cyl + d->n_cylinders;
+  const size_t q_hyp = q_cone + d->n_cones, tri_base = q_hyp + d->n_hyperboloids;
+  const size_t n_prims = tri_base + n_tris;
   std::vector<PrimBox> boxes(n_prims);
   struct TriRef { const mrt_mesh* m; uint32_t t; };
   std::vector<TriRef> tris;
@@ -517,8 +523,60 @@ extern "C" int mrt_scene_build(mrt_ctx* c, const mrt_scene_desc* d) {
     for (int k = 0; k < 3; ++k) { mn[k] = s.center[k] - r; mx[k] = s.center[k] + r; }
     prim_box_from_double(boxes[i], mn, mx);
   }
+  // quadric bounds as bvh_obj_bounds.c computes them (axis-aligned extents of
+  // the end discs, :41-96); a zero orientation takes the default the hit
+  // functions give it (+y for cylinders and cones, +z for hyperboloids)
+  auto finite3 = [](const double* q) { return std::isfinite(q[0]) && std::isfinite(q[1]) && std::isfinite(q[2]); };
+  auto axis_of = [](const double* o, double dz, V3& axis) {
+    V3 a = v3(o);
+    if (a.x == 0 && a.y == 0 && a.z == 0) a = dz ? V3{0, 0, 1} : V3{0, 1, 0};
+    axis = unitv(a);
+  };
+  auto disc_box = [&](size_t idx, const V3& p0, const V3& p1, const V3& a, double r) {
+    const double e[3] = {r * std::sqrt(std::max(0.0, 1.0 - a.x * a.x)), r * std::sqrt(std::max(0.0, 1.0 - a.y * a.y)),
+                         r * std::sqrt(std::max(0.0, 1.0 - a.z * a.z))};
+    const double lo[3] = {std::min(p0.x, p1.x), std::min(p0.y, p1.y), std::min(p0.z, p1.z)};
+    const double hi[3] = {std::max(p0.x, p1.x), std::max(p0.y, p1.y), std::max(p0.z, p1.z)};
+    double mn[3], mx[3];
+    for (int k = 0; k < 3; ++k) { mn[k] = lo[k] - e[k]; mx[k] = hi[k] + e[k]; }
+    prim_box_from_double(boxes[idx], mn, mx);
+  };
+  for (int i = 0; i < d->n_cylinders; ++i) {
+    const mrt_cylinder& q = d->cylinders[i];
+    if (!finite3(q.position) || !finite3(q.orientation) || !(q.diameter >= 0) || !(q.height >= 0) ||
+        !std::isfinite(q.diameter) || !std::isfinite(q.height))
+      return set_err(MRT_ERR_INVALID, "cylinder %d is not finite or has a negative size", i);
+    V3 a;
+    axis_of(q.orientation, 0, a);
+    const V3 c = v3(q.position), h = mul(a, q.height * 0.5);
+    disc_box(q_cyl + i, sub(c, h), add(c, h), a, q.diameter * 0.5);
+  }
+  for (int i = 0; i < d->n_cones; ++i) {
+    const mrt_cone& q = d->cones[i];
+    if (!finite3(q.position) || !finite3(q.orientation) || !(q.diameter >= 0) || !(q.height > 0) ||
+        !std::isfinite(q.diameter) || !std::isfinite(q.height))
+      return set_err(MRT_ERR_INVALID, "cone %d is not finite or has a non-positive height", i);
+    V3 a;
+    axis_of(q.orientation, 0, a);
+    const V3 c = v3(q.position);
+    disc_box(q_cone + i, c, add(c, mul(a, q.height)), a, q.diameter * 0.5);
+  }
+  for (int i = 0; i < d->n_hyperboloids; ++i) {
+    const mrt_hyperboloid& q = d->hyperboloids[i];
+    if (!finite3(q.position) || !finite3(q.orientation) || !std::isfinite(q.a) || !std::isfinite(q.b) ||
+        !std::isfinite(q.c) || !std::isfinite(q.shape) || !(q.height >= 0) || !std::isfinite(q.height) ||
+        q.a == 0 || q.b == 0 || q.c == 0)
+      return set_err(MRT_ERR_INVALID, "hyperboloid %d is not finite or has a zero semi-axis", i);
+    V3 a = v3(q.orientation);
+    a = (a.x * a.x + a.y * a.y + a.z * a.z) < 1e-6 ? V3{0, 0, 1} : unitv(a);
+    const V3 c = v3(q.position), h = mul(a, q.height * 0.5);
+    const double hh = q.height * 0.5;
+    const double rmax = std::max(std::fabs(q.a), std::fabs(q.b)) *
+                        std::sqrt(std::max(0.0, q.shape + (hh * hh) / (q.c * q.c)));
+    disc_box(q_hyp + i, sub(c, h), add(c, h), a, rmax);
+  }
   {
-    size_t p = d->n_spheres;
+    size_t p = tri_base;
     for (int i = 0; i < d->n_meshes; ++i) {
       const mrt_mesh& me = d->meshes[i];
       for (uint32_t t = 0; t < me.n_triangles; ++t, ++p) {
@@ -547,9 +605,45 @@ extern "C" int mrt_scene_build(mrt_ctx* c, const mrt_scene_desc* d) {
   std::vector<float4> geom(3 * std::max<size_t>(n_prims, 1));
   std::vector<int4> meta(std::max<size_t>(n_prims, 1));
   std::vector<float4> shade(4 * std::max<size_t>(n_prims, 1));
+  auto mat_or = [&](int32_t m) { return (m >= 0 && m < d->n_materials) ? m : -1; };
   for (size_t k = 0; k < n_prims; ++k) {
     const uint32_t src = bvh.order[k];
-    if (src < (uint32_t)d->n_spheres) {
+    if (src >= q_cyl && src < tri_base) {
+      // quadric records: (position, type) (orientation as given, radius or a) (...)
+      const float f0 = 0.f;
+      if (src < q_cone) {
+        const mrt_cylinder& q = d->cylinders[src - q_cyl];
+        V3 o = v3(q.orientation);
+        if (o.x == 0 && o.y == 0 && o.z == 0) o = V3{0, 1, 0};
+        geom[3 * k] = make_float4((float)q.position[0], (float)q.position[1], (float)q.position[2],
+                                  int_bits_as_float(PRIM_CYL));
+        geom[3 * k + 1] = make_float4((float)o.x, (float)o.y, (float)o.z, (float)(q.diameter * 0.5));
+        geom[3 * k + 2] = make_float4((float)q.height, int_bits_as_float(mat_or(q.material_top)),
+                                      int_bits_as_float(mat_or(q.material_bot)), f0);
+        meta[k] = make_int4((int)src, q.material < d->n_materials ? q.material : -1, PRIM_CYL,
+                            (int)pack_color(q.color));
+      } else if (src < q_hyp) {
+        const mrt_cone& q = d->cones[src - q_cone];
+        V3 o = v3(q.orientation);
+        if (o.x == 0 && o.y == 0 && o.z == 0) o = V3{0, 1, 0};
+        geom[3 * k] = make_float4((float)q.position[0], (float)q.position[1], (float)q.position[2],
+                                  int_bits_as_float(PRIM_CONE));
+        geom[3 * k + 1] = make_float4((float)o.x, (float)o.y, (float)o.z, (float)(q.diameter * 0.5));
+        geom[3 * k + 2] = make_float4((float)q.height, int_bits_as_float(mat_or(q.material_top)), f0, f0);
+        meta[k] = make_int4((int)src, q.material < d->n_materials ? q.material : -1, PRIM_CONE,
+                            (int)pack_color(q.color));
+      } else {
+        const mrt_hyperboloid& q = d->hyperboloids[src - q_hyp];
+        V3 o = v3(q.orientation);
+        if (o.x * o.x + o.y * o.y + o.z * o.z < 1e-6) o = V3{0, 0, 1};
+        geom[3 * k] = make_float4((float)q.position[0], (float)q.position[1], (float)q.position[2],
+                                  int_bits_as_float(PRIM_HYP));
+        geom[3 * k + 1] = make_float4((float)o.x, (float)o.y, (float)o.z, (float)q.a);
+        geom[3 * k + 2] = make_float4((float)q.b, (float)q.c, (float)q.shape, (float)q.height);
+        meta[k] = make_int4((int)src, q.material < d->n_materials ? q.material : -1, PRIM_HYP,
+                            (int)pack_color(q.color));
+      }
+    } else if (src < (uint32_t)d->n_spheres) {
       const mrt_sphere& s = d->spheres[src];
       const double r = (s.radius * 2.0) * 0.5;
       geom[3 * k] = make_float4((float)s.center[0], (float)s.center[1], (float)s.center[2],
@@ -559,7 +653,7 @@ extern "C" int mrt_scene_build(mrt_ctx* c, const mrt_scene_desc* d) {
       const int mat = s.material < d->n_materials ? s.material : -1;
       meta[k] = make_int4((int)src, mat, PRIM_SPHERE, (int)pack_color(s.color));
     } else {
-      const TriRef& tr = tris[src - d->n_spheres];
+      const TriRef& tr = tris[src - tri_base];
       const mrt_mesh& me = *tr.m;
       uint32_t vi[3];
       for (int cidx = 0; cidx < 3; ++cidx)
@@ -634,6 +728,7 @@ extern "C" int mrt_scene_build(mrt_ctx* c, const mrt_scene_desc* d) {
   v.n_mats = d->n_materials;
   v.n_lights = d->n_lights;
   v.has_bvh = n_prims > 0;
+  v.has_quadrics = (d->n_cylinders + d->n_cones + d->n_hyperboloids) > 0;
   v.root_leaf = bvh.root_leaf;
   set_viewport(v, d->camera, c->W, c->H);
 
@@ -953,7 +1048,10 @@ extern "C" int mrt_render_batch(mrt_ctx** ctxs, const mrt_render_params* params,
   for (int i = 0; i < n; ++i)
     if (ctxs[i]->stream != st) CK(cudaStreamSynchronize(ctxs[i]->stream));
   CK(cudaEventRecord(c0->ev0, st));
-  CK(launch_megakernel_batch(dv, di, n, total, c0->status.p, c0->counters.p + 7, params[0].block_size, st));
+  bool quadrics = false;
+  for (int i = 0; i < n; ++i) quadrics = quadrics || ctxs[i]->view.has_quadrics;
+  CK(launch_megakernel_batch(dv, di, n, total, c0->status.p, c0->counters.p + 7, params[0].block_size, quadrics,
+                             st));
   CK(cudaEventRecord(c0->ev1, st));
   CK(cudaFreeAsync(dv, st));
   CK(cudaFreeAsync(di, st));

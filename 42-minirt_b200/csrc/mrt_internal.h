@@ -26,7 +26,7 @@
 
 namespace mrt {
 
-enum PrimType : int { PRIM_TRI = 0, PRIM_SPHERE = 1 };
+enum PrimType : int { PRIM_TRI = 0, PRIM_SPHERE = 1, PRIM_CYL = 2, PRIM_CONE = 3, PRIM_HYP = 4 };
 
 constexpr int kLeafMax = 8;          // primitives per leaf (3-bit count)
 constexpr int kStackSize = 64;       // traversal stack; the builder bounds depth below it
@@ -75,7 +75,12 @@ struct PlaneD {
 };
 
 // Everything a kernel needs, passed by value (kernel parameter space).
+// Kernels are instantiated for SceneView (spheres, triangles, planes) and for
+// SceneViewQ (the same plus cylinders, cones and hyperboloids), chosen per
+// scene at launch: the quadric tests compute in double, and their registers
+// stay out of the kernels of scenes without quadrics.
 struct SceneView {
+  static constexpr bool kQuadrics = false;
   const Node* nodes;
   const float4* geom;
   const int4* meta;
@@ -91,6 +96,7 @@ struct SceneView {
   int one_sided;
   int root_leaf;         // scene with a single leaf: the link of that leaf, else 0
   int has_bvh;
+  int has_quadrics;      // launch the SceneViewQ instantiation
   // camera (viewport.c:38-87), float
   float cam[3];
   float pixel00[3];
@@ -122,7 +128,7 @@ struct SceneView {
   const float* pdf_joint;  // W*H   (calc_pdf.c:93)
   const float* cdf_m_inv;  // H     (calc_cdf.c:39)
   const float* cdf_c_inv;  // W*H   (calc_cdf.c:112)
-  // caustics (photon hash grid)
+  // caustics (photon map)
   int caustic;
   int knn;
   float caustic_radius2; // compared against the k-th squared distance (get_caustic.c:45)
@@ -139,6 +145,21 @@ struct SceneView {
   float fixed_radius2;
   int n_photons;
 };
+
+struct SceneViewQ : SceneView {
+  static constexpr bool kQuadrics = true;
+};
+
+// Calls f with the view as the type its kernels are instantiated for.
+template <class F>
+inline auto with_view(const SceneView& S, F&& f) {
+  if (S.has_quadrics) {
+    SceneViewQ q;
+    static_cast<SceneView&>(q) = S;
+    return f(q);
+  }
+  return f(S);
+}
 
 // Device status word bits -> mrt_status on the host.
 enum StatusBits : int {

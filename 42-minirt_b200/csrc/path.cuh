@@ -13,7 +13,8 @@ struct PathCounters {
 };
 
 // importance_sampling (material_default.c:41-69): HDRI next-event estimate.
-__device__ __forceinline__ void env_nee(const SceneView& S, PathState& P, const Surf& s,
+template <class V>
+__device__ __forceinline__ void env_nee(const V& S, PathState& P, const Surf& s,
                                         int* status, PathCounters& C) {
   const int k = env_sample(S, P.rng);
   const float4 e = __ldg(S.env_rec0 + k);
@@ -34,7 +35,8 @@ __device__ __forceinline__ void env_nee(const SceneView& S, PathState& P, const 
 }
 
 // default_mat (material_default.c:71-92).
-__device__ __forceinline__ void default_mat(const SceneView& S, PathState& P, const Surf& s,
+template <class V>
+__device__ __forceinline__ void default_mat(const V& S, PathState& P, const Surf& s,
                                             int* status, PathCounters& C) {
   float3 direct = compute_light(S, P.rng, s, status, C.shadow);
   float3 caus = caustic_estimate(S, s.p);
@@ -46,7 +48,8 @@ __device__ __forceinline__ void default_mat(const SceneView& S, PathState& P, co
 }
 
 // dielectric_mat (dielectric.c:37-64) with reflected_dielectric_color (:15-33).
-__device__ __forceinline__ void dielectric_mat(const SceneView& S, const MaterialD& M, PathState& P,
+template <class V>
+__device__ __forceinline__ void dielectric_mat(const V& S, const MaterialD& M, PathState& P,
                                                const Surf& s, int* status, PathCounters& C) {
   if (M.ior > 0.0f) {
     float ct = -dot(unit(P.d), s.n);
@@ -69,7 +72,8 @@ __device__ __forceinline__ void dielectric_mat(const SceneView& S, const Materia
 }
 
 // material_manager_v3 (path_trace.c:15-35).
-__device__ __forceinline__ void material_manager(const SceneView& S, PathState& P, const Surf& s,
+template <class V>
+__device__ __forceinline__ void material_manager(const V& S, PathState& P, const Surf& s,
                                                  int* status, PathCounters& C) {
   if (s.mat < 0) {
     default_mat(S, P, s, status, C);
@@ -126,7 +130,8 @@ __device__ __forceinline__ void write_event(float* ev, int k, const SceneView& S
   e[17] = (float)s.mat;
 }
 
-__device__ __forceinline__ float3 trace_path(const SceneView& S, PathState& P, int max_depth,
+template <class V>
+__device__ __forceinline__ float3 trace_path(const V& S, PathState& P, int max_depth,
                                              int render_mode, int* status, PathCounters& C,
                                              float* ev = nullptr) {
   P.power = f3(1.f, 1.f, 1.f);
@@ -176,7 +181,8 @@ __device__ __forceinline__ float3 trace_path(const SceneView& S, PathState& P, i
 // One bounce of path_trace (path_trace.c:58-72) for a path whose state lives
 // in P. Returns false when the path ended (miss, depth exhausted, or zero
 // power); P.acc then holds its radiance.
-__device__ __forceinline__ bool bounce(const SceneView& S, PathState& P, int& depth_left,
+template <class V>
+__device__ __forceinline__ bool bounce(const V& S, PathState& P, int& depth_left,
                                        int* status, PathCounters& C) {
   HitInfo h;
   int visits = 0;

@@ -45,7 +45,8 @@ __device__ __forceinline__ float3 rnd_unit(Rng& rng) {
   return f3(0.f, 1.f, 0.f);
 }
 
-__global__ void photon_emit_kernel(SceneView S, PhotonEmit E, int* status) {
+template <class V>
+__global__ void photon_emit_kernel(V S, PhotonEmit E, int* status) {
   const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const uint64_t total = E.per_light * (uint64_t)E.n_point_lights;
   bool store = false;
@@ -281,7 +282,10 @@ cudaError_t launch_photon_emit(const SceneView& S, const PhotonEmit& P, int* sta
   const uint64_t total = P.per_light * (uint64_t)P.n_point_lights;
   if (total == 0) return cudaSuccess;
   const unsigned b = 128;
-  photon_emit_kernel<<<(unsigned)((total + b - 1) / b), b, 0, st>>>(S, P, status);
+  with_view(S, [&](const auto& v) {
+    photon_emit_kernel<<<(unsigned)((total + b - 1) / b), b, 0, st>>>(v, P, status);
+    return 0;
+  });
   return cudaGetLastError();
 }
 

@@ -5,14 +5,15 @@
 // Threads are laid out so that a warp covers an 8x4 pixel tile of one
 // sample (coherent primary rays), and samples vary slowest.
 #include <algorithm>
+#include <type_traits>
 
 #include "kernels.h"
 #include "path.cuh"
 
 namespace mrt {
 
-template <bool kCount, int kBlock>
-__global__ void __launch_bounds__(kBlock) megakernel(SceneView S, LaunchParams L, float4* accum,
+template <bool kCount, int kBlock, class V>
+__global__ void __launch_bounds__(kBlock) megakernel(V S, LaunchParams L, float4* accum,
                                                    int* depth, int* status,
                                                    unsigned long long* counters) {
   const uint64_t idx = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -55,8 +56,8 @@ __global__ void __launch_bounds__(kBlock) megakernel(SceneView S, LaunchParams L
 // by one bounce per loop iteration; lanes whose path ended take the next path
 // index (one atomic per warp for all idle lanes), so warps stay full until
 // the launch runs out of paths.
-template <int kBlock>
-__global__ void __launch_bounds__(kBlock) megakernel_regen(SceneView S, LaunchParams L, float4* accum,
+template <int kBlock, class V>
+__global__ void __launch_bounds__(kBlock) megakernel_regen(V S, LaunchParams L, float4* accum,
                                                            int* status, unsigned long long* work) {
   const uint32_t npix = (uint32_t)S.width * (uint32_t)S.height;
   const int lane = threadIdx.x & 31;
@@ -108,7 +109,7 @@ __global__ void __launch_bounds__(kBlock) megakernel_regen(SceneView S, LaunchPa
 // Scenes are ordered longest-first by the host (LPT); path index g maps to
 // the scene whose [start, start + paths) range holds it (binary search over
 // <= a few hundred prefix sums). Otherwise the regenerating loop above.
-template <int kBlock>
+template <int kBlock, class V>
 __global__ void __launch_bounds__(kBlock) megakernel_batch(const SceneView* __restrict__ views,
                                                            const BatchItem* __restrict__ items,
                                                            int n_items, uint64_t total,
@@ -139,7 +140,7 @@ __global__ void __launch_bounds__(kBlock) megakernel_batch(const SceneView* __re
           }
           item = lo;
           const BatchItem it = items[item];
-          const SceneView& S = views[it.view];
+          const V& S = static_cast<const V&>(views[it.view]);
           const uint64_t idx = g - it.start;
           const uint32_t npix = (uint32_t)S.width * (uint32_t)S.height;
           const uint32_t lin = (uint32_t)(idx % npix);
@@ -161,7 +162,7 @@ __global__ void __launch_bounds__(kBlock) megakernel_batch(const SceneView* __re
     if (__all_sync(0xffffffffu, done)) break;
     if (active) {
       const BatchItem& it = items[item];
-      if (!bounce(views[it.view], P, depth_left, status, C)) {
+      if (!bounce(static_cast<const V&>(views[it.view]), P, depth_left, status, C)) {
         active = false;
         atomicAdd(it.accum + pixel, make_float4(P.acc.x, P.acc.y, P.acc.z, 1.0f));
       }
@@ -171,7 +172,7 @@ __global__ void __launch_bounds__(kBlock) megakernel_batch(const SceneView* __re
 
 cudaError_t launch_megakernel_batch(const SceneView* views, const BatchItem* items, int n_items,
                                     uint64_t total, int* status, unsigned long long* work, int block,
-                                    cudaStream_t st) {
+                                    bool quadrics, cudaStream_t st) {
   if (total == 0 || n_items == 0) return cudaSuccess;
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
@@ -179,23 +180,30 @@ cudaError_t launch_megakernel_batch(const SceneView* views, const BatchItem* ite
   block = block > 0 ? block : 128;
   cudaError_t e = cudaMemsetAsync(work, 0, sizeof(unsigned long long), st);
   if (e != cudaSuccess) return e;
-#define MRT_BT(B)                                                                          \
+#define MRT_BT(B, VT)                                                                      \
   if (block <= B) {                                                                        \
     int occ = 0;                                                                           \
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, megakernel_batch<B>, B, 0);        \
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, megakernel_batch<B, VT>, B, 0);    \
     unsigned grid = (unsigned)std::min<uint64_t>((uint64_t)sms * std::max(occ, 1), (total + B - 1) / B); \
-    megakernel_batch<B><<<grid, B, 0, st>>>(views, items, n_items, total, status, work);  \
+    megakernel_batch<B, VT><<<grid, B, 0, st>>>(views, items, n_items, total, status, work); \
     return cudaGetLastError();                                                             \
   }
-  MRT_BT(64)
-  MRT_BT(128)
-  MRT_BT(256)
+  if (quadrics) {
+    MRT_BT(64, SceneViewQ)
+    MRT_BT(128, SceneViewQ)
+    MRT_BT(256, SceneViewQ)
+  } else {
+    MRT_BT(64, SceneView)
+    MRT_BT(128, SceneView)
+    MRT_BT(256, SceneView)
+  }
 #undef MRT_BT
   return cudaErrorInvalidValue;
 }
 
 // Debug probe: full event record of single paths (pixel, sample).
-__global__ void path_events_kernel(SceneView S, LaunchParams L, const int* pix, const int* smp, int n,
+template <class V>
+__global__ void path_events_kernel(V S, LaunchParams L, const int* pix, const int* smp, int n,
                                    float* ev, float* rgb, int* status) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -218,11 +226,15 @@ __global__ void path_events_kernel(SceneView S, LaunchParams L, const int* pix, 
 cudaError_t launch_path_events(const SceneView& S, const LaunchParams& L, const int* pix, const int* smp,
                                int n, float* ev, float* rgb, int* status, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
-  path_events_kernel<<<(n + 63) / 64, 64, 0, st>>>(S, L, pix, smp, n, ev, rgb, status);
+  with_view(S, [&](const auto& v) {
+    path_events_kernel<<<(n + 63) / 64, 64, 0, st>>>(v, L, pix, smp, n, ev, rgb, status);
+    return 0;
+  });
   return cudaGetLastError();
 }
 
-__global__ void first_hit_kernel(SceneView S, const double* rays, int64_t n, HitOut* out,
+template <class V>
+__global__ void first_hit_kernel(V S, const double* rays, int64_t n, HitOut* out,
                                  int* status) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -294,17 +306,20 @@ cudaError_t launch_megakernel(const SceneView& S, const LaunchParams& L, float4*
   if (L.n_paths == 0) return cudaSuccess;
   block = block > 0 ? block : 128;
   const unsigned grid = (unsigned)((L.n_paths + block - 1) / block);
+  return with_view(S, [&](const auto& v) -> cudaError_t {
+    using VT = std::decay_t<decltype(v)>;
 #define MRT_MK(B)                                                                          \
-  if (block <= B) {                                                                        \
-    if (counters) megakernel<true, B><<<grid, block, 0, st>>>(S, L, accum, depth, status, counters); \
-    else megakernel<false, B><<<grid, block, 0, st>>>(S, L, accum, depth, status, counters);      \
-    return cudaGetLastError();                                                             \
-  }
-  MRT_MK(64)
-  MRT_MK(128)
-  MRT_MK(256)
+    if (block <= B) {                                                                      \
+      if (counters) megakernel<true, B, VT><<<grid, block, 0, st>>>(v, L, accum, depth, status, counters); \
+      else megakernel<false, B, VT><<<grid, block, 0, st>>>(v, L, accum, depth, status, counters);      \
+      return cudaGetLastError();                                                           \
+    }
+    MRT_MK(64)
+    MRT_MK(128)
+    MRT_MK(256)
 #undef MRT_MK
-  return cudaErrorInvalidValue;
+    return cudaErrorInvalidValue;
+  });
 }
 
 cudaError_t launch_megakernel_regen(const SceneView& S, const LaunchParams& L, float4* accum,
@@ -317,26 +332,32 @@ cudaError_t launch_megakernel_regen(const SceneView& S, const LaunchParams& L, f
   block = block > 0 ? block : 128;
   cudaError_t e = cudaMemsetAsync(work, 0, sizeof(unsigned long long), st);
   if (e != cudaSuccess) return e;
+  return with_view(S, [&](const auto& v) -> cudaError_t {
+    using VT = std::decay_t<decltype(v)>;
 #define MRT_RG(B)                                                                          \
-  if (block <= B) {                                                                        \
-    int occ = 0;                                                                           \
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, megakernel_regen<B>, B, 0);        \
-    int per = blocks_per_sm > 0 ? std::min(blocks_per_sm, std::max(occ, 1)) : std::max(occ, 1); \
-    unsigned grid = (unsigned)std::min<uint64_t>((uint64_t)sms * per, (L.n_paths + B - 1) / B); \
-    megakernel_regen<B><<<grid, B, 0, st>>>(S, L, accum, status, work);                    \
-    return cudaGetLastError();                                                             \
-  }
-  MRT_RG(64)
-  MRT_RG(128)
-  MRT_RG(256)
+    if (block <= B) {                                                                      \
+      int occ = 0;                                                                         \
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, megakernel_regen<B, VT>, B, 0);  \
+      int per = blocks_per_sm > 0 ? std::min(blocks_per_sm, std::max(occ, 1)) : std::max(occ, 1); \
+      unsigned grid = (unsigned)std::min<uint64_t>((uint64_t)sms * per, (L.n_paths + B - 1) / B); \
+      megakernel_regen<B, VT><<<grid, B, 0, st>>>(v, L, accum, status, work);              \
+      return cudaGetLastError();                                                           \
+    }
+    MRT_RG(64)
+    MRT_RG(128)
+    MRT_RG(256)
 #undef MRT_RG
-  return cudaErrorInvalidValue;
+    return cudaErrorInvalidValue;
+  });
 }
 
 cudaError_t launch_first_hit(const SceneView& S, const double* rays, int64_t n, HitOut* out,
                              int* status, cudaStream_t st) {
   if (n == 0) return cudaSuccess;
-  first_hit_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(S, rays, n, out, status);
+  with_view(S, [&](const auto& v) {
+    first_hit_kernel<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(v, rays, n, out, status);
+    return 0;
+  });
   return cudaGetLastError();
 }
 

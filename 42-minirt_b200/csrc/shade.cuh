@@ -68,9 +68,63 @@ __device__ __forceinline__ float3 background(const SceneView& S, float3 d, bool 
 
 // ------------------------------------------------------------- surface
 
+// Normal, facing and material of a cylinder, cone or hyperboloid hit
+// (hit_cylinder.c, hit_cone.c, hit_hyperboloid.c, hit_obj.c:16-49): the
+// hit point is already in s.p, the part hit in h.u.
+__device__ __forceinline__ void quadric_surf(const SceneView& S, const HitInfo& h, int type, float3 d, Surf& s) {
+  const float4* g = S.geom + 3 * (size_t)h.prim;
+  const float4 a = __ldg(g), b = __ldg(g + 1), c = __ldg(g + 2);
+  const float3 pos = f3(a.x, a.y, a.z), ori = f3(b.x, b.y, b.z);
+  const float3 axis = unit(ori);
+  const int part = (int)h.u;
+  float3 n;
+  if (type == PRIM_CYL) {
+    if (part == PART_SIDE) {
+      // the lateral normal is faced twice (set_normal_face, then once more
+      // at the end of hit_cylinder): it always ends facing the ray, front 1
+      const float3 base = pos - axis * (c.x * 0.5f);
+      const float3 out = unit((s.p - base) - axis * dot(s.p - base, axis));
+      s.n = dot(d, out) < 0.0f ? out : -out;
+      s.front = 1;
+    } else {
+      n = part == PART_TOP ? ori : -ori;
+      s.front = dot(d, n) < 0.0f;
+      s.n = s.front ? n : -n;
+    }
+    const int top = __float_as_int(c.y), bot = __float_as_int(c.z);
+    if (part == PART_TOP && top >= 0) s.mat = top;
+    else if (part == PART_BOTTOM && bot >= 0) s.mat = bot;
+    return;
+  }
+  if (type == PRIM_CONE) {
+    if (part == PART_SIDE) {
+      const float rr = b.w / c.x;
+      n = unit((s.p - pos) - axis * ((1.0f + rr * rr) * dot(s.p - pos, axis)));
+    } else {
+      n = axis;
+    }
+    s.front = dot(d, n) < 0.0f;
+    s.n = s.front ? n : -n;
+    const int top = __float_as_int(c.y);
+    if (part == PART_TOP && top >= 0) s.mat = top;
+    return;
+  }
+  // hyperboloid: gradient of the quadric in the frame of compute_normal
+  // (hit_hyperboloid.c:36-52)
+  const float3 to_p = s.p - pos;
+  const float3 tmp = fabsf(axis.y) < 0.99f ? f3(0.f, 1.f, 0.f) : f3(1.f, 0.f, 0.f);
+  const float3 u = unit(cross(tmp, axis));
+  const float3 v = cross(axis, u);
+  n = unit(u * (2.0f * dot(to_p, u) / (b.w * b.w)) + v * (2.0f * dot(to_p, v) / (c.x * c.x)) -
+           axis * (2.0f * dot(to_p, axis) / (c.y * c.y)));
+  s.front = dot(d, n) < 0.0f;
+  s.n = s.front ? n : -n;
+}
+
 // Hit record of handle_hit / hit_all_planes + get_hit_register_color
 // (hit_obj.c:68, hit_register.c:79-107, get_hit_color.c:17-36), untextured.
-__device__ __forceinline__ Surf make_surf(const SceneView& S, const HitInfo& h, float3 o, float3 d,
+template <class V>
+__device__ __forceinline__ Surf make_surf(const V& S, const HitInfo& h, float3 o, float3 d,
                                           int render_mode) {
   Surf s;
   s.p = o + d * h.t;
@@ -87,11 +141,13 @@ __device__ __forceinline__ Surf make_surf(const SceneView& S, const HitInfo& h, 
                          w * n0.z + h.u * n1.z + h.v * n2.z));
       if (!S.one_sided && dot(d, n) > 0.0f) { s.front = 0; s.n = -n; }
       else { s.front = 1; s.n = n; }
-    } else {
+    } else if (!V::kQuadrics || m.z == PRIM_SPHERE) {
       float4 a = __ldg(S.geom + 3 * (size_t)h.prim), b = __ldg(S.geom + 3 * (size_t)h.prim + 1);
       float3 out = (s.p - f3(a.x, a.y, a.z)) * (1.0f / b.x);
       s.front = dot(d, out) < 0.0f;
       s.n = s.front ? out : -out;
+    } else if constexpr (V::kQuadrics) {
+      quadric_surf(S, h, m.z, d, s);
     }
   } else {
     const PlaneD& pl = S.planes[-1 - h.prim];
@@ -185,7 +241,8 @@ __device__ __forceinline__ float3 reflect_v(float3 v, float3 n) { return v - n *
 // compute_light_v2 (light_manager.c:59-71) and its point / directional
 // terms (p_light.c:19-89, d_light.c:19-55). The reference sums into uint64
 // channels (t_lcolor), truncating every addition; floorf reproduces that.
-__device__ __forceinline__ float3 compute_light(const SceneView& S, Rng& rng, const Surf& s,
+template <class V>
+__device__ __forceinline__ float3 compute_light(const V& S, Rng& rng, const Surf& s,
                                                 int* status, uint32_t& shadow_rays) {
   float lc0 = 0.f, lc1 = 0.f, lc2 = 0.f;
   if (S.n_lights == 0) return f3(0.f, 0.f, 0.f);

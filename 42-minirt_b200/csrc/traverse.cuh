@@ -1,7 +1,8 @@
 // traverse.cuh — closest-hit and any-hit queries over the BVH2 + planes.
 //
 // Semantics follow hit_register_all (hit_register.c:79-120): BVH primitives
-// (spheres, triangles) count when t in [0.001, 1000) (valid_t.c:16 and the
+// (spheres, triangles, and in the SceneViewQ instantiation cylinders, cones
+// and hyperboloids) count when t in [0.001, 1000) (valid_t.c:16 and the
 // closest_t = 1000 start, hit_register.c:21), then every infinite plane is
 // tested and replaces the BVH hit only with a strictly smaller t
 // (hit_plane.c:43-71, t in [0.001, 1000]). The tree is walked near child
@@ -9,6 +10,7 @@
 // local memory (64 entries; the builder keeps the depth below that).
 #pragma once
 #include "device_common.cuh"
+#include "quadric.cuh"
 
 namespace mrt {
 
@@ -83,6 +85,31 @@ __device__ __forceinline__ bool plane_hit(const PlaneD& p, float3 o, float3 d, f
   return t >= kTMin && t <= kTMax;
 }
 
+// One primitive of a leaf: triangle, sphere or (SceneViewQ) quadric. u, v
+// receive a triangle's barycentrics, or u the part of a quadric that was hit.
+template <class V>
+__device__ __forceinline__ bool prim_hit(const V& S, int i, float3 o, float3 d, float tbest, float& t,
+                                         float& u, float& v) {
+  const float4* g = S.geom + 3 * (size_t)i;
+  const float4 a = ldg4(g), b = ldg4(g + 1);
+  const int type = __float_as_int(a.w);
+  if (type == PRIM_TRI) {
+    const float4 c = ldg4(g + 2);
+    return tri_hit(a, b, c, o, d, S.one_sided, tbest, t, u, v);
+  }
+  if constexpr (V::kQuadrics) {
+    if (type != PRIM_SPHERE) {
+      const QuadricHit q = quadric_hit(type, a, b, ldg4(g + 2), o, d, tbest);
+      if (q.t < 0.0f) return false;
+      t = q.t;
+      u = (float)q.part;
+      v = 0.f;
+      return true;
+    }
+  }
+  return sphere_hit(a, b, o, d, tbest, t);
+}
+
 // Closest hit. `visits` counts node fetches (heat-map / roofline counter).
 // Returns false on a miss. `status` receives ST_BUDGET if the bounded loop
 // ran out (a corrupted tree), never hangs.
@@ -101,8 +128,8 @@ __device__ __forceinline__ void fetch_node(const Node* nd, float4& lxy, float4& 
   ln = ldg4(&nd->link);
 }
 
-template <bool kCount, bool kAnyHit>
-__device__ __forceinline__ bool traverse(const SceneView& S, float3 o, float3 d, float tmax_in,
+template <bool kCount, bool kAnyHit, class V>
+__device__ __forceinline__ bool traverse(const V& S, float3 o, float3 d, float tmax_in,
                                          float& tbest, int& best, float& bu, float& bv, int& visits,
                                          int* status) {
   const float3 inv = f3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
@@ -150,16 +177,8 @@ __device__ __forceinline__ bool traverse(const SceneView& S, float3 o, float3 d,
       const int code = ~leaf;
       const int first = code >> 3, count = (code & 7) + 1;
       for (int i = first; i < first + count; ++i) {
-        const float4* g = S.geom + 3 * (size_t)i;
-        const float4 a = ldg4(g), b = ldg4(g + 1);
         float t, u = 0.f, v = 0.f;
-        bool ok;
-        if (__float_as_int(a.w) == PRIM_TRI) {
-          const float4 c = ldg4(g + 2);
-          ok = tri_hit(a, b, c, o, d, S.one_sided, tbest, t, u, v);
-        } else {
-          ok = sphere_hit(a, b, o, d, tbest, t);
-        }
+        const bool ok = prim_hit(S, i, o, d, tbest, t, u, v);
         if (ok) {
           if (kAnyHit) return true;
           tbest = t;
@@ -178,8 +197,8 @@ __device__ __forceinline__ bool traverse(const SceneView& S, float3 o, float3 d,
   return best != kMiss;
 }
 
-template <bool kCount>
-__device__ __forceinline__ bool closest_hit_ww(const SceneView& S, float3 o, float3 d, HitInfo& hit,
+template <bool kCount, class V>
+__device__ __forceinline__ bool closest_hit_ww(const V& S, float3 o, float3 d, HitInfo& hit,
                                                int& visits, int* status) {
   float tbest = kTMax;
   int best = kMiss;
@@ -201,7 +220,8 @@ __device__ __forceinline__ bool closest_hit_ww(const SceneView& S, float3 o, flo
 }
 
 // Any hit with t < tmax (shadow rays), while-while form. Planes first: they are cheap.
-__device__ __forceinline__ bool any_hit_ww(const SceneView& S, float3 o, float3 d, float tmax,
+template <class V>
+__device__ __forceinline__ bool any_hit_ww(const V& S, float3 o, float3 d, float tmax,
                                            int* status) {
   for (int i = 0; i < S.n_planes; ++i) {
     float t;
@@ -217,8 +237,8 @@ __device__ __forceinline__ bool any_hit_ww(const SceneView& S, float3 o, float3 
 
 // Compact single-loop traversal (one node or one leaf per iteration): the
 // megakernel's form, whose register budget is dominated by shading.
-template <bool kCount>
-__device__ __forceinline__ bool closest_hit_compact(const SceneView& S, float3 o, float3 d, HitInfo& hit,
+template <bool kCount, class V>
+__device__ __forceinline__ bool closest_hit_compact(const V& S, float3 o, float3 d, HitInfo& hit,
                                             int& visits, int* status) {
   float tbest = kTMax;
   int best = kMiss;
@@ -257,24 +277,14 @@ __device__ __forceinline__ bool closest_hit_compact(const SceneView& S, float3 o
         int code = ~cur;
         int first = code >> 3, count = (code & 7) + 1;
         for (int i = first; i < first + count; ++i) {
-          const float4* g = S.geom + 3 * (size_t)i;
-          float4 a = ldg4(g), b = ldg4(g + 1);
           float t, u = 0.f, v = 0.f;
-          bool ok;
-          if (__float_as_int(a.w) == PRIM_TRI) {
-            float4 c = ldg4(g + 2);
-            ok = tri_hit(a, b, c, o, d, S.one_sided, tbest, t, u, v);
-          } else {
-            ok = sphere_hit(a, b, o, d, tbest, t);
-          }
-          if (ok) { tbest = t; best = i; bu = u; bv = v; }
+          if (prim_hit(S, i, o, d, tbest, t, u, v)) { tbest = t; best = i; bu = u; bv = v; }
         }
       }
       if (sp == 0) break;
       cur = stack[--sp];
     }
   }
-  const bool bvh_hit = best != kMiss;
   for (int i = 0; i < S.n_planes; ++i) {
     float t;
     if (plane_hit(S.planes[i], o, d, t) && (best == kMiss || t < tbest)) {
@@ -290,7 +300,8 @@ __device__ __forceinline__ bool closest_hit_compact(const SceneView& S, float3 o
 }
 
 // Any hit, compact loop.
-__device__ __forceinline__ bool any_hit_compact(const SceneView& S, float3 o, float3 d, float tmax,
+template <class V>
+__device__ __forceinline__ bool any_hit_compact(const V& S, float3 o, float3 d, float tmax,
                                         int* status) {
   for (int i = 0; i < S.n_planes; ++i) {
     float t;
@@ -328,17 +339,8 @@ __device__ __forceinline__ bool any_hit_compact(const SceneView& S, float3 o, fl
       int code = ~cur;
       int first = code >> 3, count = (code & 7) + 1;
       for (int i = first; i < first + count; ++i) {
-        const float4* g = S.geom + 3 * (size_t)i;
-        float4 a = ldg4(g), b = ldg4(g + 1);
         float t, u, v;
-        bool ok;
-        if (__float_as_int(a.w) == PRIM_TRI) {
-          float4 c = ldg4(g + 2);
-          ok = tri_hit(a, b, c, o, d, S.one_sided, tlim, t, u, v);
-        } else {
-          ok = sphere_hit(a, b, o, d, tlim, t);
-        }
-        if (ok) return true;
+        if (prim_hit(S, i, o, d, tlim, t, u, v)) return true;
       }
     }
     if (sp == 0) return false;
@@ -348,13 +350,14 @@ __device__ __forceinline__ bool any_hit_compact(const SceneView& S, float3 o, fl
 
 // The megakernel and the debug probes use the compact loop; the wavefront's
 // traversal kernels call the while-while form directly.
-template <bool kCount>
-__device__ __forceinline__ bool closest_hit(const SceneView& S, float3 o, float3 d, HitInfo& hit,
+template <bool kCount, class V>
+__device__ __forceinline__ bool closest_hit(const V& S, float3 o, float3 d, HitInfo& hit,
                                             int& visits, int* status) {
   return closest_hit_compact<kCount>(S, o, d, hit, visits, status);
 }
 
-__device__ __forceinline__ bool any_hit(const SceneView& S, float3 o, float3 d, float tmax, int* status) {
+template <class V>
+__device__ __forceinline__ bool any_hit(const V& S, float3 o, float3 d, float tmax, int* status) {
   return any_hit_compact(S, o, d, tmax, status);
 }
 

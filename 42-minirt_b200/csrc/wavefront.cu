@@ -127,8 +127,8 @@ __global__ void __launch_bounds__(kWfBlock) wf_generate(SceneView S, WfState W, 
 }
 
 // --------------------------------------------------------------- extend
-template <int kBounceParity>
-__global__ void __launch_bounds__(kWfBlock) wf_extend(SceneView S, WfState W, int* status) {
+template <int kBounceParity, class V>
+__global__ void __launch_bounds__(kWfBlock) wf_extend(V S, WfState W, int* status) {
   const int n = W.counters[kBounceParity ? C_LIVE1 : C_LIVE0];
   const int* q = W.q_live[kBounceParity];
   const int lane = threadIdx.x & 31;
@@ -215,8 +215,8 @@ __device__ __forceinline__ void emit_shadow(const WfState& W, int path, int slot
   W.sh_d[s] = make_float4(d.x, d.y, d.z, __int_as_float((path << 4) | slot));
 }
 
-template <int kBounceParity>
-__global__ void __launch_bounds__(kWfBlock) wf_sample(SceneView S, WfState W, const WfParams* __restrict__ Pp, int* status) {
+template <int kBounceParity, class V>
+__global__ void __launch_bounds__(kWfBlock) wf_sample(V S, WfState W, const WfParams* __restrict__ Pp, int* status) {
   int cum[kKinds + 1];
   cum[0] = 0;
   for (int c = 0; c < kKinds; ++c) cum[c + 1] = cum[c] + W.counters[C_KIND + c];
@@ -343,7 +343,8 @@ __global__ void __launch_bounds__(kWfBlock) wf_sample(SceneView S, WfState W, co
 }
 
 // -------------------------------------------------------------- connect
-__global__ void __launch_bounds__(kWfBlock) wf_connect(SceneView S, WfState W, int* status) {
+template <class V>
+__global__ void __launch_bounds__(kWfBlock) wf_connect(V S, WfState W, int* status) {
   const int n = min(W.counters[C_SH], W.sh_capacity);
   const int lane = threadIdx.x & 31;
   while (true) {
@@ -544,9 +545,11 @@ static cudaError_t wf_shadow_alloc(WfHost* H, size_t sh_cap) {
   return cudaSuccess;
 }
 
-// Enqueues one wave (generate + max_bounces x stages) on `st`.
-static void wf_enqueue_wave(WfHost* H, const SceneView& v, const WfParams& P, int* status,
-                            cudaStream_t st, unsigned* launches) {
+// Enqueues one wave (generate + max_bounces x stages) on `st`; the
+// traversal and shading stages are the instantiation for the view's type.
+template <class VT>
+static void wf_enqueue_wave_t(WfHost* H, const VT& v, const WfParams& P, int* status,
+                              cudaStream_t st, unsigned* launches) {
   const WfParams* dP = H->dparams;
   const int sms = H->sms;
   const int gen_blocks = std::max(1, std::min((H->capacity + kWfBlock - 1) / kWfBlock, sms * 16));
@@ -557,19 +560,19 @@ static void wf_enqueue_wave(WfHost* H, const SceneView& v, const WfParams& P, in
   unsigned n = 2;
   for (int b = 0; b < P.max_bounces; ++b) {
     if ((b & 1) == 0) {
-      wf_extend<0><<<pers, kWfBlock, 0, st>>>(v, s, status);
+      wf_extend<0, VT><<<pers, kWfBlock, 0, st>>>(v, s, status);
       wf_classify<0><<<gen_blocks, kWfBlock, 0, st>>>(v, s, dP);
-      wf_sample<0><<<gen_blocks, kWfBlock, 0, st>>>(v, s, dP, status);
+      wf_sample<0, VT><<<gen_blocks, kWfBlock, 0, st>>>(v, s, dP, status);
       wf_work_reset<<<1, 32, 0, st>>>(s);
-      wf_connect<<<pers, kWfBlock, 0, st>>>(v, s, status);
+      wf_connect<VT><<<pers, kWfBlock, 0, st>>>(v, s, status);
       wf_finish<0><<<gen_blocks, kWfBlock, 0, st>>>(v, s);
       wf_reset<0><<<1, 32, 0, st>>>(s);
     } else {
-      wf_extend<1><<<pers, kWfBlock, 0, st>>>(v, s, status);
+      wf_extend<1, VT><<<pers, kWfBlock, 0, st>>>(v, s, status);
       wf_classify<1><<<gen_blocks, kWfBlock, 0, st>>>(v, s, dP);
-      wf_sample<1><<<gen_blocks, kWfBlock, 0, st>>>(v, s, dP, status);
+      wf_sample<1, VT><<<gen_blocks, kWfBlock, 0, st>>>(v, s, dP, status);
       wf_work_reset<<<1, 32, 0, st>>>(s);
-      wf_connect<<<pers, kWfBlock, 0, st>>>(v, s, status);
+      wf_connect<VT><<<pers, kWfBlock, 0, st>>>(v, s, status);
       wf_finish<1><<<gen_blocks, kWfBlock, 0, st>>>(v, s);
       wf_reset<1><<<1, 32, 0, st>>>(s);
     }
@@ -579,6 +582,14 @@ static void wf_enqueue_wave(WfHost* H, const SceneView& v, const WfParams& P, in
   wf_wave_end<<<1, 32, 0, st>>>(s);
   n += 1;
   if (launches) *launches += n;
+}
+
+static void wf_enqueue_wave(WfHost* H, const SceneView& v, const WfParams& P, int* status,
+                            cudaStream_t st, unsigned* launches) {
+  with_view(v, [&](const auto& vt) {
+    wf_enqueue_wave_t(H, vt, P, status, st, launches);
+    return 0;
+  });
 }
 
 __global__ void wf_retire_remaining(WfState W, int parity_count_index, int parity) {

@@ -54,6 +54,9 @@ typedef struct s_flat
 	mrt_plane		*pl;
 	mrt_light		*li;
 	mrt_mesh		*me;
+	mrt_cylinder	*cy;
+	mrt_cone		*co;
+	mrt_hyperboloid	*hy;
 	double			**buf;
 	int				nbuf;
 }	t_flat;
@@ -89,6 +92,9 @@ static void	free_flat(t_flat *f)
 	free(f->pl);
 	free(f->li);
 	free(f->me);
+	free(f->cy);
+	free(f->co);
+	free(f->hy);
 }
 
 /* t_custom_object triangles (after ft_update_obj_position) -> a
@@ -132,7 +138,7 @@ static int	add_custom(t_flat *f, t_scene *s, t_custom_object *o, mrt_mesh *m)
 
 static int	flatten(t_minirt *mrt, t_scene *s, t_flat *f)
 {
-	int	ns = 0, np = 0, nl = 0, nm = 0;
+	int	ns = 0, np = 0, nl = 0, nm = 0, nc = 0, nk = 0, nh = 0;
 
 	memset(f, 0, sizeof(*f));
 	for (int i = 0; i < s->el_amount; i++)
@@ -143,21 +149,21 @@ static int	flatten(t_minirt *mrt, t_scene *s, t_flat *f)
 		np += ty == PLANE;
 		nl += ty == LIGHT || ty == DIRECTIONAL_LIGHT;
 		nm += ty == CUSTOM;
-		if (ty == CYLINDER || ty == CONE || ty == HYPERBOLOID)
-		{
-			fprintf(stderr, "\033[0;31m[Error]\033[0m convert_scene_build: "
-				"cylinders, cones and hyperboloids are not supported by the CUDA "
-				"path yet\n");
-			return (-1);
-		}
+		nc += ty == CYLINDER;
+		nk += ty == CONE;
+		nh += ty == HYPERBOLOID;
 	}
 	f->mats = calloc(s->mat_amount + 1, sizeof(mrt_material));
 	f->sph = calloc(ns + 1, sizeof(mrt_sphere));
 	f->pl = calloc(np + 1, sizeof(mrt_plane));
 	f->li = calloc(nl + 1, sizeof(mrt_light));
 	f->me = calloc(nm + 1, sizeof(mrt_mesh));
+	f->cy = calloc(nc + 1, sizeof(mrt_cylinder));
+	f->co = calloc(nk + 1, sizeof(mrt_cone));
+	f->hy = calloc(nh + 1, sizeof(mrt_hyperboloid));
 	f->buf = calloc(3 * nm + 1, sizeof(double *));
-	if (!f->mats || !f->sph || !f->pl || !f->li || !f->me || !f->buf)
+	if (!f->mats || !f->sph || !f->pl || !f->li || !f->me || !f->buf
+		|| !f->cy || !f->co || !f->hy)
 		return (-1);
 	for (int i = 0; i < s->mat_amount; i++)
 	{
@@ -174,7 +180,7 @@ static int	flatten(t_minirt *mrt, t_scene *s, t_flat *f)
 		o->emission_strength = m->emission_strength;
 		o->scale = m->scale;
 	}
-	ns = np = nl = nm = 0;
+	ns = np = nl = nm = nc = nk = nh = 0;
 	for (int i = 0; i < s->el_amount; i++)
 	{
 		void	*ob = s->elements[i].object;
@@ -216,6 +222,45 @@ static int	flatten(t_minirt *mrt, t_scene *s, t_flat *f)
 			v3(f->li[nl].position, l->orientation);
 			f->li[nl].brightness = l->brightness;
 			c3(f->li[nl++].color, l->color);
+		}
+		else if (s->elements[i].type == CYLINDER)
+		{
+			t_cylinder	*c = ob;
+
+			v3(f->cy[nc].position, c->position);
+			v3(f->cy[nc].orientation, c->orientation);
+			f->cy[nc].diameter = c->diameter;
+			f->cy[nc].height = c->height;
+			f->cy[nc].material = mat_index(s, c->material);
+			f->cy[nc].material_top = mat_index(s, c->material_top);
+			f->cy[nc].material_bot = mat_index(s, c->material_bot);
+			c3(f->cy[nc++].color, c->color);
+		}
+		else if (s->elements[i].type == CONE)
+		{
+			t_cone	*c = ob;
+
+			v3(f->co[nk].position, c->position);
+			v3(f->co[nk].orientation, c->orientation);
+			f->co[nk].diameter = c->diameter;
+			f->co[nk].height = c->height;
+			f->co[nk].material = mat_index(s, c->material);
+			f->co[nk].material_top = mat_index(s, c->material_top);
+			c3(f->co[nk++].color, c->color);
+		}
+		else if (s->elements[i].type == HYPERBOLOID)
+		{
+			t_hyperboloid	*c = ob;
+
+			v3(f->hy[nh].position, c->position);
+			v3(f->hy[nh].orientation, c->orientation);
+			f->hy[nh].a = c->a;
+			f->hy[nh].b = c->b;
+			f->hy[nh].c = c->c;
+			f->hy[nh].shape = c->shape;
+			f->hy[nh].height = c->height;
+			f->hy[nh].material = mat_index(s, c->material);
+			c3(f->hy[nh++].color, c->color);
 		}
 		else if (s->elements[i].type == CUSTOM)
 		{
@@ -266,6 +311,12 @@ static int	flatten(t_minirt *mrt, t_scene *s, t_flat *f)
 	f->d.n_lights = nl;
 	f->d.meshes = f->me;
 	f->d.n_meshes = nm;
+	f->d.cylinders = f->cy;
+	f->d.n_cylinders = nc;
+	f->d.cones = f->co;
+	f->d.n_cones = nk;
+	f->d.hyperboloids = f->hy;
+	f->d.n_hyperboloids = nh;
 	return (0);
 }
 

@@ -384,8 +384,10 @@ typedef struct mrt_ray
 }	mrt_ray;
 
 /* Closest hit (hit_register_all, hit_register.c:109).
- * prim: flat primitive id — spheres [0,S), triangles [S,S+T) in mesh order,
- * planes [S+T, S+T+P) — or -1 for a miss. */
+ * prim: flat primitive id — spheres, cylinders, cones, hyperboloids,
+ * triangles in mesh order, then planes — or -1 for a miss. u, v: a
+ * triangle's barycentrics; for a quadric u is the part hit (0 lateral
+ * surface, 1 top cap, 2 bottom cap). */
 typedef struct mrt_hit
 {
 	int32_t	prim;

@@ -293,3 +293,56 @@ def test_adam_fit_recovers_albedo(mrt, scenes, oracle):
     err0 = np.abs(th[:3 * M] - target_theta[:3 * M])[seen].mean()
     err1 = np.abs(fit[:3 * M] - target_theta[:3 * M])[seen].mean()
     assert err1 < 0.7 * err0, (err0, err1)
+
+
+@gpu
+def test_adjoint_on_quadrics_matches_fp64_gradient_per_path(mrt, scenes, oracle):
+    """Cylinders, cones and hyperboloids in the path: the hit point and
+    normal of a quadric follow the ray through the implicit-surface
+    derivative of t. Single paths (spp 1) against the FP64 central
+    difference of the same path, as for triangles and spheres."""
+    lib = mrt.load()
+    if lib.mrt_device_count() <= 0:
+        pytest.skip("no CUDA device")
+    W, H = 64, 48
+    sc = scenes.make_quadrics(5, W, H, spp=1, depth=6)
+    for m in sc.materials:            # rough metals: roughness gradients through quadric normals
+        if m.get("metallic", 0.0) == 1.0:
+            m["roughness"] = max(m.get("roughness", 0.0), 0.15)
+    ctx = mrt.Context(W, H)
+    ctx.build(oracle.canonical_scene(sc))
+    th = ctx.diff_params()
+    M, seed = len(sc.materials), 7
+    ro = oracle.Restatement(sc)
+    ro.set_params(th.astype(np.float64), exact=True)
+    rng = np.random.default_rng(4)
+    pix, ev = _matched_paths(ctx, ro, rng.choice(W * H, 400, replace=False).astype(np.int32), seed)
+    quad = set(range(len(sc.spheres), len(sc.spheres) + len(sc.cylinders) + len(sc.cones) + len(sc.hyperboloids)))
+    on_quad = [i for i in range(len(pix)) if any(int(ev[i][k, 0]) in quad for k in range(16))]
+    assert len(on_quad) >= 60, len(on_quad)
+    checked = bad = rough = 0
+    for i in on_quad[:80]:
+        p = int(pix[i])
+        dimg = np.zeros((H, W, 3), np.float32)
+        dimg.reshape(-1, 3)[p] = (0.7, 1.0, 1.3)
+        g = ctx.backward(th, dimg, spp=1, seed=seed).astype(np.float64)
+        idx = [j for j in range(5 * M) if g[j] != 0.0]
+        if not idx:
+            continue
+        dirs = np.zeros((len(idx), len(th)))
+        dirs[np.arange(len(idx)), idx] = 1.0
+        w = np.array([[0.7, 1.0, 1.3]])
+        f6 = ro.fd_gradient(th, dirs, w, seed, 1, np.array([p], np.int32), h=1e-6)
+        f7 = ro.fd_gradient(th, dirs, w, seed, 1, np.array([p], np.int32), h=1e-7)
+        for k, j in enumerate(idx):
+            if 4 * M <= j < 5 * M and th[j] == 0.0:
+                continue
+            if abs(f6[k] - f7[k]) > 1e-3 * (abs(f7[k]) + 1e-3):
+                continue
+            checked += 1
+            rough += 3 * M <= j < 4 * M
+            if abs(g[j] - f7[k]) > 1e-2 * abs(f7[k]) + 1e-4:
+                bad += 1
+    print("quadric paths", len(on_quad), "checked", checked, "roughness", rough, "bad", bad)
+    assert checked >= 100 and rough >= 5
+    assert bad <= 0.03 * checked, (bad, checked)

@@ -61,7 +61,7 @@ def random_rays(rng, vp, n, spread=0.3):
     return o, d
 
 
-@pytest.mark.parametrize("name", ["c0", "c1", "c2"])
+@pytest.mark.parametrize("name", ["c0", "c1", "c2", "q0"])
 def test_first_hit_matches_reference_golden(mrt, oracle, mg, name):
     g = golden(f"{name}_pins.npz")
     sc = mg.CASES[name]["make"]()
@@ -77,7 +77,7 @@ def test_first_hit_matches_reference_golden(mrt, oracle, mg, name):
     np.testing.assert_array_equal(h["front_face"][hit], g["hit_front_face"][hit])
 
 
-@pytest.mark.parametrize("name", ["c0", "c1", "c2"])
+@pytest.mark.parametrize("name", ["c0", "c1", "c2", "q0"])
 def test_first_hit_matches_oracle_on_fresh_rays(mrt, oracle, mg, name):
     sc = mg.CASES[name]["make"]()
     ro = oracle.Restatement(sc)
@@ -153,7 +153,8 @@ def _diffuse(sc):
     return sc
 
 
-STREAM_CASES = {"c0": 0.99, "c1": 0.85, "c2": 0.99, "c1_noglass": 0.85, "c1_diffuse": 0.99}
+STREAM_CASES = {"c0": 0.99, "c1": 0.85, "c2": 0.99, "c1_noglass": 0.85, "c1_diffuse": 0.99, "q0": 0.95,
+                "q0_diffuse": 0.99}
 
 
 @pytest.mark.parametrize("name", sorted(STREAM_CASES))
@@ -193,7 +194,7 @@ def test_paths_match_oracle_stream(mrt, oracle, mg, name):
     assert abs(diff.mean()) <= 4 * se, (diff.mean(), se)
 
 
-@pytest.mark.parametrize("name", ["c0", "c1", "c2"])
+@pytest.mark.parametrize("name", ["c0", "c1", "c2", "q0"])
 def test_wavefront_matches_megakernel(mrt, oracle, mg, name):
     """Both forms run the same estimator on the same random streams."""
     sc = mg.CASES[name]["make"]()
@@ -362,3 +363,35 @@ def test_batch_matches_individual_renders(mrt, oracle, scenes):
         c.render(params[i]["spp"], seed=params[i]["seed"])
         single, _ = c.read_accum()
         np.testing.assert_allclose(batch[i][0], single, rtol=1e-4, atol=1e-5)
+
+
+def test_batch_with_quadrics_matches_individual_renders(mrt, oracle, scenes):
+    """A batch holding a scene with cylinders, cones and hyperboloids runs
+    the quadric instantiation of the batch kernel for every scene; each
+    accumulator still equals its own single-scene render."""
+    specs = [scenes.make_quadrics(5, 40, 30, depth=6), scenes.make_c0(0, 32, 24)]
+    ctxs = []
+    for sc in specs:
+        c = mrt.Context(sc.width, sc.height)
+        c.build(oracle.canonical_scene(sc))
+        ctxs.append(c)
+    params = [dict(spp=4 + i, seed=21 + i, max_bounces=0) for i in range(len(ctxs))]
+    mrt.render_batch(ctxs, params)
+    batch = [c.read_accum() for c in ctxs]
+    for i, c in enumerate(ctxs):
+        c.clear()
+        c.render(params[i]["spp"], seed=params[i]["seed"])
+        single, _ = c.read_accum()
+        np.testing.assert_allclose(batch[i][0], single, rtol=1e-4, atol=1e-5)
+
+
+def test_quadric_scene_rejects_malformed_objects(mrt, scenes):
+    sc = scenes.make_quadrics(5, 16, 12)
+    sc.cones[0]["height"] = 0.0
+    ctx = mrt.Context(16, 12)
+    with pytest.raises(Exception, match="cone 0"):
+        ctx.build(sc)
+    sc = scenes.make_quadrics(5, 16, 12)
+    sc.hyperboloids[1]["c"] = 0.0
+    with pytest.raises(Exception, match="hyperboloid 1"):
+        ctx.build(sc)
