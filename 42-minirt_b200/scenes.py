@@ -15,6 +15,8 @@ of the benchmark configurations:
   c3  64 scenes of uneven size (batched workload).
   c4  512x512, 64 spp, depth 8: c1 generator at 200,000 triangles with 32
       materials and a 512x256 sky (inverse rendering).
+  q0  320x240, 64 spp, depth 8: two cylinders, two cones, two hyperboloids,
+      two spheres and a ground plane (the reference's quadric objects).
 
 Values use the reference's own types: 8-bit colours, RGBE sky texels,
 horizontal integer-degree field of view (viewport.c:57), so that the oracle and
@@ -600,4 +602,5 @@ def make_quadrics(seed: int = 5, width: int = 320, height: int = 240, spp: int =
     return sc
 
 
-CONFIGS = {"c0": make_c0, "c1": make_c1, "c2": make_c2, "c2p": make_c2_progressive, "c4": make_c4}
+CONFIGS = {"c0": make_c0, "c1": make_c1, "c2": make_c2, "c2p": make_c2_progressive, "c4": make_c4,
+           "q0": make_quadrics}

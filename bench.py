@@ -319,12 +319,20 @@ def bench_c3(a) -> int:
     return 0
 
 
+WORKLOADS = {
+    "c1": "c1: 1920x1080, 256 spp, depth 12, 1,310,720-triangle displaced geodesic sphere, "
+          "16 materials, 2048x1024 RGBE sky with importance sampling",
+    "q0": "q0: 320x240, 64 spp, depth 8, two cylinders, two cones, two hyperboloids, two spheres, "
+          "ground plane, point light",
+}
+
+
 def workload_config(a, sc) -> dict:
-    return {"workload": f"{a.config}: 1920x1080, 256 spp, depth 12, 1,310,720-triangle displaced "
-                        "geodesic sphere, 16 materials, 2048x1024 RGBE sky with importance sampling"
-                        if a.config == "c1" else a.config,
+    return {"workload": WORKLOADS.get(a.config, a.config),
             "spp_per_step": a.spp_per_step,
-            "l2": "scene arrays (BVH, triangles, shading, sky tables) exceed the 126 MB L2",
+            "l2": ("scene arrays (BVH, triangles, shading, sky tables) exceed the 126 MB L2"
+                   if a.config != "q0" else "the scene (a few KB) stays in L2, as in any render of it; "
+                   "each step traces new paths"),
             "parallelism": f"sample-parallel dp{a.gpus}"}
 
 

@@ -306,9 +306,11 @@ def test_adjoint_on_quadrics_matches_fp64_gradient_per_path(mrt, scenes, oracle)
         pytest.skip("no CUDA device")
     W, H = 64, 48
     sc = scenes.make_quadrics(5, W, H, spp=1, depth=6)
-    for m in sc.materials:            # rough metals: roughness gradients through quadric normals
-        if m.get("metallic", 0.0) == 1.0:
-            m["roughness"] = max(m.get("roughness", 0.0), 0.15)
+    # the quadrics' lambertian materials become rough metals, so that GGX
+    # samples (and roughness gradients) are taken about quadric normals
+    for i, m in enumerate(sc.materials):
+        if i > 0 and m.get("ior", 0.0) == 0.0 and m.get("emission_strength", 0.0) == 0.0:
+            m.update(metallic=1.0, roughness=max(m.get("roughness", 0.0), 0.2))
     ctx = mrt.Context(W, H)
     ctx.build(oracle.canonical_scene(sc))
     th = ctx.diff_params()
@@ -344,5 +346,5 @@ def test_adjoint_on_quadrics_matches_fp64_gradient_per_path(mrt, scenes, oracle)
             if abs(g[j] - f7[k]) > 1e-2 * abs(f7[k]) + 1e-4:
                 bad += 1
     print("quadric paths", len(on_quad), "checked", checked, "roughness", rough, "bad", bad)
-    assert checked >= 100 and rough >= 5
+    assert checked >= 100 and rough >= 20
     assert bad <= 0.03 * checked, (bad, checked)
