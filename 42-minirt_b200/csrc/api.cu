@@ -455,6 +455,12 @@ extern "C" int mrt_scene_build(mrt_ctx* c, const mrt_scene_desc* d) {
       (d->n_cylinders && !d->cylinders) || (d->n_cones && !d->cones) ||
       (d->n_hyperboloids && !d->hyperboloids))
     return set_err(MRT_ERR_INVALID, "null element array with a non-zero count");
+  for (int i = 0; i < d->n_materials; ++i) {
+    const mrt_material& m = d->materials[i];
+    if (m.color_tex || m.metallic_tex || m.roughness_tex || m.transmission_tex || m.ao_tex ||
+        m.emission_strength_tex || m.emission_color_tex || m.normal_tex)
+      return set_err(MRT_ERR_INVALID, "material %d: textures are not supported by the CUDA path yet", i);
+  }
   c->has_scene = false;
   if (c->diff) {
     cudaStreamSynchronize(c->stream);

@@ -20,7 +20,7 @@ HERE = Path(__file__).resolve().parent
 LIB_PATH = HERE / "libmrt.so"
 MINIRT_LIB_PATH = HERE / "libmrt_minirt.so"
 
-MRT_ABI_VERSION = 3
+MRT_ABI_VERSION = 4
 
 MRT_OK = 0
 STATUS_NAMES = {
@@ -38,11 +38,23 @@ f64x3 = C.c_double * 3
 f32x3 = C.c_float * 3
 
 
+TEX_IMAGE, TEX_HDR, TEX_COLOR, TEX_CHECKER_LOCAL, TEX_CHECKER_GLOBAL = range(5)
+TEX_SLOTS = ["color_tex", "metallic_tex", "roughness_tex", "transmission_tex", "ao_tex",
+             "emission_strength_tex", "emission_color_tex", "normal_tex"]
+
+
+class Texture(C.Structure):
+    _fields_ = [("type", C.c_int32), ("width", C.c_uint32), ("height", C.c_uint32),
+                ("pad_", C.c_int32), ("rgba", C.POINTER(C.c_uint8)), ("checker_scale", C.c_double),
+                ("c1", u8x3), ("c2", u8x3), ("pad2_", C.c_uint8 * 2)]
+
+
 class Material(C.Structure):
     _fields_ = [("color", u8x3), ("emission_color", u8x3), ("pad_", C.c_uint8 * 2),
                 ("metallic", C.c_double), ("roughness", C.c_double), ("ior", C.c_double),
                 ("transmission", C.c_double), ("ao", C.c_double),
-                ("emission_strength", C.c_double), ("scale", C.c_double)]
+                ("emission_strength", C.c_double), ("scale", C.c_double)] + \
+        [(k, C.c_int32) for k in TEX_SLOTS] + [("normal_intensity", C.c_double)]
 
 
 class Sphere(C.Structure):
@@ -122,7 +134,8 @@ class SceneDesc(C.Structure):
                 ("pad2_", C.c_int32),
                 ("cylinders", C.POINTER(Cylinder)), ("cones", C.POINTER(Cone)),
                 ("hyperboloids", C.POINTER(Hyperboloid)), ("n_cylinders", C.c_int32),
-                ("n_cones", C.c_int32), ("n_hyperboloids", C.c_int32), ("pad3_", C.c_int32)]
+                ("n_cones", C.c_int32), ("n_hyperboloids", C.c_int32), ("n_textures", C.c_int32),
+                ("textures", C.POINTER(Texture))]
 
 
 class RenderParams(C.Structure):

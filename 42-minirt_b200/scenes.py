@@ -17,6 +17,8 @@ of the benchmark configurations:
       materials and a 512x256 sky (inverse rendering).
   q0  320x240, 64 spp, depth 8: two cylinders, two cones, two hyperboloids,
       two spheres and a ground plane (the reference's quadric objects).
+  t0  320x240, 64 spp, depth 8: image, checker and fallback textures, normal,
+      roughness, metallic, ao and emission maps (make_textured).
 
 Values use the reference's own types: 8-bit colours, RGBE sky texels,
 horizontal integer-degree field of view (viewport.c:57), so that the oracle and
@@ -69,6 +71,7 @@ class Scene:
     cylinders: list = field(default_factory=list)  # dicts: position, orientation, diameter, height, ...
     cones: list = field(default_factory=list)      # dicts: position (apex), orientation, diameter, height
     hyperboloids: list = field(default_factory=list)  # dicts: position, orientation, a, b, c, shape, height
+    textures: list = field(default_factory=list)  # dicts: type, rgba (H,W,4) uint8 | checker_scale, c1, c2
     ambient_ratio: float = 0.0
     ambient_color: tuple = (0, 0, 0)
     hdr: np.ndarray | None = None                 # (H,W,4) uint8 RGBE
@@ -130,7 +133,23 @@ class Scene:
             mats[i].ao = m.get("ao", 1.0)
             mats[i].emission_strength = m.get("emission_strength", 0.0)
             mats[i].scale = m.get("scale", 1.0)
+            for k in mrt.TEX_SLOTS:
+                setattr(mats[i], k, int(m.get(k, 0)))
+            mats[i].normal_intensity = m.get("normal_intensity", 1.0)
         keep.append(mats)
+        tx = (mrt.Texture * max(1, len(self.textures)))()
+        for i, t in enumerate(self.textures):
+            tx[i].type = t["type"]
+            if t.get("rgba") is not None:
+                px = np.ascontiguousarray(t["rgba"], np.uint8)
+                keep.append(px)
+                tx[i].height, tx[i].width = px.shape[0], px.shape[1]
+                tx[i].rgba = px.ctypes.data_as(C.POINTER(C.c_uint8))
+            tx[i].checker_scale = t.get("checker_scale", 1.0)
+            tx[i].c1[:] = t.get("c1", (0, 0, 0))
+            tx[i].c2[:] = t.get("c2", (0, 0, 0))
+        keep.append(tx)
+        d.textures, d.n_textures = tx, len(self.textures)
         d.materials, d.n_materials = mats, len(self.materials)
         sph = (mrt.Sphere * max(1, len(self.spheres)))()
         for i, (c, r, mi, col) in enumerate(self.spheres):
@@ -602,5 +621,88 @@ def make_quadrics(seed: int = 5, width: int = 320, height: int = 240, spp: int =
     return sc
 
 
+def make_textured(seed: int = 6, width: int = 320, height: int = 240, spp: int = 64, depth: int = 8,
+                  partial_alpha: bool = False) -> Scene:
+    """Textures and maps (t_tex / apply_all_map): a ground plane with a 3-D
+    checker, an image-textured sphere with cut-out (alpha 0) texels, a
+    uv-checker sphere, a metal sphere with roughness and normal maps, a
+    sphere with metallic and ao maps, an emissive sphere with emission
+    strength and colour maps, an image-textured quad of two triangles with
+    uvs, a cylinder with a uv checker, a sphere with an empty image (the
+    reference's fallback checker) and one with an HDR-type texture (black in
+    the reference). Every scalar-mapped material sits on one sphere only.
+    partial_alpha adds texels of alpha 128 to the cut-out image."""
+    rng = np.random.default_rng(seed)
+    aspect = width / height
+    sc = Scene("textured", width, height, spp, depth,
+               camera=dict(position=(0.0, 2.5, 11.0), orientation=look_at((0, 2.5, 11), (0, 1, 0)),
+                           fov=hfov_from_vfov(45.0, aspect)), seed=seed)
+
+    def tex(**t):
+        sc.textures.append(t)
+        return len(sc.textures)            # 1-based, as the ABI names textures
+
+    def mat(**m):
+        sc.materials.append(m)
+        return len(sc.materials) - 1
+
+    img = rng.integers(0, 256, (16, 16, 4), dtype=np.uint8)
+    img[..., 3] = 255
+    img[rng.uniform(size=(16, 16)) < 0.25, 3] = 0
+    if partial_alpha:
+        img[rng.uniform(size=(16, 16)) < 0.2, 3] = 128
+    t_img = tex(type=mrt.TEX_IMAGE, rgba=img)
+    t_uvck = tex(type=mrt.TEX_CHECKER_LOCAL, checker_scale=8.0, c1=(230, 60, 40), c2=(30, 40, 200))
+    t_glob = tex(type=mrt.TEX_CHECKER_GLOBAL, checker_scale=1.5, c1=(220, 220, 210), c2=(40, 40, 40))
+    nrm = np.zeros((8, 8, 4), np.uint8)
+    nrm[..., :2] = rng.integers(64, 192, (8, 8, 2))
+    nrm[..., 2] = rng.integers(200, 256, (8, 8))
+    nrm[..., 3] = 255
+    t_nrm = tex(type=mrt.TEX_IMAGE, rgba=nrm)
+
+    def grey(lo, hi, n=8):
+        g = np.zeros((n, n, 4), np.uint8)
+        g[..., :3] = rng.integers(lo, hi, (n, n))[..., None]
+        g[..., 3] = 255
+        return tex(type=mrt.TEX_IMAGE, rgba=g)
+
+    t_rough, t_metal, t_ao, t_es = grey(10, 120), grey(0, 256), grey(100, 256), grey(0, 256)
+    t_ec = tex(type=mrt.TEX_IMAGE, rgba=np.concatenate(
+        [rng.integers(0, 256, (4, 4, 3), dtype=np.uint8), np.full((4, 4, 1), 255, np.uint8)], axis=2))
+    t_empty = tex(type=mrt.TEX_IMAGE, rgba=None)
+    t_hdr = tex(type=mrt.TEX_HDR)
+
+    ground = mat(color=(200, 200, 200), metallic=0.0, ior=0.0, color_tex=t_glob, scale=1.0)
+    sc.planes.append(((0.0, 0.0, 0.0), (0.0, 1.0, 0.0), ground, (200, 200, 200)))
+    m_img = mat(color=(255, 255, 255), metallic=0.0, ior=0.0, color_tex=t_img)
+    m_uv = mat(color=(255, 255, 255), metallic=0.0, ior=0.0, color_tex=t_uvck, scale=2.0)
+    m_rough = mat(color=(210, 180, 120), metallic=1.0, roughness=0.3, roughness_tex=t_rough, normal_tex=t_nrm)
+    m_metal = mat(color=(120, 200, 160), metallic=0.5, roughness=0.2, ior=1.5, metallic_tex=t_metal,
+                  ao_tex=t_ao, normal_tex=t_nrm, normal_intensity=0.5)
+    m_emit = mat(color=(0, 0, 0), metallic=0.0, ior=0.0, emission_strength=6.0, emission_color=(255, 255, 255),
+                 emission_strength_tex=t_es, emission_color_tex=t_ec)
+    m_quad = mat(color=(255, 255, 255), metallic=0.0, ior=0.0, color_tex=t_img, scale=1.0)
+    m_cyl = mat(color=(255, 255, 255), metallic=0.0, ior=0.0, color_tex=t_uvck)
+    m_empty = mat(color=(255, 255, 255), metallic=0.0, ior=0.0, color_tex=t_empty)
+    m_hdr = mat(color=(255, 255, 255), metallic=0.0, ior=0.0, color_tex=t_hdr)
+    sc.spheres += [((-3.0, 1.0, 0.0), 1.0, m_img, (255, 255, 255)),
+                   ((-0.8, 0.8, 1.5), 0.8, m_uv, (255, 255, 255)),
+                   ((1.3, 1.0, 0.2), 1.0, m_rough, (255, 255, 255)),
+                   ((3.4, 0.7, 1.6), 0.7, m_metal, (255, 255, 255)),
+                   ((0.5, 5.5, 1.0), 0.6, m_emit, (0, 0, 0)),
+                   ((-1.9, 0.45, 3.2), 0.45, m_empty, (255, 255, 255)),
+                   ((2.2, 0.45, 3.4), 0.45, m_hdr, (255, 255, 255))]
+    pos = np.array([[-2.5, 0.0, -2.5], [2.5, 0.0, -2.5], [2.5, 3.5, -2.5], [-2.5, 3.5, -2.5]], np.float64)
+    nrm_v = np.tile([0.0, 0.0, 1.0], (4, 1))
+    uvs = np.array([[0.0, 1.0], [1.0, 1.0], [1.0, 0.0], [0.0, 0.0]], np.float64)
+    sc.meshes.append(MeshData(pos, nrm_v, np.array([[0, 1, 2], [0, 2, 3]], np.uint32), None, uvs, m_quad,
+                              (255, 255, 255)))
+    sc.cylinders.append(dict(position=(4.3, 1.0, -1.0), orientation=(0.0, 1.0, 0.0), diameter=1.0, height=2.0,
+                             material=m_cyl, color=(255, 255, 255)))
+    sc.lights.append(dict(position=(-2.0, 6.0, 5.0), brightness=0.7, color=(255, 255, 255)))
+    sc.ambient_ratio, sc.ambient_color = 0.25, (150, 170, 210)
+    return sc
+
+
 CONFIGS = {"c0": make_c0, "c1": make_c1, "c2": make_c2, "c2p": make_c2_progressive, "c4": make_c4,
-           "q0": make_quadrics}
+           "q0": make_quadrics, "t0": make_textured}

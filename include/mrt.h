@@ -36,7 +36,7 @@
 extern "C" {
 # endif
 
-# define MRT_ABI_VERSION 3
+# define MRT_ABI_VERSION 4
 
 # if defined(__GNUC__)
 #  define MRT_API __attribute__((visibility("default")))
@@ -59,9 +59,38 @@ typedef enum mrt_status
 
 /* ------------------------------------------------------------------ scene */
 
-/* t_mat (scene_structs.h:84-106), untextured fields. Colours are the 8-bit
- * values the reference stores; emission_color is emission_color_tmp, which
- * set_values_mat turns into emission_color = c / 255 (set_dependant_values_objs2.c:34). */
+/* t_tex (scene_structs.h:61-82), t_tex_type order (scene_structs.h:20-27). */
+typedef enum mrt_tex_type
+{
+	MRT_TEX_IMAGE = 0,          /* nearest texel of rgba (get_tex_color.c:31-37) */
+	MRT_TEX_HDR = 1,            /* the reference returns black for it (get_tex_color.c:46) */
+	MRT_TEX_COLOR = 2,          /* black, as the reference */
+	MRT_TEX_CHECKER_LOCAL = 3,  /* uv checker (get_tex_color.c:38-44) */
+	MRT_TEX_CHECKER_GLOBAL = 4  /* 3-D checker of the hit point (get_solid_texture.c:31) */
+}	mrt_tex_type;
+
+typedef struct mrt_texture
+{
+	int32_t			type;          /* mrt_tex_type */
+	uint32_t		width;         /* IMAGE */
+	uint32_t		height;
+	int32_t			pad_;
+	const uint8_t	*rgba;         /* IMAGE: 4 * width * height bytes, row-major, or NULL
+	                                * (a NULL or empty image reads the reference's
+	                                * magenta/black fallback checker) */
+	double			checker_scale; /* CHECKER_* */
+	uint8_t			c1[3];
+	uint8_t			c2[3];
+	uint8_t			pad2_[2];
+}	mrt_texture;
+
+/* t_mat (scene_structs.h:84-106). Colours are the 8-bit values the
+ * reference stores; emission_color is emission_color_tmp, which
+ * set_values_mat turns into emission_color = c / 255
+ * (set_dependant_values_objs2.c:34). The *_tex fields name a texture as
+ * 1 + its index in mrt_scene_desc.textures, 0 for none (so a zeroed struct
+ * is untextured); a texture replaces the value at each hit with its texel
+ * (the .r channel for scalars), as apply_all_map does (apply_map.c:60-85). */
 typedef struct mrt_material
 {
 	uint8_t	color[3];
@@ -74,6 +103,18 @@ typedef struct mrt_material
 	double	ao;                /* ambient occlusion factor, default 1 */
 	double	emission_strength;
 	double	scale;             /* uv scale, default 1 */
+	int32_t	color_tex;         /* texture colour and, for IMAGE, alpha: a texel of
+	                            * alpha a hides the object with probability
+	                            * 1 - a/255 (hit_register.c:62-72) */
+	int32_t	metallic_tex;
+	int32_t	roughness_tex;
+	int32_t	transmission_tex;  /* also read at shadow-ray hits (is_light) */
+	int32_t	ao_tex;
+	int32_t	emission_strength_tex;
+	int32_t	emission_color_tex;
+	int32_t	normal_tex;        /* tangent-space normal map (apply_map.c:38-58) */
+	double	normal_intensity;  /* lerp weight of the mapped normal; the reference's
+	                            * default is 1 */
 }	mrt_material;
 
 /* t_sphere (scene_structs.h:167-175); material < 0 means no material
@@ -259,7 +300,8 @@ typedef struct mrt_scene_desc
 	int32_t				n_cylinders;
 	int32_t				n_cones;
 	int32_t				n_hyperboloids;
-	int32_t				pad3_;
+	int32_t				n_textures;
+	const mrt_texture	*textures;
 }	mrt_scene_desc;
 
 /* ------------------------------------------------------------- rendering */

@@ -164,12 +164,28 @@ static v3 rnd_unit(rng_t *r)
 
 /* ---------------------------------------------------------------- scene */
 
+enum { TX_COLOR = 0, TX_METALLIC, TX_ROUGHNESS, TX_TRANSMISSION, TX_AO, TX_EMIS_STRENGTH,
+	TX_EMIS_COLOR, TX_NORMAL, TX_SLOTS };
+
 typedef struct
 {
 	uint8_t	c8[3];
 	double	metallic, roughness, ior, transmission, ao, emission_strength, scale;
 	fc		emission_color;
+	int		tex[TX_SLOTS];     /* 1 + texture index, 0 none */
+	double	normal_intensity;
+	int		textured;          /* any tex[] set */
 }	mat_t;
+
+/* t_tex (scene_structs.h:61-82) */
+typedef struct
+{
+	int			type;
+	uint32_t	w, h;
+	uint8_t		*rgba;
+	double		scale;
+	uint8_t		c1[3], c2[3];
+}	tex_t;
 
 enum { PT_SPHERE = 0, PT_TRI = 1, PT_CYL = 2, PT_CONE = 3, PT_HYP = 4 };
 
@@ -231,6 +247,10 @@ struct ro_scene
 	double		ior_all;
 	mat_t		*mats;
 	int			n_mats;
+	tex_t		*texs;
+	int			n_texs;
+	rng_t		*rg;                /* the path's random stream (alpha test) */
+	int			is_light;           /* tracing a shadow ray (apply_all_map's is_light) */
 	prim_t		*prims;             /* bvh_make_lst order */
 	int			n_prims;
 	uint32_t	*prim_idx;          /* prim_indices after the median build */
@@ -533,7 +553,17 @@ typedef struct
 	int		mat;
 	const uint8_t	*objcolor;
 	fc		color;
+	int		has_hm;     /* hm holds this hit's textured material values */
+	mat_t	hm;
 }	hrec_t;
+
+/* The material values at a hit: the material, or its copy with this hit's
+ * texels (apply_all_map writes them into the shared t_mat before every use,
+ * apply_map.c:60-85, which for one path at a time is the same thing). */
+static inline const mat_t *hmat(ro_scene *s, const hrec_t *h)
+{
+	return (h->has_hm ? &h->hm : &s->mats[h->mat]);
+}
 
 /* intersect_aabb (bvh_utils.c:38-59); also returns the entry distance. */
 static int isect_aabb(const ray_t *r, v3 mn, v3 mx, double *tentry)
@@ -1038,6 +1068,95 @@ static int hit_plane(ro_scene *s, plane_t *p, const ray_t *r, hrec_t *rec)
  * left-to-right in prim_indices order, that is: minimum t, ties to the lowest
  * leaf position. This traversal visits near children first and skips boxes
  * entered beyond the best t (strictly), which gives the same answer. */
+/* ------------------------------------------------------------ textures */
+
+/* get_solid_texture_default / get_solid_texture (get_solid_texture.c:15-43) */
+static fc solid_checker(v3 p, double scale, const uint8_t *c1, const uint8_t *c2)
+{
+	int	a, b, c;
+
+	p = vscale(p, scale);
+	a = floor(p.x);
+	b = floor(p.y + 0.5);
+	c = floor(p.z);
+	if ((a + b + c) % 2 == 0)
+		return (c2f(c1));
+	return (c2f(c2));
+}
+
+/* get_tex_color (get_tex_color.c:27-48); k is 1 + the texture index */
+static fc tex_color(ro_scene *s, int k, double u, double v, v3 point)
+{
+	static const uint8_t	black[3] = {0, 0, 0}, magenta[3] = {243, 0, 243};
+	tex_t					*t = &s->texs[k - 1];
+	int						a, b;
+
+	if (t->type == MRT_TEX_IMAGE)
+	{
+		const uint8_t	*px;
+
+		if (!t->rgba || !t->w || !t->h)
+			return (solid_checker(point, 2, black, magenta));
+		px = t->rgba + 4 * ((size_t)t->w * (int)(v * (t->h - 1)) + (int)(u * (t->w - 1)));
+		return ((fc){px[0] / 255.0, px[1] / 255.0, px[2] / 255.0});
+	}
+	if (t->type == MRT_TEX_CHECKER_LOCAL)
+	{
+		a = floor(u * t->scale);
+		b = floor(v * t->scale);
+		if ((a + b) % 2 == 0)
+			return (c2f(t->c1));
+		return (c2f(t->c2));
+	}
+	if (t->type == MRT_TEX_CHECKER_GLOBAL)
+		return (solid_checker(point, t->scale, t->c1, t->c2));
+	return ((fc){0.0, 0.0, 0.0});
+}
+
+/* get_tex_transparency (get_tex_color.c:51-62) */
+static double tex_transparency(ro_scene *s, int k, double u, double v)
+{
+	tex_t	*t = &s->texs[k - 1];
+
+	if (t->type != MRT_TEX_IMAGE || !t->rgba || !t->w || !t->h)
+		return (0.0);
+	return (1 - t->rgba[4 * ((size_t)t->w * (int)(v * (t->h - 1)) + (int)(u * (t->w - 1))) + 3] / 255.0);
+}
+
+/* Uniform of the partial-transparency test in counter mode: a hash of the
+ * path's stream state at the traversal and the object's flat id, the same
+ * function as the kernels' alpha_uniform. The reference draws
+ * random_double() here (hit_register.c:66-71), in the order of its
+ * exhaustive leaf recursion, which no culled traversal reproduces. */
+static double alpha_uniform(uint64_t key, uint32_t flat)
+{
+	uint64_t	z = key ^ ((uint64_t)(flat + 1) * 0x9E3779B97F4A7C15ULL);
+
+	z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+	z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+	z ^= z >> 31;
+	return (double)(float)((float)(z >> 40) * (1.0f / 16777216.0f));
+}
+
+/* The leaf's alpha test (hit_register_bvh, hit_register.c:62-72): 1 when
+ * the candidate hit is dropped. */
+static int alpha_drops(ro_scene *s, const hrec_t *h, uint32_t flat)
+{
+	double	tr;
+	rng_t	ref = {RO_RNG_REFERENCE, 0};
+
+	if (h->mat < 0 || !s->mats[h->mat].tex[TX_COLOR])
+		return (0);
+	tr = tex_transparency(s, s->mats[h->mat].tex[TX_COLOR], h->u, h->v);
+	if (tr == 1)
+		return (1);
+	if (tr == 0)
+		return (0);
+	if (s->rg && s->rg->mode == RO_RNG_COUNTER)
+		return (alpha_uniform(s->rg->state, flat) < tr);
+	return (rnd(s->rg ? s->rg : &ref) < tr);
+}
+
 static void bvh_closest(ro_scene *s, const ray_t *r, hrec_t *best, int *best_pos)
 {
 	uint32_t	stack[128];
@@ -1066,6 +1185,10 @@ static void bvh_closest(ro_scene *s, const ray_t *r, hrec_t *best, int *best_pos
 			memset(&tmp, 0, sizeof(tmp));
 			ok = hit_prim(s, p, r, &tmp);
 			if (!ok || tmp.t >= 1000)
+				continue ;
+			if (p->type == PT_SPHERE || p->type == PT_TRI)
+				tmp.mat = p->mat;
+			if (s->n_texs && alpha_drops(s, &tmp, p->flat))
 				continue ;
 			if (!best->hit || tmp.t < best->t || (tmp.t == best->t && (int)nd->first < *best_pos))
 			{
@@ -1118,11 +1241,76 @@ static int bvh_depth_count(ro_scene *s, const ray_t *r, uint32_t idx)
 	return c;
 }
 
-/* get_hit_register_color (get_hit_color.c:17-36) without textures. */
+/* apply_normal_map + init_tbn (apply_map.c:15-58): the texel in [-1, 1]
+ * (float arithmetic, as map.r / 127.5f - 1.0f) in the frame tangent =
+ * unit(n x (0,-1,0)) (or n x (0,0,1)), bitangent = unit(n x tangent), n. */
+static void normal_map(ro_scene *s, hrec_t *h, const mat_t *m)
+{
+	tex_t			*t = &s->texs[m->tex[TX_NORMAL] - 1];
+	const uint8_t	*px;
+	v3				mp, tg, bt, n = h->normal, res;
+
+	if (!t->rgba)
+		return ;
+	px = t->rgba + 4 * ((size_t)t->w * (int)(h->v * (t->h - 1)) + (int)(h->u * (t->w - 1)));
+	mp = (v3){(px[0] / 127.5f) - 1.0f, (px[1] / 127.5f) - 1.0f, (px[2] / 127.5f) - 1.0f};
+	tg = vcross(n, (v3){0, -1, 0});
+	if (vlen(tg) == 0)
+		tg = vcross(n, (v3){0, 0, 1});
+	tg = vunit(tg);
+	bt = vunit(vcross(n, tg));
+	res.x = mp.x * tg.x + mp.y * bt.x + mp.z * n.x;
+	res.y = mp.x * tg.y + mp.y * bt.y + mp.z * n.y;
+	res.z = mp.x * tg.z + mp.y * bt.z + mp.z * n.z;
+	if (m->normal_intensity == 1.0)
+		h->normal = vunit(res);
+	else
+	{
+		double	w = m->normal_intensity;
+		v3		b = vunit(res);
+
+		h->normal = vunit((v3){(1 - w) * n.x + w * b.x, (1 - w) * n.y + w * b.y, (1 - w) * n.z + w * b.z});
+	}
+}
+
+/* apply_all_map (apply_map.c:60-85) into the hit's own copy of the
+ * material: normal map, transmission, then (not for shadow rays) roughness,
+ * metallic, ao, emission strength and colour, each the texel's .r (the
+ * colour for emission colour). */
+static void apply_maps(ro_scene *s, hrec_t *h)
+{
+	const mat_t	*m;
+
+	if (h->mat < 0 || !s->mats[h->mat].textured)
+		return ;
+	m = &s->mats[h->mat];
+	h->hm = *m;
+	h->has_hm = 1;
+	if (m->tex[TX_NORMAL])
+		normal_map(s, h, m);
+	if (m->tex[TX_TRANSMISSION])
+		h->hm.transmission = tex_color(s, m->tex[TX_TRANSMISSION], h->u, h->v, h->point).r;
+	if (s->is_light)
+		return ;
+	if (m->tex[TX_ROUGHNESS])
+		h->hm.roughness = tex_color(s, m->tex[TX_ROUGHNESS], h->u, h->v, h->point).r;
+	if (m->tex[TX_METALLIC])
+		h->hm.metallic = tex_color(s, m->tex[TX_METALLIC], h->u, h->v, h->point).r;
+	if (m->tex[TX_AO])
+		h->hm.ao = tex_color(s, m->tex[TX_AO], h->u, h->v, h->point).r;
+	if (m->tex[TX_EMIS_STRENGTH])
+		h->hm.emission_strength = tex_color(s, m->tex[TX_EMIS_STRENGTH], h->u, h->v, h->point).r;
+	if (m->tex[TX_EMIS_COLOR])
+		h->hm.emission_color = tex_color(s, m->tex[TX_EMIS_COLOR], h->u, h->v, h->point);
+}
+
+/* get_hit_register_color (get_hit_color.c:17-36). */
 static fc hit_color(ro_scene *s, hrec_t *h)
 {
 	if (s->render_mode == 2)
 		return (fc){(h->normal.x + 1) * 0.5, (h->normal.z + 1) * 0.5, (h->normal.y + 1) * 0.5};
+	if (h->mat >= 0 && s->mats[h->mat].tex[TX_COLOR])
+		return tex_color(s, s->mats[h->mat].tex[TX_COLOR], h->u, h->v, h->point);
 	if (h->mat >= 0 && s->albedo_d)
 		return (fc){s->albedo_d[3 * h->mat], s->albedo_d[3 * h->mat + 1], s->albedo_d[3 * h->mat + 2]};
 	if (h->mat >= 0)
@@ -1143,7 +1331,10 @@ static int hit_register_all_(ro_scene *s, const ray_t *r, hrec_t *out, int *bvh_
 	if (bvh_hit)
 		*bvh_hit = best.hit;
 	if (best.hit)
+	{
+		apply_maps(s, &best);
 		best.color = hit_color(s, &best);
+	}
 	for (int i = 0; i < s->n_planes; i++)
 	{
 		memset(&tmp, 0, sizeof(tmp));
@@ -1155,6 +1346,7 @@ static int hit_register_all_(ro_scene *s, const ray_t *r, hrec_t *out, int *bvh_
 				tmp.prim = -1 - i;
 				tmp.mat = s->planes[i].mat;
 				tmp.objcolor = s->planes[i].color;
+				apply_maps(s, &tmp);
 				tmp.color = hit_color(s, &tmp);
 				best = tmp;
 			}
@@ -1599,7 +1791,7 @@ static double fresnel_f(double ct, double f0) { return f0 + ((1 - f0) * powf(1 -
 static void metallic(rng_t *rg, ro_scene *s, ray_t *r, hrec_t *h, fc *power)
 {
 	double	ct = cos_theta_in(r->dir, h->normal);
-	v3		m = s->mats[h->mat].roughness > 0.0 ? ggx_sample(rg, h->normal, s->mats[h->mat].roughness)
+	v3		m = hmat(s, h)->roughness > 0.0 ? ggx_sample(rg, h->normal, hmat(s, h)->roughness)
 		: h->normal;
 
 	r->dir = vunit(vsub(r->dir, vscale(m, 2 * vdot(r->dir, m))));
@@ -1612,7 +1804,7 @@ static void metallic(rng_t *rg, ro_scene *s, ray_t *r, hrec_t *h, fc *power)
 /* reflected_dielectric_color (dielectric.c:15-33). */
 static void dielectric_reflect(rng_t *rg, ro_scene *s, ray_t *r, hrec_t *h)
 {
-	v3	m = s->mats[h->mat].roughness > 0.0 ? ggx_sample(rg, h->normal, s->mats[h->mat].roughness)
+	v3	m = hmat(s, h)->roughness > 0.0 ? ggx_sample(rg, h->normal, hmat(s, h)->roughness)
 		: h->normal;
 
 	r->dir = vunit(vsub(r->dir, vscale(m, 2 * vdot(r->dir, m))));
@@ -1621,7 +1813,7 @@ static void dielectric_reflect(rng_t *rg, ro_scene *s, ray_t *r, hrec_t *h)
 /* refracted_ray + refracted_value + refracted_v (refraction.c:15-78). */
 static void refract_ray(rng_t *rg, ro_scene *s, ray_t *r, hrec_t *h, fc *power)
 {
-	mat_t	*m = &s->mats[h->mat];
+	const mat_t	*m = hmat(s, h);
 	double	eta = h->front_face ? s->ior_all / m->ior : m->ior / s->ior_all;
 	double	ct, st;
 	v3		perp, d;
@@ -1664,8 +1856,13 @@ static v3 cos_hemisphere(rng_t *rg, v3 *n)
 
 static int shadow_any(ro_scene *s, const ray_t *r, hrec_t *h)
 {
+	int	hit;
+
 	s->cnt.shadow_rays++;
-	return hit_register_all(s, r, h);
+	s->is_light = 1;
+	hit = hit_register_all(s, r, h);
+	s->is_light = 0;
+	return hit;
 }
 
 /* compute_light_v2 (light_manager.c:59-71) with add_all_light_contribution
@@ -1800,7 +1997,7 @@ static void env_nee(rng_t *rg, ro_scene *s, ray_t *r, hrec_t *h, fc *power, fc *
 			return ;
 		rad = background(s, *r, 0);
 		if (h->mat >= 0)
-			rad = fscale(rad, s->mats[h->mat].ao);
+			rad = fscale(rad, hmat(s, h)->ao);
 		rad = fscale(fmul(rad, *power), ctd / pdfd);
 		*acc = fadd(*acc, rad);
 		*power = fscale(*power, 1 - ctd);
@@ -1812,7 +2009,7 @@ static void env_nee(rng_t *rg, ro_scene *s, ray_t *r, hrec_t *h, fc *power, fc *
 		return ;
 	rad = background(s, *r, 0);
 	if (h->mat >= 0)
-		rad = fscale(rad, s->mats[h->mat].ao);
+		rad = fscale(rad, hmat(s, h)->ao);
 	rad = fmul(rad, *power);
 	rad = fscale(rad, ct / (pdf));
 	*acc = fadd(*acc, rad);
@@ -1836,7 +2033,7 @@ static void default_mat(rng_t *rg, ro_scene *s, ray_t *r, hrec_t *h, fc *power, 
 /* dielectric_mat (dielectric.c:37-64). */
 static void dielectric_mat(rng_t *rg, ro_scene *s, ray_t *r, hrec_t *h, fc *power, fc *acc)
 {
-	mat_t	*m = &s->mats[h->mat];
+	const mat_t	*m = hmat(s, h);
 
 	if (m->ior > 0)
 	{
@@ -1861,14 +2058,14 @@ static void dielectric_mat(rng_t *rg, ro_scene *s, ray_t *r, hrec_t *h, fc *powe
 /* material_manager_v3 (path_trace.c:15-35). */
 static void material_manager(rng_t *rg, ro_scene *s, ray_t *r, hrec_t *h, fc *power, fc *acc)
 {
-	mat_t	*m;
+	const mat_t	*m;
 
 	if (h->mat < 0)
 	{
 		default_mat(rg, s, r, h, power, acc);
 		return ;
 	}
-	m = &s->mats[h->mat];
+	m = hmat(s, h);
 	if (m->emission_strength > 0)
 		*acc = fadd(*acc, fmul(fscale(m->emission_color, m->emission_strength), *power));
 	if (m->metallic == 1.0)
@@ -1930,7 +2127,7 @@ static fc path_trace(rng_t *rg, ro_scene *s, ray_t r, int depth)
 			fc	bg = background(s, r, 1);
 
 			if (h.mat >= 0)
-				acc = fadd(acc, fmul(fscale(bg, s->mats[h.mat].ao), power));
+				acc = fadd(acc, fmul(fscale(bg, hmat(s, &h)->ao), power));
 			else
 				acc = fadd(acc, fmul(bg, power));
 			put_event(k, s, &h, 0, &r, power, acc);
@@ -1961,6 +2158,7 @@ static fc sample_pixel(rng_t *rg, ro_scene *s, uint32_t i, double ox, double oy)
 	ray_t	r;
 	hrec_t	h;
 
+	s->rg = rg;
 	if (s->defocus_angle <= 0)
 		r.orig = s->cam_pos;
 	else
@@ -1976,7 +2174,22 @@ static fc sample_pixel(rng_t *rg, ro_scene *s, uint32_t i, double ox, double oy)
 
 /* trace_single_photon_path + material_manager_v3_phothon
  * (trace_photon_path.c:18-72), dielectric_mat_photon (dielectric.c:66-91). */
+static int trace_photon_(rng_t *rg, ro_scene *s, v3 lp, fc p0, photon_t *out);
+
+/* Photon paths trace with is_light set (init_single_photon_path,
+ * trace_photon_path.c:42): only normal and transmission maps apply. */
 static int trace_photon(rng_t *rg, ro_scene *s, v3 lp, fc p0, photon_t *out)
+{
+	int	stored;
+
+	s->rg = rg;
+	s->is_light = 1;
+	stored = trace_photon_(rg, s, lp, p0, out);
+	s->is_light = 0;
+	return stored;
+}
+
+static int trace_photon_(rng_t *rg, ro_scene *s, v3 lp, fc p0, photon_t *out)
 {
 	ray_t	r;
 	fc		pw = p0;
@@ -1998,7 +2211,7 @@ static int trace_photon(rng_t *rg, ro_scene *s, v3 lp, fc p0, photon_t *out)
 		}
 		else
 		{
-			mat_t	*m = &s->mats[h.mat];
+			const mat_t	*m = hmat(s, &h);
 			int		as_metal;
 
 			if (m->metallic == 1.0)
@@ -2159,6 +2372,25 @@ ro_scene	*ro_create(const mrt_scene_desc *d)
 	s->max_bounces = d->max_bounces;
 	s->one_sided = d->triangle_one_sided;
 	s->ior_all = d->ior_all;
+	s->n_texs = (d->n_textures > 0 && d->textures) ? d->n_textures : 0;
+	s->texs = calloc(s->n_texs + 1, sizeof(tex_t));
+	for (int i = 0; i < s->n_texs; i++)
+	{
+		const mrt_texture	*t = &d->textures[i];
+		tex_t				*o = &s->texs[i];
+
+		o->type = t->type;
+		o->scale = t->checker_scale;
+		memcpy(o->c1, t->c1, 3);
+		memcpy(o->c2, t->c2, 3);
+		if (t->rgba && t->width && t->height)
+		{
+			o->w = t->width;
+			o->h = t->height;
+			o->rgba = malloc(4 * (size_t)t->width * t->height);
+			memcpy(o->rgba, t->rgba, 4 * (size_t)t->width * t->height);
+		}
+	}
 	s->n_mats = d->n_materials;
 	s->mats = calloc(d->n_materials + 1, sizeof(mat_t));
 	for (int i = 0; i < d->n_materials; i++)
@@ -2175,6 +2407,16 @@ ro_scene	*ro_create(const mrt_scene_desc *d)
 		o->emission_strength = m->emission_strength;
 		o->scale = m->scale;
 		o->emission_color = c2f(m->emission_color);
+		{
+			const int32_t	*tx = &m->color_tex;   /* color_tex .. normal_tex, in TX_ order */
+
+			for (int k = 0; k < TX_SLOTS; k++)
+			{
+				o->tex[k] = (tx[k] > 0 && tx[k] <= s->n_texs) ? tx[k] : 0;
+				o->textured |= o->tex[k] != 0;
+			}
+			o->normal_intensity = m->normal_intensity;
+		}
 	}
 	/* primitive order of bvh_make_lst (bvh_make_lst.c:46-65) over the object
 	 * list spheres, cylinders, cones, hyperboloids, then one custom object
@@ -2356,6 +2598,9 @@ void	ro_destroy(ro_scene *s)
 {
 	if (!s)
 		return ;
+	for (int i = 0; i < s->n_texs; i++)
+		free(s->texs[i].rgba);
+	free(s->texs);
 	free(s->mats);
 	free(s->prims);
 	free(s->prim_idx);

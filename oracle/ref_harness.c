@@ -80,6 +80,44 @@ static t_vec3	v3(const double *p)
 	return ((t_vec3){p[0], p[1], p[2]});
 }
 
+/* texture k (1-based, 0 none) of the scene's t_tex array */
+static t_tex	*tex_ptr(t_scene *sc, int32_t k)
+{
+	if (k <= 0 || k > sc->tex_amount)
+		return (NULL);
+	return (&sc->textures[k - 1]);
+}
+
+/* t_tex from an mrt_texture (scene_structs.h:61-82); the image copied */
+static void	fill_texture(t_tex *o, const mrt_texture *t, int i)
+{
+	snprintf(o->name, sizeof(o->name), "t%d", i);
+	o->type = (t_tex_type)t->type;
+	o->checker.scale = t->checker_scale;
+	o->checker.c1 = c3(t->c1);
+	o->checker.c2 = c3(t->c2);
+	if (t->rgba && t->width && t->height)
+	{
+		o->img.width = t->width;
+		o->img.height = t->height;
+		o->img.rgba = malloc(sizeof(t_rgba) * (size_t)t->width * t->height);
+		memcpy(o->img.rgba, t->rgba, 4 * (size_t)t->width * t->height);
+	}
+}
+
+static void	fill_material_tex(t_scene *sc, t_mat *m, const mrt_material *s)
+{
+	m->color_tex = tex_ptr(sc, s->color_tex);
+	m->metallic_tex = tex_ptr(sc, s->metallic_tex);
+	m->roughness_tex = tex_ptr(sc, s->roughness_tex);
+	m->transmission_tex = tex_ptr(sc, s->transmission_tex);
+	m->ao_tex = tex_ptr(sc, s->ao_tex);
+	m->emission_strength_tex = tex_ptr(sc, s->emission_strength_tex);
+	m->emission_color_tex = tex_ptr(sc, s->emission_color_tex);
+	m->normal = tex_ptr(sc, s->normal_tex);
+	m->normal_intensity = s->normal_intensity;
+}
+
 static void	fill_material(t_mat *m, const mrt_material *s, int i)
 {
 	snprintf(m->name, sizeof(m->name), "m%d", i);
@@ -253,8 +291,15 @@ void	*refh_create(const mrt_scene_desc *d)
 	strcpy(sc->name, "flat");
 	sc->mat_amount = d->n_materials;
 	sc->materials = calloc(d->n_materials + 1, sizeof(t_mat));
+	sc->tex_amount = (d->n_textures > 0 && d->textures) ? d->n_textures : 0;
+	sc->textures = calloc(sc->tex_amount + 1, sizeof(t_tex));
+	for (int i = 0; i < sc->tex_amount; i++)
+		fill_texture(&sc->textures[i], &d->textures[i], i);
 	for (int i = 0; i < d->n_materials; i++)
+	{
 		fill_material(&sc->materials[i], &d->materials[i], i);
+		fill_material_tex(sc, &sc->materials[i], &d->materials[i]);
+	}
 	ngroups = 0;
 	for (int i = 0; i < d->n_meshes; i++)
 		ngroups += count_groups(&d->meshes[i]);

@@ -30,6 +30,7 @@ CASES = {
     "c1": dict(make=lambda: scenes.make_c1(1, 24, 16, depth=6, freq=12, sky=(48, 24)), spp=2),
     "c2": dict(make=lambda: scenes.make_c2(2, 24, 16, depth=6, grid=16, photons=3000), spp=2),
     "q0": dict(make=lambda: scenes.make_quadrics(5, 32, 24, depth=6), spp=4),
+    "t0": dict(make=lambda: scenes.make_textured(6, 32, 24, depth=6), spp=4),
 }
 
 
@@ -43,6 +44,10 @@ def scene_digest(sc) -> str:
         h.update(repr(p).encode())
     for q in sc.cylinders + sc.cones + sc.hyperboloids:
         h.update(repr(sorted(q.items())).encode())
+    for t in sc.textures:
+        h.update(repr(sorted((k, v) for k, v in t.items() if k != "rgba")).encode())
+        if t.get("rgba") is not None:
+            h.update(np.ascontiguousarray(t["rgba"]).tobytes())
     for m in sc.meshes:
         for a in (m.positions, m.normals, m.indices, m.tri_material):
             if a is not None:

@@ -43,7 +43,7 @@ def test_library_loads_and_exports_every_declared_symbol(mrt):
 def test_ctypes_layouts_match_c(mrt):
     structs = {"mrt_material": mrt.Material, "mrt_sphere": mrt.Sphere, "mrt_plane": mrt.Plane,
                "mrt_mesh": mrt.Mesh, "mrt_cylinder": mrt.Cylinder, "mrt_cone": mrt.Cone,
-               "mrt_hyperboloid": mrt.Hyperboloid, "mrt_light": mrt.Light, "mrt_camera": mrt.Camera,
+               "mrt_hyperboloid": mrt.Hyperboloid, "mrt_texture": mrt.Texture, "mrt_light": mrt.Light, "mrt_camera": mrt.Camera,
                "mrt_ambient": mrt.Ambient, "mrt_caustic": mrt.Caustic,
                "mrt_scene_desc": mrt.SceneDesc, "mrt_render_params": mrt.RenderParams,
                "mrt_render_stats": mrt.RenderStats, "mrt_ray": mrt.Ray, "mrt_hit": mrt.Hit,
@@ -54,6 +54,8 @@ def test_ctypes_layouts_match_c(mrt):
     src += '  printf("off_scene_materials %zu\\n", offsetof(mrt_scene_desc, materials));\n'
     src += '  printf("off_scene_lights %zu\\n", offsetof(mrt_scene_desc, lights));\n'
     src += '  printf("off_scene_hyperboloids %zu\\n", offsetof(mrt_scene_desc, hyperboloids));\n'
+    src += '  printf("off_scene_textures %zu\\n", offsetof(mrt_scene_desc, textures));\n'
+    src += '  printf("off_mat_normal_intensity %zu\\n", offsetof(mrt_material, normal_intensity));\n'
     src += "  return 0;}\n"
     with tempfile.TemporaryDirectory() as d:
         c = Path(d) / "sizes.c"
@@ -67,6 +69,8 @@ def test_ctypes_layouts_match_c(mrt):
     assert int(got["off_scene_materials"]) == mrt.SceneDesc.materials.offset
     assert int(got["off_scene_lights"]) == mrt.SceneDesc.lights.offset
     assert int(got["off_scene_hyperboloids"]) == mrt.SceneDesc.hyperboloids.offset
+    assert int(got["off_scene_textures"]) == mrt.SceneDesc.textures.offset
+    assert int(got["off_mat_normal_intensity"]) == mrt.Material.normal_intensity.offset
 
 
 def test_null_context_is_rejected_with_invalid(mrt):

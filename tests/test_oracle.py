@@ -21,14 +21,14 @@ def mg():
     return make_golden
 
 
-@pytest.mark.parametrize("name", ["c0", "c1", "c2", "q0"])
+@pytest.mark.parametrize("name", ["c0", "c1", "c2", "q0", "t0"])
 def test_scene_generator_is_deterministic(mg, name):
     g = golden(f"{name}_pins.npz")
     sc = mg.CASES[name]["make"]()
     assert mg.scene_digest(sc) == str(g["digest"])
 
 
-@pytest.mark.parametrize("name", ["c0", "c1", "c2", "q0"])
+@pytest.mark.parametrize("name", ["c0", "c1", "c2", "q0", "t0"])
 def test_first_hits_match_reference_golden(mg, oracle, name):
     g = golden(f"{name}_pins.npz")
     sc = mg.CASES[name]["make"]()
@@ -40,7 +40,7 @@ def test_first_hits_match_reference_golden(mg, oracle, name):
     assert (g["hit_prim"] >= 0).sum() > 100
 
 
-@pytest.mark.parametrize("name", ["c0", "c1", "c2", "q0"])
+@pytest.mark.parametrize("name", ["c0", "c1", "c2", "q0", "t0"])
 def test_render_matches_reference_golden_bit_exact(mg, oracle, name):
     g = golden(f"{name}_pins.npz")
     sc = mg.CASES[name]["make"]()
@@ -104,7 +104,7 @@ def test_pcg_stream_matches_python_restatement(oracle):
         np.testing.assert_array_equal(oracle.pcg_stream(*args, 16), stream(*args, 16))
 
 
-@pytest.mark.parametrize("name,seed", [("c0", 11), ("c1", 12), ("c2", 13), ("q0", 14)])
+@pytest.mark.parametrize("name,seed", [("c0", 11), ("c1", 12), ("c2", 13), ("q0", 14), ("t0", 15)])
 def test_restatement_matches_live_reference(mg, oracle, has_reference, name, seed):
     if not has_reference:
         pytest.skip("reference not built here (oracle/_ref)")
