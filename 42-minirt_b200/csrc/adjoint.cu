@@ -713,6 +713,9 @@ cudaError_t launch_adjoint_chunk(const SceneView& S, const AdjointArgs& A, TapeE
   if (e != cudaSuccess) return e;
   return with_view(S, [&](const auto& v) -> cudaError_t {
     using VT = std::decay_t<decltype(v)>;
+    if constexpr (VT::kTextures) {
+      return cudaErrorNotSupported;   // mrt_forward / mrt_backward refuse textured scenes
+    } else {
     cudaError_t e2 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, adj_replay_kernel<kBlock, VT>, kBlock, 0);
     if (e2 != cudaSuccess) return e2;
     const uint64_t want = (A.n_paths + kBlock - 1) / kBlock;
@@ -728,6 +731,7 @@ cudaError_t launch_adjoint_chunk(const SceneView& S, const AdjointArgs& A, TapeE
       if ((e2 = cudaGetLastError()) != cudaSuccess) return e2;
     }
     return cudaSuccess;
+    }
   });
 }
 

@@ -143,6 +143,9 @@ struct mrt_ctx {
   DevBuf<PlaneD> planes;
   DevBuf<MaterialD> mats;
   DevBuf<LightD> lights;
+  DevBuf<MatTexD> mat_tex;
+  DevBuf<TexD> texs;
+  DevBuf<uchar4> texels;
   DevBuf<int> point_lights;
   int n_point_lights = 0;
   DevBuf<uint32_t> rgbe;
@@ -455,11 +458,23 @@ extern "C" int mrt_scene_build(mrt_ctx* c, const mrt_scene_desc* d) {
       (d->n_cylinders && !d->cylinders) || (d->n_cones && !d->cones) ||
       (d->n_hyperboloids && !d->hyperboloids))
     return set_err(MRT_ERR_INVALID, "null element array with a non-zero count");
+  if (d->n_textures < 0 || (d->n_textures && !d->textures))
+    return set_err(MRT_ERR_INVALID, "bad texture array");
+  for (int i = 0; i < d->n_textures; ++i) {
+    const mrt_texture& t = d->textures[i];
+    if (t.type < MRT_TEX_IMAGE || t.type > MRT_TEX_CHECKER_GLOBAL)
+      return set_err(MRT_ERR_INVALID, "texture %d: unknown type %d", i, t.type);
+    if (t.rgba && (uint64_t)t.width * t.height > (1ull << 28))
+      return set_err(MRT_ERR_INVALID, "texture %d: %ux%u texels is too large", i, t.width, t.height);
+    if (!std::isfinite(t.checker_scale))
+      return set_err(MRT_ERR_INVALID, "texture %d: checker scale is not finite", i);
+  }
   for (int i = 0; i < d->n_materials; ++i) {
-    const mrt_material& m = d->materials[i];
-    if (m.color_tex || m.metallic_tex || m.roughness_tex || m.transmission_tex || m.ao_tex ||
-        m.emission_strength_tex || m.emission_color_tex || m.normal_tex)
-      return set_err(MRT_ERR_INVALID, "material %d: textures are not supported by the CUDA path yet", i);
+    const int32_t* tx = &d->materials[i].color_tex;   // color_tex .. normal_tex
+    for (int k = 0; k < TS_COUNT; ++k)
+      if (tx[k] < 0 || tx[k] > d->n_textures)
+        return set_err(MRT_ERR_INVALID, "material %d: texture slot %d names texture %d of %d", i, k, tx[k],
+                       d->n_textures);
   }
   c->has_scene = false;
   if (c->diff) {
@@ -719,6 +734,58 @@ extern "C" int mrt_scene_build(mrt_ctx* c, const mrt_scene_desc* d) {
   CK(c->planes.upload(planes.data(), planes.size(), st));
   CK(c->mats.upload(mats.data(), mats.size(), st));
   CK(c->lights.upload(lights.data(), lights.size(), st));
+  // textures: RGBA8 images back to back, per-material slots
+  {
+    std::vector<TexD> texs(std::max(1, d->n_textures));
+    std::vector<uchar4> texels;
+    for (int i = 0; i < d->n_textures; ++i) {
+      const mrt_texture& t = d->textures[i];
+      TexD& o = texs[i];
+      o = TexD{};
+      o.type = t.type;
+      o.scale = (float)t.checker_scale;
+      for (int k = 0; k < 3; ++k) {
+        o.c1[k] = (float)(t.c1[k] / 255.0);
+        o.c2[k] = (float)(t.c2[k] / 255.0);
+      }
+      if (t.rgba && t.width && t.height) {
+        o.w = (int)t.width;
+        o.h = (int)t.height;
+        o.offset = (uint32_t)texels.size();
+        const size_t n = (size_t)t.width * t.height;
+        texels.resize(texels.size() + n);
+        std::memcpy(texels.data() + o.offset, t.rgba, 4 * n);
+      }
+    }
+    if (texels.empty()) texels.push_back(uchar4{0, 0, 0, 0});
+    std::vector<MatTexD> mt(std::max(1, d->n_materials));
+    bool any = false;
+    for (int i = 0; i < d->n_materials; ++i) {
+      const mrt_material& m = d->materials[i];
+      const int32_t* tx = &m.color_tex;
+      MatTexD& o = mt[i];
+      o = MatTexD{};
+      for (int k = 0; k < TS_COUNT; ++k) {
+        o.tex[k] = tx[k];
+        o.any |= tx[k] != 0;
+      }
+      o.normal_intensity = (float)m.normal_intensity;
+      o.uv_scale = (float)m.scale;
+      if (o.tex[TS_COLOR]) {
+        const TexD& t = texs[o.tex[TS_COLOR] - 1];
+        if (t.type == MRT_TEX_IMAGE && t.w > 0)
+          for (size_t q = 0; q < (size_t)t.w * t.h && !o.alpha; ++q) o.alpha = texels[t.offset + q].w < 255;
+      }
+      any = any || o.any;
+    }
+    CK(c->texs.upload(texs.data(), texs.size(), st));
+    CK(c->texels.upload(texels.data(), texels.size(), st));
+    CK(c->mat_tex.upload(mt.data(), mt.size(), st));
+    v.texs = c->texs.p;
+    v.texels = c->texels.p;
+    v.mat_tex = c->mat_tex.p;
+    v.has_textures = any ? 1 : 0;
+  }
   CK(c->point_lights.upload(point_lights.data(), point_lights.size(), st));
   c->n_point_lights = (int)point_lights.size();
   v.nodes = c->nodes.p;
@@ -943,6 +1010,10 @@ extern "C" int mrt_render(mrt_ctx* c, const mrt_render_params* p, mrt_render_sta
   const int block_size = p->block_size ? p->block_size : (tuned ? c->auto_block : 0);
   const int queue_capacity = p->queue_capacity ? p->queue_capacity : (tuned ? c->auto_capacity : 0);
   const int sort_threshold = p->sort_threshold ? p->sort_threshold : (tuned ? c->auto_sort : 0);
+  if (form == MRT_FORM_WAVEFRONT && v.has_textures) {
+    if (!tuned) return set_err(MRT_ERR_INVALID, "textured scenes render with the megakernel forms");
+    form = MRT_FORM_MEGAKERNEL;
+  }
   if (form == MRT_FORM_WAVEFRONT && p->render_mode == 0) {
     L.sample_base = (uint32_t)p->sample_base;
     if (!c->wf) c->wf = wf_create();
@@ -1054,9 +1125,10 @@ extern "C" int mrt_render_batch(mrt_ctx** ctxs, const mrt_render_params* params,
   for (int i = 0; i < n; ++i)
     if (ctxs[i]->stream != st) CK(cudaStreamSynchronize(ctxs[i]->stream));
   CK(cudaEventRecord(c0->ev0, st));
-  bool quadrics = false;
-  for (int i = 0; i < n; ++i) quadrics = quadrics || ctxs[i]->view.has_quadrics;
-  CK(launch_megakernel_batch(dv, di, n, total, c0->status.p, c0->counters.p + 7, params[0].block_size, quadrics,
+  int kind = 0;
+  for (int i = 0; i < n; ++i)
+    kind = std::max(kind, ctxs[i]->view.has_textures ? 2 : (ctxs[i]->view.has_quadrics ? 1 : 0));
+  CK(launch_megakernel_batch(dv, di, n, total, c0->status.p, c0->counters.p + 7, params[0].block_size, kind,
                              st));
   CK(cudaEventRecord(c0->ev1, st));
   CK(cudaFreeAsync(dv, st));
@@ -1091,8 +1163,9 @@ extern "C" int mrt_tune(mrt_ctx* c, int32_t spp, uint64_t seed, mrt_tune_result*
     if (out->n < MRT_TUNE_MAX) out->entry[out->n++] = mrt_tune_entry{form, block, cap, sort, 0.0};
   };
   for (int b : {64, 128, 256}) add(MRT_FORM_MEGAKERNEL, b, 0, 0);
-  for (int cap : {1 << 20, 1 << 21, 1 << 22})
-    for (int sort : {1 << 30, 1 << 16}) add(MRT_FORM_WAVEFRONT, 0, cap, sort);
+  if (!c->view.has_textures)   // the wavefront has no textured instantiation
+    for (int cap : {1 << 20, 1 << 21, 1 << 22})
+      for (int sort : {1 << 30, 1 << 16}) add(MRT_FORM_WAVEFRONT, 0, cap, sort);
   int best = -1;
   for (int i = 0; i < out->n; ++i) {
     mrt_tune_entry& t = out->entry[i];
@@ -1378,6 +1451,8 @@ int diff_check(mrt_ctx* c, const float* theta, const mrt_render_params* p) {
                    kDiffMaxMats);
   if (c->view.has_env && c->view.env_inv_gamma != 1.0f)
     return set_err(MRT_ERR_INVALID, "a differentiable sky needs a linear HDR (gamma 1)");
+  if (c->view.has_textures)
+    return set_err(MRT_ERR_INVALID, "textured materials are not differentiable (their texels are not parameters)");
   return MRT_OK;
 }
 

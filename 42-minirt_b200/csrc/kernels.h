@@ -46,10 +46,11 @@ cudaError_t launch_megakernel(const SceneView& S, const LaunchParams& L, float4*
 cudaError_t launch_megakernel_regen(const SceneView& S, const LaunchParams& L, float4* accum,
                                     int* status, unsigned long long* work, int block, int blocks_per_sm,
                                     cudaStream_t st);
-// quadrics: some scene of the batch has cylinders, cones or hyperboloids
+// kind: 2 when some scene of the batch has textures, 1 when some has
+// cylinders, cones or hyperboloids, else 0 (the view type instantiated)
 cudaError_t launch_megakernel_batch(const SceneView* views, const BatchItem* items, int n_items,
                                     uint64_t total, int* status, unsigned long long* work, int block,
-                                    bool quadrics, cudaStream_t st);
+                                    int kind, cudaStream_t st);
 cudaError_t launch_path_events(const SceneView& S, const LaunchParams& L, const int* pix, const int* smp,
                                int n, float* ev, float* rgb, int* status, cudaStream_t st);
 cudaError_t launch_first_hit(const SceneView& S, const double* rays, int64_t n, HitOut* out,

@@ -58,6 +58,31 @@ struct MaterialD {
   float alpha4;          // roughness^4 for the GGX-like sampler (utils.c:47-48)
 };
 
+// Texture (t_tex): type as mrt_tex_type; an IMAGE's texels are
+// texels[offset, offset + w*h) as RGBA8, w = 0 for a missing image.
+struct TexD {
+  int type;
+  int w, h;
+  uint32_t offset;
+  float c1[3], c2[3];    // checker colours / 255
+  float scale;           // checker scale
+  int pad;
+};
+
+// Texture slots of a material (1 + texture index, 0 none), in the order of
+// mrt_material's *_tex fields.
+enum TexSlot : int {
+  TS_COLOR = 0, TS_METALLIC, TS_ROUGHNESS, TS_TRANSMISSION, TS_AO, TS_EMIS_STRENGTH, TS_EMIS_COLOR,
+  TS_NORMAL, TS_COUNT
+};
+struct MatTexD {
+  int tex[TS_COUNT];
+  float normal_intensity;
+  float uv_scale;        // t_mat.scale (uv tiling)
+  int any;               // some slot is set
+  int alpha;             // the colour texture is an image with a texel of alpha < 255
+};
+
 struct LightD {
   float pos[3];          // point: position; directional: unit orientation
   float brightness;
@@ -81,6 +106,7 @@ struct PlaneD {
 // stay out of the kernels of scenes without quadrics.
 struct SceneView {
   static constexpr bool kQuadrics = false;
+  static constexpr bool kTextures = false;
   const Node* nodes;
   const float4* geom;
   const int4* meta;
@@ -97,6 +123,10 @@ struct SceneView {
   int root_leaf;         // scene with a single leaf: the link of that leaf, else 0
   int has_bvh;
   int has_quadrics;      // launch the SceneViewQ instantiation
+  int has_textures;      // launch the SceneViewT instantiation
+  const MatTexD* mat_tex;    // per material
+  const TexD* texs;
+  const uchar4* texels;
   // camera (viewport.c:38-87), float
   float cam[3];
   float pixel00[3];
@@ -149,10 +179,21 @@ struct SceneView {
 struct SceneViewQ : SceneView {
   static constexpr bool kQuadrics = true;
 };
+// Scenes with textured materials (and any objects): texture lookups, maps
+// and the alpha test, with a per-hit copy of the material values.
+struct SceneViewT : SceneView {
+  static constexpr bool kQuadrics = true;
+  static constexpr bool kTextures = true;
+};
 
 // Calls f with the view as the type its kernels are instantiated for.
 template <class F>
 inline auto with_view(const SceneView& S, F&& f) {
+  if (S.has_textures) {
+    SceneViewT t;
+    static_cast<SceneView&>(t) = S;
+    return f(t);
+  }
   if (S.has_quadrics) {
     SceneViewQ q;
     static_cast<SceneView&>(q) = S;

@@ -21,13 +21,13 @@ __device__ __forceinline__ void env_nee(const V& S, PathState& P, const Surf& s,
   const float3 dir = f3(e.x, e.y, e.z);
   P.d = dir;
   C.shadow++;
-  if (any_hit(S, s.p, dir, INFINITY, status)) return;
+  if (any_hit(S, s.p, dir, INFINITY, status, P.rng.s)) return;
   float ct = dot(s.n, dir);
   float pdf = e.w;
   if (pdf <= 0.0f) return;
   const float4 r = __ldg(S.env_rec1 + k);
   float3 rad = f3(r.x, r.y, r.z);
-  if (s.mat >= 0) rad = rad * S.mats[s.mat].ao;
+  if (s.mat >= 0) rad = rad * surf_mat(S, s).ao;
   rad = rad * P.power;
   rad = rad * (ct / pdf);
   P.acc = P.acc + rad;
@@ -79,7 +79,7 @@ __device__ __forceinline__ void material_manager(const V& S, PathState& P, const
     default_mat(S, P, s, status, C);
     return;
   }
-  const MaterialD& M = S.mats[s.mat];
+  const MaterialD& M = surf_mat(S, s);
   if (M.emission_strength > 0.0f)
     P.acc = P.acc + (ld3(M.emission) * M.emission_strength) * P.power;
   if (M.metallic == 1.0f) metallic(M, P, s);
@@ -140,7 +140,7 @@ __device__ __forceinline__ float3 trace_path(const V& S, PathState& P, int max_d
   if (render_mode != 0) {
     HitInfo h;
     int visits = 0;
-    bool hit = closest_hit<true>(S, P.o, P.d, h, visits, status);
+    bool hit = closest_hit<true>(S, P.o, P.d, h, visits, status, P.rng.s);
     C.segments++;
     C.visits += visits;
     if (render_mode == 1) return f3(hit ? (float)visits : -1.0f, 0.f, 0.f);
@@ -152,11 +152,11 @@ __device__ __forceinline__ float3 trace_path(const V& S, PathState& P, int max_d
     HitInfo h;
     int visits = 0;
     C.segments++;
-    bool hit = closest_hit<true>(S, P.o, P.d, h, visits, status);
+    bool hit = closest_hit<true>(S, P.o, P.d, h, visits, status, P.rng.s);
     C.visits += visits;
     if (!hit) {
       float3 bg = background(S, P.d, true);
-      if (P.last_mat >= 0) bg = bg * S.mats[P.last_mat].ao;
+      if (P.last_mat >= 0) bg = bg * last_hit_ao(S, P);
       P.acc = P.acc + bg * P.power;
       if (ev && ev_k < kMaxEvents) {
         Surf z{};
@@ -168,7 +168,7 @@ __device__ __forceinline__ float3 trace_path(const V& S, PathState& P, int max_d
     }
     Surf s = make_surf(S, h, P.o, P.d, 0);
     P.o = s.p;
-    P.last_mat = s.mat;
+    set_last_hit(S, P, s);
     material_manager(S, P, s, status, C);
     if (ev && ev_k < kMaxEvents) write_event(ev, ev_k++, S, h, s, P);
     // Every later term is multiplied by the path power: a path whose power
@@ -187,16 +187,16 @@ __device__ __forceinline__ bool bounce(const V& S, PathState& P, int& depth_left
   HitInfo h;
   int visits = 0;
   C.segments++;
-  const bool hit = closest_hit<false>(S, P.o, P.d, h, visits, status);
+  const bool hit = closest_hit<false>(S, P.o, P.d, h, visits, status, P.rng.s);
   if (!hit) {
     float3 bg = background(S, P.d, true);
-    if (P.last_mat >= 0) bg = bg * S.mats[P.last_mat].ao;
+    if (P.last_mat >= 0) bg = bg * last_hit_ao(S, P);
     P.acc = P.acc + bg * P.power;
     return false;
   }
   Surf s = make_surf(S, h, P.o, P.d, 0);
   P.o = s.p;
-  P.last_mat = s.mat;
+  set_last_hit(S, P, s);
   material_manager(S, P, s, status, C);
   --depth_left;
   if (P.power.x == 0.0f && P.power.y == 0.0f && P.power.z == 0.0f) return false;

@@ -65,14 +65,15 @@ __global__ void photon_emit_kernel(V S, PhotonEmit E, int* status) {
     for (int depth = 0; depth < 10; ++depth) {
       HitInfo h;
       int visits = 0;
-      if (!closest_hit<false>(S, P.o, P.d, h, visits, status)) break;
-      Surf s = make_surf(S, h, P.o, P.d, 0);
+      if (!closest_hit<false>(S, P.o, P.d, h, visits, status, P.rng.s)) break;
+      // photon paths trace with is_light set (trace_photon_path.c:42)
+      Surf s = make_surf(S, h, P.o, P.d, 0, true);
       P.o = s.p;
       bool diffuse = false;
       if (s.mat < 0) {
         diffuse = true;
       } else {
-        const MaterialD& M = S.mats[s.mat];
+        const MaterialD& M = surf_mat(S, s);
         bool as_metal;
         if (M.metallic == 1.0f) as_metal = true;
         else if (M.metallic == 0.0f) as_metal = false;

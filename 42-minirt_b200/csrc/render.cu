@@ -172,7 +172,7 @@ __global__ void __launch_bounds__(kBlock) megakernel_batch(const SceneView* __re
 
 cudaError_t launch_megakernel_batch(const SceneView* views, const BatchItem* items, int n_items,
                                     uint64_t total, int* status, unsigned long long* work, int block,
-                                    bool quadrics, cudaStream_t st) {
+                                    int kind, cudaStream_t st) {
   if (total == 0 || n_items == 0) return cudaSuccess;
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
@@ -188,7 +188,11 @@ cudaError_t launch_megakernel_batch(const SceneView* views, const BatchItem* ite
     megakernel_batch<B, VT><<<grid, B, 0, st>>>(views, items, n_items, total, status, work); \
     return cudaGetLastError();                                                             \
   }
-  if (quadrics) {
+  if (kind == 2) {
+    MRT_BT(64, SceneViewT)
+    MRT_BT(128, SceneViewT)
+    MRT_BT(256, SceneViewT)
+  } else if (kind == 1) {
     MRT_BT(64, SceneViewQ)
     MRT_BT(128, SceneViewQ)
     MRT_BT(256, SceneViewQ)

@@ -14,6 +14,10 @@ struct Surf {
   float3 color;
   int mat;
   int front;
+  // SceneViewT only: this hit's material values with its texels applied
+  // (apply_all_map writes them into the shared t_mat, apply_map.c:60-85)
+  int has_hm;
+  MaterialD hm;
 };
 
 struct PathState {
@@ -21,7 +25,31 @@ struct PathState {
   float3 power, acc;
   Rng rng;
   int last_mat;     // material of the last hit (sky * ao on a miss, path_trace.c:37-48)
+  float last_ao;    // SceneViewT: that hit's ao value
 };
+
+// The material values of a hit: its own copy in a textured scene, else the
+// material table's entry.
+template <class V>
+__device__ __forceinline__ const MaterialD& surf_mat(const V& S, const Surf& s) {
+  if constexpr (V::kTextures) {
+    if (s.has_hm) return s.hm;
+  }
+  return S.mats[s.mat];
+}
+
+// ao of the last hit for the sky term of a miss (path_trace.c:37-48).
+template <class V>
+__device__ __forceinline__ float last_hit_ao(const V& S, const PathState& P) {
+  if constexpr (V::kTextures) return P.last_ao;
+  return S.mats[P.last_mat].ao;
+}
+
+template <class V>
+__device__ __forceinline__ void set_last_hit(const V& S, PathState& P, const Surf& s) {
+  P.last_mat = s.mat;
+  if constexpr (V::kTextures) P.last_ao = s.mat >= 0 ? surf_mat(S, s).ao : 1.0f;
+}
 
 // ----------------------------------------------------------------- sky
 
@@ -125,9 +153,10 @@ __device__ __forceinline__ void quadric_surf(const SceneView& S, const HitInfo& 
 // (hit_obj.c:68, hit_register.c:79-107, get_hit_color.c:17-36), untextured.
 template <class V>
 __device__ __forceinline__ Surf make_surf(const V& S, const HitInfo& h, float3 o, float3 d,
-                                          int render_mode) {
+                                          int render_mode, bool is_light = false) {
   Surf s;
   s.p = o + d * h.t;
+  s.has_hm = 0;
   uint32_t col;
   if (h.prim >= 0) {
     int4 m = __ldg(S.meta + h.prim);
@@ -156,6 +185,41 @@ __device__ __forceinline__ Surf make_surf(const V& S, const HitInfo& h, float3 o
     s.n = s.front ? n : -n;
     s.mat = pl.meta.y;
     col = (uint32_t)pl.meta.w;
+  }
+  if constexpr (V::kTextures) {
+    if (s.mat >= 0 && S.mat_tex[s.mat].any) {
+      // apply_all_map (apply_map.c:60-85) into this hit's copy
+      const MatTexD& mt = S.mat_tex[s.mat];
+      float u, v;
+      if (h.prim >= 0) prim_uv(S, h.prim, s.p, h.u, h.v, mt.uv_scale, u, v);
+      else plane_uv(S.planes[-1 - h.prim], s.p, mt.uv_scale, true, u, v);
+      s.hm = S.mats[s.mat];
+      s.has_hm = 1;
+      if (mt.tex[TS_NORMAL]) s.n = normal_map(S, mt, u, v, s.n);
+      if (mt.tex[TS_TRANSMISSION]) s.hm.transmission = tex_lookup(S, mt.tex[TS_TRANSMISSION], u, v, s.p).x;
+      if (!is_light) {
+        if (mt.tex[TS_ROUGHNESS]) {
+          const float r = tex_lookup(S, mt.tex[TS_ROUGHNESS], u, v, s.p).x;
+          s.hm.roughness = r;
+          s.hm.alpha4 = (r * r) * (r * r);
+        }
+        if (mt.tex[TS_METALLIC]) s.hm.metallic = tex_lookup(S, mt.tex[TS_METALLIC], u, v, s.p).x;
+        if (mt.tex[TS_AO]) s.hm.ao = tex_lookup(S, mt.tex[TS_AO], u, v, s.p).x;
+        if (mt.tex[TS_EMIS_STRENGTH])
+          s.hm.emission_strength = tex_lookup(S, mt.tex[TS_EMIS_STRENGTH], u, v, s.p).x;
+        if (mt.tex[TS_EMIS_COLOR]) {
+          const float4 e = tex_lookup(S, mt.tex[TS_EMIS_COLOR], u, v, s.p);
+          s.hm.emission[0] = e.x;
+          s.hm.emission[1] = e.y;
+          s.hm.emission[2] = e.z;
+        }
+      }
+      if (render_mode != 2 && mt.tex[TS_COLOR]) {
+        const float4 c = tex_lookup(S, mt.tex[TS_COLOR], u, v, s.p);
+        s.color = f3(c.x, c.y, c.z);
+        return s;
+      }
+    }
   }
   if (render_mode == 2)
     s.color = f3((s.n.x + 1) * 0.5f, (s.n.z + 1) * 0.5f, (s.n.y + 1) * 0.5f);
@@ -258,14 +322,14 @@ __device__ __forceinline__ float3 compute_light(const V& S, Rng& rng, const Surf
         float3 to = lp - s.p;
         float dist = sqrtf(len2(to));
         shadow_rays++;
-        vis = !any_hit(S, s.p, unit(to), dist, status);
+        vis = !any_hit(S, s.p, unit(to), dist, status, rng.s);
       } else {
         int hits = 0;
         for (int k = 0; k < L.shadow_sample; ++k) {
           float3 tgt = lp + rnd_in_unit_sphere(rng) * L.radius;
           float3 to = tgt - s.p;
           shadow_rays++;
-          if (!any_hit(S, s.p, unit(to), sqrtf(len2(to)), status)) hits++;
+          if (!any_hit(S, s.p, unit(to), sqrtf(len2(to)), status, rng.s)) hits++;
         }
         sf = (float)hits / (float)L.shadow_sample;
         vis = sf > 0.0f;
@@ -287,7 +351,7 @@ __device__ __forceinline__ float3 compute_light(const V& S, Rng& rng, const Surf
       }
     } else {
       shadow_rays++;
-      if (!any_hit(S, s.p, unit(-lp), INFINITY, status)) {
+      if (!any_hit(S, s.p, unit(-lp), INFINITY, status, rng.s)) {
         float3 ld = -lp;
         float ndl = dot(s.n, ld);
         if (ndl > 0.0f) {

@@ -11,6 +11,7 @@
 #pragma once
 #include "device_common.cuh"
 #include "quadric.cuh"
+#include "texture.cuh"
 
 namespace mrt {
 
@@ -87,12 +88,11 @@ __device__ __forceinline__ bool plane_hit(const PlaneD& p, float3 o, float3 d, f
 
 // One primitive of a leaf: triangle, sphere or (SceneViewQ) quadric. u, v
 // receive a triangle's barycentrics, or u the part of a quadric that was hit.
+// akey: the path stream's state, for the alpha test of textured scenes.
 template <class V>
-__device__ __forceinline__ bool prim_hit(const V& S, int i, float3 o, float3 d, float tbest, float& t,
-                                         float& u, float& v) {
-  const float4* g = S.geom + 3 * (size_t)i;
-  const float4 a = ldg4(g), b = ldg4(g + 1);
-  const int type = __float_as_int(a.w);
+__device__ __forceinline__ bool prim_hit_geom(const V& S, int i, int type, const float4& a, const float4& b,
+                                              const float4* g, float3 o, float3 d, float tbest, float& t,
+                                              float& u, float& v) {
   if (type == PRIM_TRI) {
     const float4 c = ldg4(g + 2);
     return tri_hit(a, b, c, o, d, S.one_sided, tbest, t, u, v);
@@ -108,6 +108,19 @@ __device__ __forceinline__ bool prim_hit(const V& S, int i, float3 o, float3 d, 
     }
   }
   return sphere_hit(a, b, o, d, tbest, t);
+}
+
+template <class V>
+__device__ __forceinline__ bool prim_hit(const V& S, int i, float3 o, float3 d, float tbest, float& t,
+                                         float& u, float& v, uint64_t akey = 0) {
+  const float4* g = S.geom + 3 * (size_t)i;
+  const float4 a = ldg4(g), b = ldg4(g + 1);
+  const int type = __float_as_int(a.w);
+  if (!prim_hit_geom(S, i, type, a, b, g, o, d, tbest, t, u, v)) return false;
+  if constexpr (V::kTextures) {
+    if (alpha_drops(S, i, type, o, d, t, u, v, akey)) return false;
+  }
+  return true;
 }
 
 // Closest hit. `visits` counts node fetches (heat-map / roofline counter).
@@ -131,7 +144,7 @@ __device__ __forceinline__ void fetch_node(const Node* nd, float4& lxy, float4& 
 template <bool kCount, bool kAnyHit, class V>
 __device__ __forceinline__ bool traverse(const V& S, float3 o, float3 d, float tmax_in,
                                          float& tbest, int& best, float& bu, float& bv, int& visits,
-                                         int* status) {
+                                         int* status, uint64_t akey = 0) {
   const float3 inv = f3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
   const float3 oi = o * inv;
   int stack[kStackSize];
@@ -178,7 +191,7 @@ __device__ __forceinline__ bool traverse(const V& S, float3 o, float3 d, float t
       const int first = code >> 3, count = (code & 7) + 1;
       for (int i = first; i < first + count; ++i) {
         float t, u = 0.f, v = 0.f;
-        const bool ok = prim_hit(S, i, o, d, tbest, t, u, v);
+        const bool ok = prim_hit(S, i, o, d, tbest, t, u, v, akey);
         if (ok) {
           if (kAnyHit) return true;
           tbest = t;
@@ -199,11 +212,11 @@ __device__ __forceinline__ bool traverse(const V& S, float3 o, float3 d, float t
 
 template <bool kCount, class V>
 __device__ __forceinline__ bool closest_hit_ww(const V& S, float3 o, float3 d, HitInfo& hit,
-                                               int& visits, int* status) {
+                                               int& visits, int* status, uint64_t akey = 0) {
   float tbest = kTMax;
   int best = kMiss;
   float bu = 0.f, bv = 0.f;
-  if (S.has_bvh) traverse<kCount, false>(S, o, d, kTMax, tbest, best, bu, bv, visits, status);
+  if (S.has_bvh) traverse<kCount, false>(S, o, d, kTMax, tbest, best, bu, bv, visits, status, akey);
   if (best == kMiss) tbest = kTMax;
   for (int i = 0; i < S.n_planes; ++i) {
     float t;
@@ -222,7 +235,7 @@ __device__ __forceinline__ bool closest_hit_ww(const V& S, float3 o, float3 d, H
 // Any hit with t < tmax (shadow rays), while-while form. Planes first: they are cheap.
 template <class V>
 __device__ __forceinline__ bool any_hit_ww(const V& S, float3 o, float3 d, float tmax,
-                                           int* status) {
+                                           int* status, uint64_t akey = 0) {
   for (int i = 0; i < S.n_planes; ++i) {
     float t;
     if (plane_hit(S.planes[i], o, d, t) && t < tmax) return true;
@@ -232,14 +245,14 @@ __device__ __forceinline__ bool any_hit_ww(const V& S, float3 o, float3 d, float
   int best = kMiss;
   float bu, bv;
   int visits = 0;
-  return traverse<false, true>(S, o, d, fminf(tmax, kTMax), tbest, best, bu, bv, visits, status);
+  return traverse<false, true>(S, o, d, fminf(tmax, kTMax), tbest, best, bu, bv, visits, status, akey);
 }
 
 // Compact single-loop traversal (one node or one leaf per iteration): the
 // megakernel's form, whose register budget is dominated by shading.
 template <bool kCount, class V>
 __device__ __forceinline__ bool closest_hit_compact(const V& S, float3 o, float3 d, HitInfo& hit,
-                                            int& visits, int* status) {
+                                            int& visits, int* status, uint64_t akey = 0) {
   float tbest = kTMax;
   int best = kMiss;
   float bu = 0.f, bv = 0.f;
@@ -278,7 +291,7 @@ __device__ __forceinline__ bool closest_hit_compact(const V& S, float3 o, float3
         int first = code >> 3, count = (code & 7) + 1;
         for (int i = first; i < first + count; ++i) {
           float t, u = 0.f, v = 0.f;
-          if (prim_hit(S, i, o, d, tbest, t, u, v)) { tbest = t; best = i; bu = u; bv = v; }
+          if (prim_hit(S, i, o, d, tbest, t, u, v, akey)) { tbest = t; best = i; bu = u; bv = v; }
         }
       }
       if (sp == 0) break;
@@ -302,7 +315,7 @@ __device__ __forceinline__ bool closest_hit_compact(const V& S, float3 o, float3
 // Any hit, compact loop.
 template <class V>
 __device__ __forceinline__ bool any_hit_compact(const V& S, float3 o, float3 d, float tmax,
-                                        int* status) {
+                                        int* status, uint64_t akey = 0) {
   for (int i = 0; i < S.n_planes; ++i) {
     float t;
     if (plane_hit(S.planes[i], o, d, t) && t < tmax) return true;
@@ -340,7 +353,7 @@ __device__ __forceinline__ bool any_hit_compact(const V& S, float3 o, float3 d, 
       int first = code >> 3, count = (code & 7) + 1;
       for (int i = first; i < first + count; ++i) {
         float t, u, v;
-        if (prim_hit(S, i, o, d, tlim, t, u, v)) return true;
+        if (prim_hit(S, i, o, d, tlim, t, u, v, akey)) return true;
       }
     }
     if (sp == 0) return false;
@@ -352,13 +365,14 @@ __device__ __forceinline__ bool any_hit_compact(const V& S, float3 o, float3 d, 
 // traversal kernels call the while-while form directly.
 template <bool kCount, class V>
 __device__ __forceinline__ bool closest_hit(const V& S, float3 o, float3 d, HitInfo& hit,
-                                            int& visits, int* status) {
-  return closest_hit_compact<kCount>(S, o, d, hit, visits, status);
+                                            int& visits, int* status, uint64_t akey = 0) {
+  return closest_hit_compact<kCount>(S, o, d, hit, visits, status, akey);
 }
 
 template <class V>
-__device__ __forceinline__ bool any_hit(const V& S, float3 o, float3 d, float tmax, int* status) {
-  return any_hit_compact(S, o, d, tmax, status);
+__device__ __forceinline__ bool any_hit(const V& S, float3 o, float3 d, float tmax, int* status,
+                                        uint64_t akey = 0) {
+  return any_hit_compact(S, o, d, tmax, status, akey);
 }
 
 }  // namespace mrt

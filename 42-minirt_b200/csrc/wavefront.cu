@@ -23,6 +23,7 @@
 //   retire   : accumulates finished paths into the frame
 // A whole wave (generate + depth x stages) is captured once in a CUDA graph
 // and replayed; kernels read their queue lengths from device counters.
+#include <type_traits>
 #include <vector>
 
 #include "../../include/mrt.h"
@@ -586,8 +587,9 @@ static void wf_enqueue_wave_t(WfHost* H, const VT& v, const WfParams& P, int* st
 
 static void wf_enqueue_wave(WfHost* H, const SceneView& v, const WfParams& P, int* status,
                             cudaStream_t st, unsigned* launches) {
+  // textured scenes never reach the wavefront (mrt_render refuses them)
   with_view(v, [&](const auto& vt) {
-    wf_enqueue_wave_t(H, vt, P, status, st, launches);
+    if constexpr (!std::decay_t<decltype(vt)>::kTextures) wf_enqueue_wave_t(H, vt, P, status, st, launches);
     return 0;
   });
 }

@@ -57,6 +57,7 @@ typedef struct s_flat
 	mrt_cylinder	*cy;
 	mrt_cone		*co;
 	mrt_hyperboloid	*hy;
+	mrt_texture		*tx;
 	double			**buf;
 	int				nbuf;
 }	t_flat;
@@ -66,6 +67,14 @@ static int	mat_index(t_scene *s, t_mat *m)
 	if (!m || m < s->materials || m >= s->materials + s->mat_amount)
 		return (-1);
 	return ((int)(m - s->materials));
+}
+
+/* 1 + the index of t in the scene's t_tex array, 0 for none */
+static int	tex_index(t_scene *s, t_tex *t)
+{
+	if (!t || t < s->textures || t >= s->textures + s->tex_amount)
+		return (0);
+	return ((int)(t - s->textures) + 1);
 }
 
 static void	c3(uint8_t *o, t_color c)
@@ -95,6 +104,7 @@ static void	free_flat(t_flat *f)
 	free(f->cy);
 	free(f->co);
 	free(f->hy);
+	free(f->tx);
 }
 
 /* t_custom_object triangles (after ft_update_obj_position) -> a
@@ -158,13 +168,30 @@ static int	flatten(t_minirt *mrt, t_scene *s, t_flat *f)
 	f->pl = calloc(np + 1, sizeof(mrt_plane));
 	f->li = calloc(nl + 1, sizeof(mrt_light));
 	f->me = calloc(nm + 1, sizeof(mrt_mesh));
+	f->tx = calloc(s->tex_amount + 1, sizeof(mrt_texture));
 	f->cy = calloc(nc + 1, sizeof(mrt_cylinder));
 	f->co = calloc(nk + 1, sizeof(mrt_cone));
 	f->hy = calloc(nh + 1, sizeof(mrt_hyperboloid));
 	f->buf = calloc(3 * nm + 1, sizeof(double *));
 	if (!f->mats || !f->sph || !f->pl || !f->li || !f->me || !f->buf
-		|| !f->cy || !f->co || !f->hy)
+		|| !f->cy || !f->co || !f->hy || !f->tx)
 		return (-1);
+	for (int i = 0; i < s->tex_amount; i++)
+	{
+		t_tex		*t = &s->textures[i];
+		mrt_texture	*o = &f->tx[i];
+
+		o->type = (int32_t)t->type;
+		if (t->img.rgba && t->img.width && t->img.height)
+		{
+			o->rgba = (const uint8_t *)t->img.rgba;
+			o->width = t->img.width;
+			o->height = t->img.height;
+		}
+		o->checker_scale = t->checker.scale;
+		c3(o->c1, t->checker.c1);
+		c3(o->c2, t->checker.c2);
+	}
 	for (int i = 0; i < s->mat_amount; i++)
 	{
 		t_mat			*m = &s->materials[i];
@@ -179,6 +206,15 @@ static int	flatten(t_minirt *mrt, t_scene *s, t_flat *f)
 		o->ao = m->ao_value;
 		o->emission_strength = m->emission_strength;
 		o->scale = m->scale;
+		o->color_tex = tex_index(s, m->color_tex);
+		o->metallic_tex = tex_index(s, m->metallic_tex);
+		o->roughness_tex = tex_index(s, m->roughness_tex);
+		o->transmission_tex = tex_index(s, m->transmission_tex);
+		o->ao_tex = tex_index(s, m->ao_tex);
+		o->emission_strength_tex = tex_index(s, m->emission_strength_tex);
+		o->emission_color_tex = tex_index(s, m->emission_color_tex);
+		o->normal_tex = tex_index(s, m->normal);
+		o->normal_intensity = m->normal_intensity;
 	}
 	ns = np = nl = nm = nc = nk = nh = 0;
 	for (int i = 0; i < s->el_amount; i++)
@@ -317,6 +353,8 @@ static int	flatten(t_minirt *mrt, t_scene *s, t_flat *f)
 	f->d.n_cones = nk;
 	f->d.hyperboloids = f->hy;
 	f->d.n_hyperboloids = nh;
+	f->d.textures = f->tx;
+	f->d.n_textures = s->tex_amount;
 	return (0);
 }
 

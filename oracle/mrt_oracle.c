@@ -2153,12 +2153,24 @@ static v3 defocus_origin(rng_t *rg, ro_scene *s)
 }
 
 /* calc_one_sample_task (calc_sample.c:44-71), render_mode 0 and 2. */
+static fc sample_pixel_(rng_t *rg, ro_scene *s, uint32_t i, double ox, double oy);
+
+/* One camera path; its stream keys the alpha test of its traversals. */
 static fc sample_pixel(rng_t *rg, ro_scene *s, uint32_t i, double ox, double oy)
+{
+	fc	c;
+
+	s->rg = rg;
+	c = sample_pixel_(rg, s, i, ox, oy);
+	s->rg = NULL;
+	return c;
+}
+
+static fc sample_pixel_(rng_t *rg, ro_scene *s, uint32_t i, double ox, double oy)
 {
 	ray_t	r;
 	hrec_t	h;
 
-	s->rg = rg;
 	if (s->defocus_angle <= 0)
 		r.orig = s->cam_pos;
 	else
@@ -2186,6 +2198,7 @@ static int trace_photon(rng_t *rg, ro_scene *s, v3 lp, fc p0, photon_t *out)
 	s->is_light = 1;
 	stored = trace_photon_(rg, s, lp, p0, out);
 	s->is_light = 0;
+	s->rg = NULL;
 	return stored;
 }
 

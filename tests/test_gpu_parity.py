@@ -61,7 +61,7 @@ def random_rays(rng, vp, n, spread=0.3):
     return o, d
 
 
-@pytest.mark.parametrize("name", ["c0", "c1", "c2", "q0"])
+@pytest.mark.parametrize("name", ["c0", "c1", "c2", "q0", "t0"])
 def test_first_hit_matches_reference_golden(mrt, oracle, mg, name):
     g = golden(f"{name}_pins.npz")
     sc = mg.CASES[name]["make"]()
@@ -73,11 +73,17 @@ def test_first_hit_matches_reference_golden(mrt, oracle, mg, name):
     assert exact.mean() >= 0.998
     assert other.sum() <= max(2, int(0.001 * len(h)))
     hit = (h["prim"] >= 0) & exact
-    np.testing.assert_allclose(h["normal"][hit], g["hit_normal"][hit], atol=2e-4)
     np.testing.assert_array_equal(h["front_face"][hit], g["hit_front_face"][hit])
+    close = np.abs(h["normal"][hit] - g["hit_normal"][hit]).max(axis=1) <= 2e-4
+    if name == "t0":
+        # normal-mapped hits: a float uv can fall in the neighbouring texel
+        # of the map where the double one does not
+        assert close.mean() >= 0.995, close.mean()
+    else:
+        assert close.all(), np.nonzero(~close)[0][:5]
 
 
-@pytest.mark.parametrize("name", ["c0", "c1", "c2", "q0"])
+@pytest.mark.parametrize("name", ["c0", "c1", "c2", "q0", "t0"])
 def test_first_hit_matches_oracle_on_fresh_rays(mrt, oracle, mg, name):
     sc = mg.CASES[name]["make"]()
     ro = oracle.Restatement(sc)
@@ -154,7 +160,7 @@ def _diffuse(sc):
 
 
 STREAM_CASES = {"c0": 0.99, "c1": 0.85, "c2": 0.99, "c1_noglass": 0.85, "c1_diffuse": 0.99, "q0": 0.95,
-                "q0_diffuse": 0.99}
+                "q0_diffuse": 0.99, "t0": 0.95, "t0_partial": 0.95}
 
 
 @pytest.mark.parametrize("name", sorted(STREAM_CASES))
@@ -167,6 +173,10 @@ def test_paths_match_oracle_stream(mrt, oracle, mg, name):
     statistically."""
     base = name.split("_")[0]
     sc = mg.CASES[base]["make"]()
+    if name == "t0_partial":
+        # texels of alpha 128: the alpha test draws the same hashed uniform
+        # on both sides
+        sc = mg.scenes.make_textured(6, 32, 24, depth=6, partial_alpha=True)
     if name.endswith("noglass"):
         sc = _no_glass(sc)
     if name.endswith("diffuse"):
@@ -395,3 +405,47 @@ def test_quadric_scene_rejects_malformed_objects(mrt, scenes):
     sc.hyperboloids[1]["c"] = 0.0
     with pytest.raises(Exception, match="hyperboloid 1"):
         ctx.build(sc)
+
+
+def test_textured_scene_forms(mrt, oracle, scenes):
+    """Textured scenes render with the megakernel forms; an explicit
+    wavefront request is refused with a message, the autotuner and
+    FORM_AUTO pick a megakernel, and the plain and regenerating megakernels
+    agree per pixel on the same streams."""
+    sc = scenes.make_textured(6, 48, 36, depth=6)
+    ctx = mrt.Context(48, 36)
+    ctx.build(oracle.canonical_scene(sc))
+    with pytest.raises(mrt.MRTError, match="megakernel"):
+        ctx.render(2, seed=3, form=mrt.FORM_WAVEFRONT)
+    ctx.clear()
+    ctx.render(8, seed=3, form=mrt.FORM_MEGAKERNEL)
+    a, _ = ctx.read_accum()
+    ctx.clear()
+    ctx.render(8, seed=3, form=mrt.FORM_MEGAKERNEL_PLAIN)
+    b, _ = ctx.read_accum()
+    err = np.abs(a - b).max(axis=2) / np.maximum(np.abs(a).max(axis=2), 1e-2)
+    assert (err <= 1e-4).mean() >= 0.99
+    ctx.tune(2, seed=3)
+    ctx.clear()
+    ctx.render(2, seed=3, form=mrt.FORM_AUTO)
+
+
+def test_partial_alpha_matches_reference_in_the_mean(mrt, oracle, scenes):
+    """Texels of alpha 128 hide an object with probability 1/2. The kernels
+    draw that from a hash of the path stream; the reference from its global
+    random stream: the images agree statistically."""
+    sc = scenes.make_textured(6, 40, 30, depth=6, partial_alpha=True)
+    ctx = mrt.Context(40, 30)
+    ctx.build(oracle.canonical_scene(sc))
+    n = 512
+    ctx.render(n, seed=17, form=mrt.FORM_MEGAKERNEL)
+    gpu, _ = ctx.read_accum()
+    gpu = gpu / n
+    ref = oracle.RefOracle(sc)
+    ref.set_seed(4321)
+    ref.render(n)
+    cpu = ref.accum() / n
+    d = (gpu - cpu).mean(axis=2).reshape(-1)
+    se = d.std() / np.sqrt(d.size)
+    print("partial alpha: mean gpu", gpu.mean(), "reference", cpu.mean(), "z", d.mean() / se)
+    assert abs(d.mean()) <= 4 * se

@@ -125,3 +125,29 @@ def test_compute_frame_gpu_with_quadrics_matches_reference_render(adapter, oracl
     assert abs(d.mean()) <= 4 * se
     adapter.clean_shaders(sd)
     adapter.clean_scene(g)
+
+
+def test_compute_frame_gpu_with_textures_matches_reference_render(adapter, oracle, scenes):
+    """t_tex images, checkers and maps of t_scene reach the drop-in."""
+    sc = scenes.make_textured(6, 48, 36, depth=6)
+    ref = oracle.RefOracle(sc)
+    L = ref.lib
+    m, scn, vp = L.refh_minirt(ref.h), L.refh_scene_ptr(ref.h), L.refh_viewport_ptr(ref.h)
+    sd, g = L.refh_shader_data(ref.h), L.refh_gpu_structs(ref.h)
+    assert adapter.init_shader(sd, sc.width, sc.height, scn) == 0
+    assert adapter.convert_scene_build(m, scn, vp, g) == 0
+    adapter.convert_scene(m, scn, vp, g)
+    n = 256
+    for _ in range(n):
+        adapter.compute_frame_gpu(m)
+    gpu = ref.accum() / n
+    ref2 = oracle.RefOracle(sc)
+    ref2.set_seed(77)
+    ref2.render(n)
+    cpu = ref2.accum() / n
+    d = (gpu - cpu).mean(axis=2).reshape(-1)
+    se = d.std() / np.sqrt(d.size)
+    print("textures image mean gpu", gpu.mean(), "cpu", cpu.mean(), "z", d.mean() / se)
+    assert abs(d.mean()) <= 4 * se
+    adapter.clean_shaders(sd)
+    adapter.clean_scene(g)
