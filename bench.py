@@ -324,6 +324,8 @@ WORKLOADS = {
           "16 materials, 2048x1024 RGBE sky with importance sampling",
     "q0": "q0: 320x240, 64 spp, depth 8, two cylinders, two cones, two hyperboloids, two spheres, "
           "ground plane, point light",
+    "t0": "t0: 320x240, 64 spp, depth 8, image / checker / fallback textures, normal, roughness, metallic, "
+          "ao and emission maps, alpha cut-outs",
 }
 
 
@@ -331,7 +333,7 @@ def workload_config(a, sc) -> dict:
     return {"workload": WORKLOADS.get(a.config, a.config),
             "spp_per_step": a.spp_per_step,
             "l2": ("scene arrays (BVH, triangles, shading, sky tables) exceed the 126 MB L2"
-                   if a.config != "q0" else "the scene (a few KB) stays in L2, as in any render of it; "
+                   if a.config not in ("q0", "t0") else "the scene (a few KB) stays in L2, as in any render of it; "
                    "each step traces new paths"),
             "parallelism": f"sample-parallel dp{a.gpus}"}
 

@@ -10,7 +10,8 @@ and prices every access with the per-unit sizes below:
   48 B per cylinder / cone / hyperboloid test, 32 B per plane test, 80 B per traced ray (32 read + 32 write + 16 hit
   record), 160 B per shading event (64 vertex normals/uv + 96 material
   record), 28 B per HDRI importance sample (8 inverse tables + 4 pdf + 16
-  texel), plus 12 B / spp for the frame buffer.
+  texel), plus 12 B / spp for the frame buffer. Texel fetches of textured
+  scenes are not priced (so t0's figure is a lower bound).
 The result is frozen in oracle/algorithmic_bytes.json so kernel or BVH
 changes cannot move it.  Run:  python oracle/make_algorithmic_bytes.py [config ...]
 (named configs only: the other entries of the file are kept as they are).
@@ -50,7 +51,8 @@ def main(only=None):
     out["units"] = UNIT
     cases = [("c0", scenes.make_c0, 64, 20000), ("c1", scenes.make_c1, 256, 4000),
              ("c2", lambda: scenes.make_c2(photons=20000), 128, 4000),
-             ("c4", scenes.make_c4, 64, 4000), ("q0", scenes.make_quadrics, 64, 20000)]
+             ("c4", scenes.make_c4, 64, 4000), ("q0", scenes.make_quadrics, 64, 20000),
+             ("t0", scenes.make_textured, 64, 20000)]
     for name, make, spp, n in cases:
         if only and name not in only:
             continue
