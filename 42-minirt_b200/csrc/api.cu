@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cerrno>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -1227,6 +1228,72 @@ extern "C" int mrt_accumulate_double(mrt_ctx* c, double* float_render) {
   if (rc) return rc;
   for (size_t i = 0; i < 3 * n; ++i) float_render[i] += rgb[i];
   return mrt_clear(c);
+}
+
+namespace {
+void put_i32(unsigned char* p, int32_t v) {
+  for (int k = 0; k < 4; ++k) p[k] = (unsigned char)(((uint32_t)v >> (8 * k)) & 0xff);
+}
+int32_t get_i32(const unsigned char* p) {
+  uint32_t v = 0;
+  for (int k = 0; k < 4; ++k) v |= (uint32_t)p[k] << (8 * k);
+  return (int32_t)v;
+}
+}  // namespace
+
+extern "C" int mrt_render_state_save(mrt_ctx* c, const char* path) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!path) return set_err(MRT_ERR_INVALID, "null path");
+  const size_t n = (size_t)c->W * c->H;
+  std::vector<float> rgb(n * 3);
+  rc = mrt_read_accum(c, rgb.data(), nullptr);
+  if (rc) return rc;
+  std::vector<unsigned char> buf(12 + n * 3 * sizeof(double));
+  put_i32(buf.data(), c->W);
+  put_i32(buf.data() + 4, c->H);
+  put_i32(buf.data() + 8, c->accum_spp);
+  for (size_t i = 0; i < 3 * n; ++i) {
+    const double v = rgb[i];
+    std::memcpy(buf.data() + 12 + 8 * i, &v, 8);   // IEEE double, little-endian hosts
+  }
+  FILE* f = std::fopen(path, "wb");
+  if (!f) return set_err(MRT_ERR_INVALID, "creating %s: %s", path, std::strerror(errno));
+  const size_t w = std::fwrite(buf.data(), 1, buf.size(), f);
+  const int closed = std::fclose(f);
+  if (w != buf.size() || closed != 0) return set_err(MRT_ERR_INVALID, "writing %s failed", path);
+  return MRT_OK;
+}
+
+extern "C" int mrt_render_state_load(mrt_ctx* c, const char* path) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!path) return set_err(MRT_ERR_INVALID, "null path");
+  FILE* f = std::fopen(path, "rb");
+  if (!f) return set_err(MRT_ERR_INVALID, "opening %s: %s", path, std::strerror(errno));
+  std::vector<unsigned char> buf;
+  unsigned char chunk[1 << 16];
+  size_t got;
+  while ((got = std::fread(chunk, 1, sizeof(chunk), f)) > 0) buf.insert(buf.end(), chunk, chunk + got);
+  std::fclose(f);
+  if (buf.size() < 12) return set_err(MRT_ERR_INVALID, "%s: %zu bytes, no header", path, buf.size());
+  const int32_t w = get_i32(buf.data()), h = get_i32(buf.data() + 4), sample = get_i32(buf.data() + 8);
+  if (w != c->W || h != c->H)
+    return set_err(MRT_ERR_INVALID, "%s holds a %dx%d render, the context is %dx%d", path, w, h, c->W, c->H);
+  const size_t n = (size_t)c->W * c->H;
+  if (buf.size() - 12 != n * 3 * sizeof(double) || sample < 0)
+    return set_err(MRT_ERR_INVALID, "%s: %zu data bytes for %zu pixels, sample %d", path, buf.size() - 12, n,
+                   sample);
+  std::vector<float4> acc(n);
+  for (size_t i = 0; i < n; ++i) {
+    double v[3];
+    std::memcpy(v, buf.data() + 12 + 24 * i, 24);
+    acc[i] = make_float4((float)v[0], (float)v[1], (float)v[2], (float)sample);
+  }
+  CK(cudaMemcpyAsync(c->accum.p, acc.data(), n * sizeof(float4), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->accum_spp = sample;
+  return MRT_OK;
 }
 
 extern "C" int mrt_read_depth(mrt_ctx* c, int32_t* depth) {

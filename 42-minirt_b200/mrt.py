@@ -195,6 +195,8 @@ SIGNATURES = {
     "mrt_read_accum": (C.c_int, [_P, _P, C.POINTER(C.c_int32)]),
     "mrt_accumulate_double": (C.c_int, [_P, _P]),
     "mrt_read_depth": (C.c_int, [_P, _P]),
+    "mrt_render_state_save": (C.c_int, [_P, C.c_char_p]),
+    "mrt_render_state_load": (C.c_int, [_P, C.c_char_p]),
     "mrt_trace_first_hit": (C.c_int, [_P, _P, C.c_int64, _P]),
     "mrt_trace_paths": (C.c_int, [_P, C.POINTER(RenderParams), _P, _P, C.c_int32, _P, _P]),
     "mrt_read_env_tables": (C.c_int, [_P, _P, _P, _P]),
@@ -345,6 +347,12 @@ class Context:
         assert buf.dtype == np.float64 and buf.size == self.width * self.height * 3
         check(self.lib.mrt_accumulate_double(self.h, _ptr(buf)), "mrt_accumulate_double")
 
+    def save_state(self, path) -> None:
+        check(self.lib.mrt_render_state_save(self.h, str(path).encode()), "mrt_render_state_save")
+
+    def load_state(self, path) -> None:
+        check(self.lib.mrt_render_state_load(self.h, str(path).encode()), "mrt_render_state_load")
+
     def read_depth(self) -> np.ndarray:
         out = np.zeros((self.height, self.width), np.int32)
         check(self.lib.mrt_read_depth(self.h, _ptr(out)), "mrt_read_depth")
@@ -459,3 +467,28 @@ class Context:
                                     C.byref(st)), "mrt_backward")
         return (out, st) if stats else out
 
+
+
+# ------------------------------------------------ render_state.rts (host side)
+
+def write_rts(path, float_render: np.ndarray, sample: int) -> None:
+    """render_state.rts as export_render_state writes it
+    (export_render_state.c:15-33): int32 width, height, sample, then the
+    (H, W, 3) double per-pixel sums, little-endian."""
+    fr = np.ascontiguousarray(float_render, "<f8")
+    h, w = fr.shape[:2]
+    with open(path, "wb") as f:
+        f.write(np.array([w, h, sample], "<i4").tobytes())
+        f.write(fr.tobytes())
+
+
+def read_rts(path) -> tuple[np.ndarray, int]:
+    """(float_render (H, W, 3) float64, sample) of a render_state.rts, with
+    init_float_render's size check (export_render_state.c:35-51)."""
+    raw = open(path, "rb").read()
+    if len(raw) < 12:
+        raise ValueError(f"{path}: no header")
+    w, h, sample = (int(x) for x in np.frombuffer(raw[:12], "<i4"))
+    if len(raw) - 12 != w * h * 3 * 8:
+        raise ValueError(f"{path}: {len(raw) - 12} data bytes for a {w}x{h} render")
+    return np.frombuffer(raw[12:], "<f8").reshape(h, w, 3).copy(), sample

@@ -388,6 +388,18 @@ MRT_API int			mrt_accumulate_double(mrt_ctx *ctx, double *float_render);
 /* BVH heat map (render_mode 1): per-pixel node-visit count of the last call. */
 MRT_API int			mrt_read_depth(mrt_ctx *ctx, int32_t *depth);
 
+/* Checkpoint of a progressive render in the reference's render_state.rts
+ * format (export_render_state.c:15-33): int32 width, int32 height, int32
+ * sample count, then width*height t_fcolor (3 doubles: the per-pixel sums),
+ * little-endian. save writes the device accumulator and its sample count;
+ * load replaces them (init_float_render, :35-51, accepts the file only when
+ * its size and dimensions match; so does load, returning MRT_ERR_INVALID
+ * otherwise), so that rendering continues from sample_base = that count.
+ * The miniRT drop-in accumulates into the host float_render, which the
+ * reference's own export_render_state / init_float_render handle. */
+MRT_API int			mrt_render_state_save(mrt_ctx *ctx, const char *path);
+MRT_API int			mrt_render_state_load(mrt_ctx *ctx, const char *path);
+
 /* ------------------------------------------------------------ autotuner */
 
 # define MRT_TUNE_MAX 32
