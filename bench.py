@@ -465,10 +465,15 @@ def main() -> int:
 
     f = forms[best]
     achieved = bpp * (paths_per_step / max(f["launches"] / a.steps, 1)) / (f["launch_ms"] / 1000.0) / 1e9
+    # DRAM bytes per path of the form, from the ncu launch list summarised
+    # in profiles/ (dram__bytes_read.sum + dram__bytes_write.sum over its
+    # kernels), scaled to the paths of one launch like `achieved`
     traffic = None
     tf = REPO / "profiles" / "traffic.json"
     if tf.exists():
-        traffic = json.loads(tf.read_text()).get(best)
+        t = json.loads(tf.read_text()).get(a.config, {}).get(best)
+        if t:
+            traffic = t["bytes_per_path"] * (paths_per_step / max(f["launches"] / a.steps, 1))
     line = {
         "metric": METRIC, "value": forms[best]["value"], "unit": UNIT, "n_gpus": world,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": f["ms_per_step"],
