@@ -56,4 +56,33 @@ int		ft_dprintf(int fd, const char *fmt, ...);
 char	*ft_sprintf(const char *fmt, ...);
 ssize_t	get_cpu_time(void);
 
+/* string / number / file helpers of the scene parser (src/parsing, src/utils
+ * loaders); restated in oracle/shim/libft_parse_shim.c */
+int		ft_strcmp(const char *a, const char *b);
+int		ft_strncmp(const char *a, const char *b, size_t n);
+size_t	ft_strlen(const char *s);
+ssize_t	ft_sstrlen(const char *s);
+char	*ft_strchr(const char *s, int c);
+char	*ft_strrchr(const char *s, int c);
+char	*ft_strnstr(const char *h, const char *n, size_t len);
+char	*ft_strdup(const char *s);
+int		ft_isdigit(int c);
+int		ft_isalpha(int c);
+int		ft_isalnum(int c);
+int		ft_atoi(const char *s);
+int		ft_abs(int x);
+double	ft_atod(const char *s);
+float	ft_atof(const char *s);
+int		is_valid_float(const char *s);
+char	**ft_split_in_line(char *s, const char *set);
+void	ft_free_tab_null_term(char **tab);
+char	*get_next_line(int fd);
+int		read_bin_file(t_bin *bin, const char *path);
+int		read_uint8_move(t_bin *bin, size_t *i, uint8_t *out);
+int		read_uint16_move(t_bin *bin, size_t *i, uint16_t *out);
+int		read_uint16_move_little(t_bin *bin, size_t *i, uint16_t *out);
+int		read_uint32_move(t_bin *bin, size_t *i, uint32_t *out);
+int		read_uint32_move_little(t_bin *bin, size_t *i, uint32_t *out);
+int		read_uint64_move_little(t_bin *bin, size_t *i, uint64_t *out);
+
 #endif

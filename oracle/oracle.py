@@ -49,6 +49,7 @@ def ref_lib():
         lib = C.CDLL(str(REF_LIB), mode=C.RTLD_GLOBAL)
         sig = {
             "refh_create": (_P, [_P]), "refh_destroy": (None, [_P]),
+            "refh_create_from_rt": (_P, [C.c_char_p, C.c_int, C.c_int, C.c_int]),
             "refh_set_seed": (None, [C.c_uint64]), "refh_get_seed": (C.c_uint64, []),
             "refh_set_quiet": (None, [C.c_int]), "refh_random_double": (C.c_double, []),
             "refh_first_hit": (C.c_int, [_P, _P, C.c_int64, _P]),
@@ -92,6 +93,18 @@ class RefOracle:
         if not self.h:
             raise ValueError("refh_create rejected the scene")
         self.W, self.H = scene.width, scene.height
+
+    @classmethod
+    def from_rt(cls, path, width: int, height: int, max_bounces: int):
+        """A .rt scene file through the reference's own parser."""
+        self = cls.__new__(cls)
+        self.lib = ref_lib()
+        self.scene, self.desc = None, None
+        self.h = self.lib.refh_create_from_rt(str(path).encode(), width, height, max_bounces)
+        if not self.h:
+            raise ValueError(f"the reference's parser rejected {path}")
+        self.W, self.H = width, height
+        return self
 
     def close(self):
         if self.h:

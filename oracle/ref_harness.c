@@ -451,6 +451,69 @@ void	*refh_create(const mrt_scene_desc *d)
 	return (h);
 }
 
+/* A .rt file through the reference's own parser (parse_scene,
+ * parse_scene.c:99) and the object set-up of set_dependant_values
+ * (set_dependant_values.c:47-73, without its UI parts), then the same
+ * render set-up as refh_create. The render size and depth are the caller's
+ * (the reference takes them from its UI controls). */
+void	*refh_create_from_rt(const char *path, int width, int height, int max_bounces)
+{
+	t_refh		*h;
+	t_minirt	*m;
+	t_scene		*sc;
+
+	if (!path || width <= 0 || height <= 0)
+		return (NULL);
+	h = calloc(1, sizeof(t_refh));
+	m = calloc(1, sizeof(t_minirt));
+	h->m = m;
+	if (parse_scene(m, (char *)path) == 0)
+		return (NULL);
+	sc = &m->scene;
+	sc->camera.orientation = vec3_unit(sc->camera.orientation);
+	for (int i = 0; i < sc->el_amount; i++)
+	{
+		void	*o = sc->elements[i].object;
+
+		if (sc->elements[i].type == SPHERE)
+			set_values_sphere(o);
+		else if (sc->elements[i].type == CYLINDER)
+			set_values_cylinder(o);
+		else if (sc->elements[i].type == PLANE)
+			set_values_plane(o);
+		else if (sc->elements[i].type == LIGHT)
+			set_values_light(o);
+		else if (sc->elements[i].type == CONE)
+			set_values_cone(o);
+		else if (sc->elements[i].type == HYPERBOLOID)
+			set_values_hyperboloid(o);
+		else if (sc->elements[i].type == CUSTOM)
+			set_values_custom(o);
+		else if (sc->elements[i].type == DIRECTIONAL_LIGHT)
+			set_values_directional_light(o);
+	}
+	for (int i = 0; i < sc->mat_amount; i++)
+		set_values_mat(&sc->materials[i]);
+	if ((!sc->amb_light.skybox_t || sc->amb_light.skybox_t->type != HDR)
+		&& sc->amb_light.ratio < 0)
+		sc->amb_light.ratio = 0;
+	if (sc->camera.focus_dist == 0)
+		sc->camera.focus_dist = 1;
+	m->controls.values.fov = sc->camera.fov;
+	sc->render_width = width;
+	sc->render_height = height;
+	sc->win_width = width;
+	sc->win_height = height;
+	sc->build_bvh = 1;
+	m->options.no_display = 1;
+	m->controls.max_bounces = max_bounces;
+	h->max_bounces = max_bounces;
+	m->render_mode = 0;
+	m->screen.float_render = calloc((size_t)width * height, sizeof(t_fcolor));
+	m->viewport = init_viewport(m);
+	return (h);
+}
+
 void	refh_destroy(void *hv)
 {
 	t_refh	*h;
