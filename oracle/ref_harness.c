@@ -456,6 +456,9 @@ void	*refh_create(const mrt_scene_desc *d)
  * (set_dependant_values.c:47-73, without its UI parts), then the same
  * render set-up as refh_create. The render size and depth are the caller's
  * (the reference takes them from its UI controls). */
+extern int	oracle_ref_parse_mat_index;
+extern int	oracle_ref_parse_tex_index;
+
 void	*refh_create_from_rt(const char *path, int width, int height, int max_bounces)
 {
 	t_refh		*h;
@@ -464,6 +467,8 @@ void	*refh_create_from_rt(const char *path, int width, int height, int max_bounc
 
 	if (!path || width <= 0 || height <= 0)
 		return (NULL);
+	oracle_ref_parse_mat_index = 0;
+	oracle_ref_parse_tex_index = 0;
 	h = calloc(1, sizeof(t_refh));
 	m = calloc(1, sizeof(t_minirt));
 	h->m = m;
