@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(kWfBlock) wf_extend(V S, WfState W, int* statu
       const float4 o = W.o[i], d = W.d[i];
       HitInfo h;
       int visits = 0;
-      bool hit = closest_hit_ww<false>(S, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), h, visits, status);
+      bool hit = closest_hit_compact<false>(S, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), h, visits, status);
       W.hit[i] = make_float4(h.t, h.u, h.v, __int_as_float(hit ? h.prim : kMiss));
     }
   }
@@ -356,7 +356,7 @@ __global__ void __launch_bounds__(kWfBlock) wf_connect(V S, WfState W, int* stat
     const int k = base + lane;
     if (k < n) {
       const float4 o = W.sh_o[k], d = W.sh_d[k];
-      const bool blocked = any_hit_ww(S, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), o.w, status);
+      const bool blocked = any_hit_compact(S, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), o.w, status);
       if (!blocked) {
         const int tag = __float_as_int(d.w);
         const int path = tag >> 4, slot = tag & 15;
