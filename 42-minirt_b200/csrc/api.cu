@@ -132,6 +132,9 @@ struct mrt_ctx {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   DevBuf<float4> accum;
+  DevBuf<float> rgb_dev;                 // read-back staging: accumulator as rgb floats
+  float* rgb_host = nullptr;             // pinned host copy of rgb_dev
+  size_t rgb_host_n = 0;
   DevBuf<int> depth;
   DevBuf<int> status;
   DevBuf<unsigned long long> counters;
@@ -368,6 +371,8 @@ void mrt_destroy(mrt_ctx* c) {
   c->alias.release(); c->env_rec0.release(); c->env_rec1.release();
   c->ph_pos.release(); c->ph_pow.release(); c->ph_pos_raw.release(); c->ph_pow_raw.release();
   c->ph_nodes.release(); c->ph_count.release();
+  c->mat_tex.release(); c->texs.release(); c->texels.release(); c->rgb_dev.release();
+  if (c->rgb_host) cudaFreeHost(c->rgb_host);
   wf_destroy(c->wf);
   if (c->diff) { c->diff->release(); delete c->diff; }
   if (c->ev0) cudaEventDestroy(c->ev0);
@@ -1203,17 +1208,49 @@ extern "C" int mrt_clear(mrt_ctx* c) {
   return MRT_OK;
 }
 
+// The accumulator as rgb floats in the context's pinned host buffer: one
+// conversion kernel into a kept device buffer, one copy (no allocation after
+// the first call of a context).
+static int fetch_rgb(mrt_ctx* c) {
+  const size_t n3 = (size_t)c->W * c->H * 3;
+  if (c->rgb_dev.n != n3) CK(c->rgb_dev.alloc(n3));
+  if (c->rgb_host_n != n3) {
+    if (c->rgb_host) cudaFreeHost(c->rgb_host);
+    c->rgb_host = nullptr;
+    c->rgb_host_n = 0;
+    CK(cudaMallocHost(&c->rgb_host, n3 * sizeof(float)));
+    c->rgb_host_n = n3;
+  }
+  CK(launch_accum_to_rgb(c->accum.p, c->rgb_dev.p, (int)(n3 / 3), c->stream));
+  CK(cudaMemcpyAsync(c->rgb_host, c->rgb_dev.p, n3 * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return MRT_OK;
+}
+
+// f(begin, end) over [0, n) on up to 16 host threads (one for small n).
+template <class F>
+static void host_parallel(size_t n, F&& f) {
+  const unsigned t = std::min(16u, std::max(1u, std::thread::hardware_concurrency()));
+  if (t == 1 || n < (size_t)1 << 20) {
+    f((size_t)0, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  const size_t chunk = (n + t - 1) / t;
+  for (unsigned i = 0; i < t; ++i) {
+    const size_t a = i * chunk, b = std::min(n, a + chunk);
+    if (a < b) th.emplace_back([&f, a, b] { f(a, b); });
+  }
+  for (auto& x : th) x.join();
+}
+
 extern "C" int mrt_read_accum(mrt_ctx* c, float* rgb, int32_t* spp) {
   int rc = check_ctx(c);
   if (rc) return rc;
   if (!rgb) return set_err(MRT_ERR_INVALID, "null output");
-  const size_t n = (size_t)c->W * c->H;
-  float* d = nullptr;
-  CK(cudaMallocAsync(&d, n * 3 * sizeof(float), c->stream));
-  CK(launch_accum_to_rgb(c->accum.p, d, (int)n, c->stream));
-  CK(cudaMemcpyAsync(rgb, d, n * 3 * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaFreeAsync(d, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
+  if ((rc = fetch_rgb(c))) return rc;
+  const float* src = c->rgb_host;
+  host_parallel(c->rgb_host_n, [&](size_t a, size_t b) { std::memcpy(rgb + a, src + a, (b - a) * sizeof(float)); });
   if (spp) *spp = c->accum_spp;
   return MRT_OK;
 }
@@ -1222,11 +1259,11 @@ extern "C" int mrt_accumulate_double(mrt_ctx* c, double* float_render) {
   int rc = check_ctx(c);
   if (rc) return rc;
   if (!float_render) return set_err(MRT_ERR_INVALID, "null output");
-  const size_t n = (size_t)c->W * c->H;
-  std::vector<float> rgb(n * 3);
-  rc = mrt_read_accum(c, rgb.data(), nullptr);
-  if (rc) return rc;
-  for (size_t i = 0; i < 3 * n; ++i) float_render[i] += rgb[i];
+  if ((rc = fetch_rgb(c))) return rc;
+  const float* src = c->rgb_host;
+  host_parallel(c->rgb_host_n, [&](size_t a, size_t b) {
+    for (size_t i = a; i < b; ++i) float_render[i] += src[i];
+  });
   return mrt_clear(c);
 }
 
