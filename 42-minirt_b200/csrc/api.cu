@@ -350,6 +350,14 @@ mrt_ctx* mrt_create(int device, int width, int height) {
   if ((e = c->depth.alloc(np)) != cudaSuccess) return fail(e, "depth buffer");
   if ((e = c->status.alloc(1)) != cudaSuccess) return fail(e, "status word");
   if ((e = c->counters.alloc(8)) != cudaSuccess) return fail(e, "counters");
+  // read-back staging, sized with the frame: allocated here, before any
+  // scene memory, so that mrt_read_accum / mrt_accumulate_double allocate
+  // nothing (a first pinned allocation later, with gigabytes of wavefront
+  // state resident, measured 150-180 ms)
+  if ((e = c->rgb_dev.alloc(3 * np)) != cudaSuccess) return fail(e, "read-back buffer");
+  if ((e = cudaMallocHost(&c->rgb_host, 3 * np * sizeof(float))) != cudaSuccess)
+    return fail(e, "pinned read-back buffer");
+  c->rgb_host_n = 3 * np;
   cudaMemsetAsync(c->accum.p, 0, c->accum.bytes(), c->stream);
   cudaMemsetAsync(c->depth.p, 0, c->depth.bytes(), c->stream);
   cudaMemsetAsync(c->status.p, 0, sizeof(int), c->stream);
@@ -1209,8 +1217,8 @@ extern "C" int mrt_clear(mrt_ctx* c) {
 }
 
 // The accumulator as rgb floats in the context's pinned host buffer: one
-// conversion kernel into a kept device buffer, one copy (no allocation after
-// the first call of a context).
+// conversion kernel into the context's device buffer, one copy; both
+// buffers are allocated by mrt_create (the checks below only guard).
 static int fetch_rgb(mrt_ctx* c) {
   const size_t n3 = (size_t)c->W * c->H * 3;
   if (c->rgb_dev.n != n3) CK(c->rgb_dev.alloc(n3));
