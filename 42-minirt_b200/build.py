@@ -21,7 +21,7 @@ CSRC = HERE / "csrc"
 INCLUDE = HERE.parent / "include"
 NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["api.cu", "render.cu", "wavefront.cu", "env.cu", "env_noalloc.cu", "photon.cu", "adjoint.cu",
+SOURCES = ["api.cu", "render.cu", "readback.cu", "wavefront.cu", "env.cu", "env_noalloc.cu", "photon.cu", "adjoint.cu",
            "bvh_build.cpp"]
 
 

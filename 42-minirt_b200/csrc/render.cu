@@ -270,24 +270,6 @@ __global__ void first_hit_kernel(V S, const double* rays, int64_t n, HitOut* out
 }
 
 // Adds the float accumulator into a double t_fcolor buffer (device side) and clears it.
-__global__ void accumulate_double_kernel(float4* accum, double* out, int n) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  float4 a = accum[i];
-  out[3 * i] += a.x;
-  out[3 * i + 1] += a.y;
-  out[3 * i + 2] += a.z;
-  accum[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-}
-
-__global__ void accum_to_rgb_kernel(const float4* accum, float* rgb, int n) {
-  int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  float4 a = accum[i];
-  rgb[3 * i] = a.x;
-  rgb[3 * i + 1] = a.y;
-  rgb[3 * i + 2] = a.z;
-}
 
 __global__ void env_sample_kernel(SceneView S, int64_t n, uint64_t seed, int* k_out, float4* out) {
   int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -365,14 +347,5 @@ cudaError_t launch_first_hit(const SceneView& S, const double* rays, int64_t n, 
   return cudaGetLastError();
 }
 
-cudaError_t launch_accumulate_double(float4* accum, double* out, int n, cudaStream_t st) {
-  accumulate_double_kernel<<<(n + 255) / 256, 256, 0, st>>>(accum, out, n);
-  return cudaGetLastError();
-}
-
-cudaError_t launch_accum_to_rgb(const float4* accum, float* rgb, int n, cudaStream_t st) {
-  accum_to_rgb_kernel<<<(n + 255) / 256, 256, 0, st>>>(accum, rgb, n);
-  return cudaGetLastError();
-}
 
 }  // namespace mrt
