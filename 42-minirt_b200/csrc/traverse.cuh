@@ -243,8 +243,8 @@ __device__ __forceinline__ bool any_hit_compact(const V& S, float3 o, float3 d, 
   }
 }
 
-// The megakernel and the debug probes use the compact loop; the wavefront's
-// traversal kernels call the while-while form directly.
+// Entry points of the shading code (megakernels, probes, photon emission);
+// the wavefront's extend and connect kernels call the compact loops directly.
 template <bool kCount, class V>
 __device__ __forceinline__ bool closest_hit(const V& S, float3 o, float3 d, HitInfo& hit,
                                             int& visits, int* status, uint64_t akey = 0) {
