@@ -32,7 +32,6 @@
 
 namespace mrt {
 
-constexpr int kMaxLightsWf = 8;
 constexpr int kKinds = 4;   // 0 diffuse/default, 1 metal, 2 dielectric, 3 mixed metallic
 constexpr int kWfBlock = 128;
 
@@ -48,8 +47,8 @@ struct WfState {
   float4* sn;         // surface normal .xyz, -
   float4* sc;         // surface colour .xyz, env pdf
   float4* env;        // env radiance * ao .xyz, env cos
-  float4* lwork;      // per light: (dist or -, -, -, -) — unused, reserved
-  unsigned* vis;      // per path: visible-sample counts, 8 bits per light (<= 4 lights in a word pair)
+  unsigned* vis;      // visible-sample counts, 8 bits per light: word w of path i at
+                      // vis[w * capacity + i] holds lights 4w..4w+3
   unsigned* vis_env;  // per path: env visibility (0/1)
   // queues (path slot indices) and counters
   int* q_live[2];     // ping-pong extend queues
@@ -62,7 +61,16 @@ struct WfState {
   int capacity;
   int sh_capacity;
   int rays_per_path;  // shadow rays a diffuse event may emit
+  int vis_words;      // ceil(n_lights / 4)
 };
+
+// A shadow ray's tag (the int bits of sh_d.w): the path slot above kSlotBits
+// bits of light index; slot kEnvSlot is the HDRI sample. Path slots stay below
+// 2^(31 - kSlotBits) = kMaxWfCapacity.
+constexpr int kSlotBits = 10;
+constexpr int kEnvSlot = (1 << kSlotBits) - 1;
+constexpr int kMaxWfLights = kEnvSlot;
+constexpr int kMaxWfCapacity = 1 << (31 - kSlotBits);
 
 enum Cnt : int {
   C_LIVE0 = 0, C_LIVE1 = 1, C_KIND = 2,          // C_KIND..C_KIND+3
@@ -213,7 +221,7 @@ __device__ __forceinline__ void emit_shadow(const WfState& W, int path, int slot
     return;
   }
   W.sh_o[s] = make_float4(o.x, o.y, o.z, tmax);
-  W.sh_d[s] = make_float4(d.x, d.y, d.z, __int_as_float((path << 4) | slot));
+  W.sh_d[s] = make_float4(d.x, d.y, d.z, __int_as_float((path << kSlotBits) | slot));
 }
 
 template <int kBounceParity, class V>
@@ -282,7 +290,6 @@ __global__ void __launch_bounds__(kWfBlock) wf_sample(V S, WfState W, const WfPa
         // default_mat (material_default.c:71-92): shadow rays of compute_light
         // (light order, soft-shadow targets drawn now), the HDRI sample, the
         // next direction; visibility-dependent terms are applied in finish.
-        int slot = 0;
         for (int l = 0; l < S.n_lights; ++l) {
           const LightD L = S.lights[l];
           const float3 lp = ld3(L.pos);
@@ -300,9 +307,8 @@ __global__ void __launch_bounds__(kWfBlock) wf_sample(V S, WfState W, const WfPa
           } else {
             emit_shadow(W, i, l, s.p, unit(-lp), INFINITY, status);
           }
-          (void)slot;
         }
-        W.vis[i] = 0u;
+        for (int w = 0; w < W.vis_words; ++w) W.vis[(size_t)w * W.capacity + i] = 0u;
         W.vis_env[i] = 0u;
         float env_pdf = 0.f, env_ct = 0.f;
         float3 env_rad = f3(0.f, 0.f, 0.f);
@@ -315,7 +321,7 @@ __global__ void __launch_bounds__(kWfBlock) wf_sample(V S, WfState W, const WfPa
           const float4 r = __ldg(S.env_rec1 + kk);
           env_rad = f3(r.x, r.y, r.z);
           if (s.mat >= 0) env_rad = env_rad * S.mats[s.mat].ao;
-          emit_shadow(W, i, 15, s.p, dir, INFINITY, status);
+          emit_shadow(W, i, kEnvSlot, s.p, dir, INFINITY, status);
         }
         ps.d = cos_hemisphere(ps.rng, s.n);
         W.sp[i] = make_float4(s.p.x, s.p.y, s.p.z, __int_as_float(s.mat));
@@ -359,9 +365,9 @@ __global__ void __launch_bounds__(kWfBlock) wf_connect(V S, WfState W, int* stat
       const bool blocked = any_hit_compact(S, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), o.w, status);
       if (!blocked) {
         const int tag = __float_as_int(d.w);
-        const int path = tag >> 4, slot = tag & 15;
-        if (slot == 15) W.vis_env[path] = 1u;
-        else atomicAdd(&W.vis[path], 1u << (8 * (slot & 3)));
+        const int path = tag >> kSlotBits, slot = tag & kEnvSlot;
+        if (slot == kEnvSlot) W.vis_env[path] = 1u;
+        else atomicAdd(&W.vis[(size_t)(slot >> 2) * W.capacity + path], 1u << (8 * (slot & 3)));
       }
     }
   }
@@ -385,14 +391,15 @@ __global__ void __launch_bounds__(kWfBlock) wf_finish(SceneView S, WfState W) {
       float3 power = f3(pw4.x, pw4.y, pw4.z);
       float4 a4 = W.acc[i];
       float3 acc = f3(a4.x, a4.y, a4.z);
-      const unsigned vis = W.vis[i];
       // compute_light_v2 with the visibility found by connect
       float lc0 = 0.f, lc1 = 0.f, lc2 = 0.f;
       if (S.n_lights) {
         const float3 view = unit(ld3(S.cam) - p);
+        unsigned vis = 0u;
         for (int l = 0; l < S.n_lights; ++l) {
           const LightD L = S.lights[l];
           const float3 lp = ld3(L.pos);
+          if ((l & 3) == 0) vis = W.vis[(size_t)(l >> 2) * W.capacity + i];
           const int seen = (int)((vis >> (8 * (l & 3))) & 255u);
           if (L.type == 0) {
             float sf;
@@ -490,6 +497,7 @@ using namespace mrt;
 
 struct WfHost {
   int capacity = 0, sh_capacity = 0;
+  int vis_words = 0;
   int sms = 0;
   WfState st{};
   WfParams* dparams = nullptr;
@@ -506,11 +514,14 @@ static cudaError_t wf_alloc(WfHost* H, int capacity, int n_lights, bool env) {
   H->graph_bounces = -1;
   H->sh_capacity = 0;          // the shadow queue went with the other buffers
   const int rays = n_lights * 1 + (env ? 1 : 0);
+  const int vis_words = std::max(1, (n_lights + 3) / 4);
   H->capacity = capacity;
+  H->vis_words = vis_words;
   WfState& s = H->st;
   s = WfState{};
   s.capacity = capacity;
   s.rays_per_path = rays;
+  s.vis_words = vis_words;
   auto A = [&](void** p, size_t bytes) -> cudaError_t {
     cudaError_t e = cudaMalloc(p, bytes > 0 ? bytes : 16);
     if (e == cudaSuccess) H->allocs.push_back(*p);
@@ -521,12 +532,11 @@ static cudaError_t wf_alloc(WfHost* H, int capacity, int n_lights, bool env) {
 #define AL(field, bytes) if ((e = A((void**)&s.field, (bytes))) != cudaSuccess) return e
   AL(o, n * 16); AL(d, n * 16); AL(pw, n * 16); AL(acc, n * 16); AL(rng, n * 8); AL(hit, n * 16);
   AL(sp, n * 16); AL(sn, n * 16); AL(sc, n * 16); AL(env, n * 16);
-  AL(vis, n * 4); AL(vis_env, n * 4);
+  AL(vis, n * 4 * vis_words); AL(vis_env, n * 4);
   AL(q_live[0], n * 4); AL(q_live[1], n * 4); AL(q_kind, n * 4 * kKinds); AL(q_def, n * 4);
   AL(counters, sizeof(int) * C_COUNT);
   if ((e = A((void**)&H->dparams, sizeof(WfParams))) != cudaSuccess) return e;
 #undef AL
-  s.lwork = nullptr;
   return cudaMemset(s.counters, 0, sizeof(int) * C_COUNT);
 }
 
@@ -611,12 +621,15 @@ int wf_render(WfHost* H, const SceneView& v, const LaunchParams& L, int spp, int
   const uint64_t npix = (uint64_t)v.width * v.height;
   const uint64_t total = npix * (uint64_t)spp;
   if (total == 0) return MRT_OK;
-  if (v.n_lights > 4) { *err = "wavefront form supports up to 4 lights (use the megakernel)"; return MRT_ERR_INVALID; }
-  for (int l = 0; l < v.n_lights; ++l) (void)l;
+  if (v.n_lights > kMaxWfLights) {
+    *err = "wavefront form supports up to 1023 lights (use the megakernel)";
+    return MRT_ERR_INVALID;
+  }
   if (capacity <= 0) capacity = 1 << 22;
+  capacity = std::min(capacity, kMaxWfCapacity);
   capacity = (int)std::min<uint64_t>((uint64_t)capacity, std::max<uint64_t>(total, 1024));
   cudaError_t e;
-  if (H->capacity != capacity) {
+  if (H->capacity != capacity || H->vis_words != std::max(1, (v.n_lights + 3) / 4)) {
     if ((e = wf_alloc(H, capacity, v.n_lights, v.env_nee)) != cudaSuccess) { *err = cudaGetErrorString(e); return MRT_ERR_OOM; }
   }
   // shadow rays per diffuse event: hard lights 1, soft lights shadow_sample, env 1
@@ -695,7 +708,8 @@ int wf_render(WfHost* H, const SceneView& v, const LaunchParams& L, int spp, int
 WfHost* wf_create() { return new WfHost(); }
 
 size_t wf_device_bytes(const WfHost* H) {
-  return H ? (size_t)H->capacity * (16 * 10 + 8 + 4 * 6 + 4 * kKinds) + (size_t)H->sh_capacity * 32 : 0;
+  return H ? (size_t)H->capacity * (16 * 10 + 8 + 4 * (4 + H->vis_words) + 4 * kKinds) + (size_t)H->sh_capacity * 32
+           : 0;
 }
 
 void wf_destroy(WfHost* H) {
