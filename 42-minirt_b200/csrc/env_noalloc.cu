@@ -10,9 +10,13 @@
 // fixed array below instead of in per-call allocations.
 //
 // The array is a file-scope __device__ variable: every GPU that loads this
-// library holds it (about 4 MiB) until the process exits. Its host-side name
-// is only a stand-in for the symbol, not a device address, so the device
-// address is looked up once per device with cudaGetSymbolAddress and cached.
+// module holds it (about 4 MiB) until the process exits. With lazy module
+// loading the module loads on the first call on a device, so that first call
+// takes the array's memory through the driver; later calls allocate nothing.
+// Its host-side name is only a stand-in for the symbol, not a device
+// address, so the device address is looked up once per device with
+// cudaGetSymbolAddress and cached; the cache is not refreshed after
+// cudaDeviceReset, which this entry point does not support.
 #include <cuda_runtime.h>
 
 #include <cmath>

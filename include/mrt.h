@@ -513,12 +513,21 @@ MRT_API int			mrt_caustic_query(mrt_ctx *ctx, const double *points3, int64_t n,
  * width*height <= MRT_ENV_NOALLOC_MAX_TEXELS (512x512 or 1024x256);
  * larger skies get MRT_ERR_INVALID with the limit in mrt_last_error(). The
  * build's scratch (about 4 MiB of doubles) is a fixed array in the library
- * that each GPU holds from the library's load until the process exits. The
- * first call on a device looks up that array's device address (set-up done
- * once per device); make that first call before any stream capture. All
- * calls on a device share the array, so calls that overlap on the GPU (from
- * several host threads or streams at once) race and must be serialised by
- * the caller. Every scratch value a call reads it has written itself, so
+ * that each GPU holds, once loaded, until the process exits.
+ *
+ * First call per device: with CUDA's lazy module loading (the default), the
+ * modules that hold the array and the table kernels load on first use, and
+ * the first call also looks up the array's device address (set-up done once
+ * per device). That first call therefore does take device memory (the
+ * modules and the 4 MiB array) through the driver: make it once at start-up,
+ * before the host fixes its arena; later calls allocate nothing.
+ * The call synchronises `stream` before it returns, so it must not be made on
+ * a stream that is being captured into a CUDA graph.
+ * The cached device address is not refreshed after cudaDeviceReset: a host
+ * that resets a device must not call this entry point on it afterwards.
+ * All calls on a device share the array, so calls that overlap on the GPU
+ * (from several host threads or streams at once) race and must be serialised
+ * by the caller. Every scratch value a call reads it has written itself, so
  * what an earlier call left there does not matter. */
 # define MRT_ENV_NOALLOC_MAX_TEXELS 262144
 # define MRT_ENV_NOALLOC_MAX_ROWS 4096
