@@ -11,11 +11,12 @@ samples per pixel (16 steps = the 256 spp render).
               steps, inputs resident in HBM; the best of the forms (plain
               one-path-per-thread megakernel, persistent regenerating
               megakernel, wavefront), each reported under "forms".
-  relmse      time to relMSE <= 1e-3: relMSE(N) = mean((img-ref)^2/(ref^2+0.01))
-              is measured at 16 and 256 spp against an independent --ref-spp
-              render; relMSE = c/N (unbiased estimator, independent
-              reference noise c/ref_spp), so N* = c/1e-3 and the time per
-              form is N* x pixels / Mpaths/s.
+  relmse      time to relMSE <= 1e-3 against the reference's own CPU render
+              at 4096 spp (tests/golden/conv_<config>.npz, a stratified
+              subset of 4,096 pixels): the best form renders progressively
+              until relMSE against the converged image (reference noise
+              subtracted) is <= 1e-3; measured device time to that point,
+              and that sample count at each other form's rate.
   e2e         the same render through the C-ABI a reference host calls:
               per step a camera upload, the render and a device->host read of
               the frame accumulated into a pinned double buffer
@@ -67,7 +68,8 @@ def parse():
     ap.add_argument("--spp-per-step", type=int, default=16)
     ap.add_argument("--forms", default="megakernel_plain,megakernel,wavefront")
     ap.add_argument("--no-relmse", action="store_true")
-    ap.add_argument("--ref-spp", type=int, default=1024)
+    ap.add_argument("--relmse-cap-spp", type=int, default=4096,
+                    help="stop the time-to-relMSE render here if 1e-3 is not reached")
     ap.add_argument("--cpu-seconds", type=float, default=8.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
@@ -152,41 +154,67 @@ def run_reference_arm(a) -> None:
     print(json.dumps(line), flush=True)
 
 
-def rel_mse(img: np.ndarray, ref: np.ndarray) -> float:
-    return float(np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2)))
+def convergence(ctx, sc, config: str, spp_step: int, forms: dict, fid: int, cap_spp: int) -> dict:
+    """Time to relMSE <= 1e-3 against the reference CPU render at 4096 spp.
 
-
-def convergence(ctx, sc, spp_step: int, ref_spp: int, forms: dict, fid: int) -> dict:
-    """Time to relMSE <= 1e-3 per form from the measured 1/N law."""
+    The comparator is the converged-radiance fixture tests/golden/conv_<config>.npz:
+    the reference's own calc_one_sample_task at 4096 samples per pixel on a
+    seeded stratified subset of 4,096 pixels (every pixel for c0), with the
+    variance of each pixel's mean. The best form renders the frame
+    progressively (spp_step samples per call); after each call its image is
+    compared at the fixture's pixels with relMSE against the converged image,
+    mean(((x - r)^2 - var_r) / (r^2 + 0.01)) (the reference's own noise
+    var_r subtracted). The time is the device time of the calls up to the
+    first one at or below 1e-3, rendered, not extrapolated; for the other
+    forms (same estimator, same paths) it is that sample count at their
+    measured rate. c = relMSE * N fitted over the run is reported beside it."""
+    import convergence as cv
+    path = REPO / "tests" / "golden" / f"conv_{config}.npz"
+    if not path.exists():
+        return {"unavailable": f"no converged-radiance fixture for {config}"}
+    fx = cv.load_fixture(path)
+    pix, r, var_r = fx["pixels"], fx["mean"].astype(np.float64), fx["var_mean"].astype(np.float64)
     ctx.clear()
-    done = 0
-    while done < ref_spp:
-        k = min(64, ref_spp - done)
-        ctx.render(k, seed=777, sample_base=done, form=fid)
-        done += k
-    ref, n = ctx.read_accum()
-    ref = ref / n
-    pts = {}
-    for n_spp in (16, 256):
-        ctx.clear()
-        done = 0
-        while done < n_spp:
-            k = min(spp_step, n_spp - done)
-            ctx.render(k, seed=31, sample_base=done, form=fid)
-            done += k
+    done, ms, trace, reached = 0, 0.0, [], None
+    while done < cap_spp:
+        st = ctx.render(spp_step, seed=31, sample_base=done, form=fid)
+        ms += st.ms
+        done += spp_step
         img, n = ctx.read_accum()
-        pts[n_spp] = rel_mse(img / n, ref)
-    c = (pts[16] - pts[256]) / (1 / 16 - 1 / 256)
-    c = max(c, 1e-12)
-    n_star = c / 1e-3
+        x = cv.pixel_values(img / n, pix)
+        rc = cv.relmse_converged(x, r, var_r)
+        trace.append((done, rc))
+        if rc <= 1e-3:
+            reached = (done, ms, rc, cv.relmse(x, r))
+            break
+    ctx.clear()
+    ns = np.array([t[0] for t in trace], np.float64)
+    rs = np.array([t[1] for t in trace], np.float64)
+    keep = ns >= 4 * spp_step
+    c = float(np.sum(rs[keep] / ns[keep]) / np.sum(1.0 / ns[keep] ** 2)) if keep.any() else None
     npix = sc.width * sc.height
-    out = {"relmse_16spp": pts[16], "relmse_256spp": pts[256], "ref_spp": ref_spp,
-           "c": c, "spp_to_1e-3": n_star, "relmse_definition": "mean((x-r)^2/(r^2+0.01))"}
+    out = {"ref": "reference CPU render, 4096 spp (tests/golden/conv_%s.npz, %d pixels)" % (config, len(pix)),
+           "relmse_definition": "mean(((x-r)^2 - var_r)/(r^2+0.01)) at the fixture's pixels: "
+                                "relMSE against the converged image the reference estimates",
+           "relmse_ref_noise": float(np.mean(var_r / (r ** 2 + 1e-2))),
+           "c_fit": c, "trace": [[int(a), float(b)] for a, b in trace[:: max(1, len(trace) // 16)]]}
+    if reached is None:
+        out.update({"reached": False, "spp_rendered": done, "relmse_last": float(rs[-1])})
+        return out
+    spp_hit, ms_hit, rc_hit, raw_hit = reached
+    out.update({"reached": True, "spp_to_1e-3": spp_hit, "relmse_at_stop": rc_hit,
+                "relmse_raw_at_stop": raw_hit, "measured_form_ms": ms_hit})
     for name, f in forms.items():
         if "value" in f:
-            out[f"time_to_1e-3_s_{name}"] = n_star * npix / (f["value"] * 1e6)
-    ctx.clear()
+            out[f"time_to_1e-3_s_{name}"] = (ms_hit / 1000.0 if form_ids_name(fid) == name
+                                             else spp_hit * npix / (f["value"] * 1e6))
     return out
+
+
+def form_ids_name(fid: int) -> str:
+    import mrt
+    return {mrt.FORM_MEGAKERNEL: "megakernel", mrt.FORM_WAVEFRONT: "wavefront",
+            mrt.FORM_MEGAKERNEL_PLAIN: "megakernel_plain"}.get(fid, "?")
 
 
 def adjoint_bench(device: int, adam_steps: int, res: int = 512) -> dict:
@@ -458,7 +486,7 @@ def main() -> int:
 
     relmse = None
     if not a.no_relmse and world == 1:
-        relmse = convergence(ctx, sc, spp, a.ref_spp, forms, form_ids[best])
+        relmse = convergence(ctx, sc, a.config, spp, forms, form_ids[best], a.relmse_cap_spp)
     adjoint = None
     if not a.no_adjoint and world == 1:
         adjoint = adjoint_bench(local, a.adam_steps)

@@ -1,0 +1,95 @@
+"""Converged radiance of the CUDA path against the reference's own CPU render.
+
+The fixtures (tests/golden/conv_*.npz, made by tests/golden/make_converged.py)
+hold the reference's calc_one_sample_task (src/ray_tracing/calc_sample.c:44)
+at 4096 samples per pixel on each benchmark configuration: every pixel of c0,
+a seeded stratified subset of 4,096 pixels of c1, c2 and c4, with the variance
+of each pixel's mean from 64 batch means. The GPU renders the same scene with
+the wavefront form (the benchmark's form) in batches through the C-ABI, and
+the two are compared with the statistics of 42-minirt_b200/convergence.py:
+
+  * relmse_bias <= 1e-3: relMSE of the expectations (noise of both renders
+    subtracted), i.e. no bias beyond the metric's bar;
+  * relmse_converged <= 1e-3 where the GPU render has enough samples for its
+    own noise to be below the bar (all configurations but c2, whose caustics
+    need ~15k samples per pixel);
+  * image-mean bias test: |mean difference| <= 4 standard errors per channel,
+    the standard error from the batch image means of both sides;
+  * per-pixel z-scores: at most 0.5 % of pixels beyond 5 standard errors.
+
+c2 is the reference's single-pass kNN mode (k = 15, 2 M photons). A kNN image
+depends on its photon set, so the GPU is given the reference's own photon
+map: the compiled reference (oracle/_ref) rebuilds it for the fixture's RNG
+seed, its digest is checked against the fixture, and its leaf photons (the
+ones the reference's kd-tree gathers) are uploaded with mrt_set_photons.
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+# samples per pixel of the GPU render, in 16 batches
+GPU_SPP = {"c0": 16384, "c1": 4096, "c2": 4096, "c4": 16384}
+BATCHES = 16
+
+
+@pytest.fixture(scope="module", autouse=True)
+def require_device(mrt):
+    lib = mrt.load()
+    assert lib.mrt_device_count() > 0, "gpu tests need a CUDA device"
+
+
+def render_batches(mrt, ctx, pixels, spp, batches, form):
+    """Per-pixel batch means at `pixels` and per-batch image means."""
+    spp_b = spp // batches
+    bm = []
+    for b in range(batches):
+        ctx.clear()
+        ctx.render(spp_b, seed=99, sample_base=b * spp_b, form=form)
+        img, n = ctx.read_accum()
+        assert n == spp_b
+        h, w = img.shape[:2]
+        bm.append(img.reshape(h * w, -1)[pixels, :3] / n)
+    bm = np.stack(bm).astype(np.float64)
+    return bm.mean(0), bm.var(0, ddof=1) / batches, bm.mean(1)
+
+
+def reference_photons(oracle, sc, seed):
+    oracle.ref_lib().refh_set_seed(seed)
+    ref = oracle.RefOracle(sc)
+    pos, pw, leaf = ref.photons()
+    ref.close()
+    return pos[leaf], pw[leaf]
+
+
+@pytest.mark.parametrize("name", ["c0", "c4", "c1", "c2"])
+def test_converged_radiance_matches_reference_cpu_render(mrt, oracle, scenes, name):
+    import convergence
+    fx = convergence.load_fixture(GOLDEN / f"conv_{name}.npz")
+    sc = {"c0": scenes.make_c0, "c1": scenes.make_c1, "c2": scenes.make_c2, "c4": scenes.make_c4}[name]()
+    assert (sc.width, sc.height, sc.max_bounces) == (fx["width"], fx["height"], fx["depth"])
+    ctx = mrt.Context(sc.width, sc.height)
+    ctx.build(oracle.canonical_scene(sc))
+    if name == "c2":
+        pos, pw = reference_photons(oracle, sc, 12345)
+        h = hashlib.sha256()
+        h.update(np.ascontiguousarray(pos, np.float64).tobytes())
+        h.update(np.ascontiguousarray(pw, np.float64).tobytes())
+        assert h.hexdigest() == fx["photon_digest"], "the reference rebuilt a different photon map"
+        ctx.set_photons(pos, pw)
+    x, var_x, bmx = render_batches(mrt, ctx, fx["pixels"], GPU_SPP[name], BATCHES, mrt.FORM_WAVEFRONT)
+    ctx.close()
+    st = convergence.compare(x, var_x, bmx, fx)
+    print(name, json.dumps(st))
+    assert st["relmse_bias"] <= 1e-3, st
+    if name != "c2":
+        assert st["relmse_converged"] <= 1e-3, st
+    assert np.all(np.abs(st["image_mean_z"]) <= 4.0), st
+    assert st["pixel_z_gt5"] <= 0.005, st

@@ -1,9 +1,10 @@
 """Parity of the CUDA path (libmrt.so, through the C-ABI) with the oracle.
 
  * first hits: primitive id bit-exact; t within 1e-5 relative (FP32 kernels vs
-   the FP64 reference). Rays whose two candidate surfaces are within 1e-4 in t
-   form a reported "tie" bucket; grazing disagreements (one side misses) are
-   bounded by a tiny fraction.
+   the FP64 reference), on every ray outside the documented buckets of
+   tests/hitcheck.py: "tie" (two surfaces within 1e-4 in t) and "boundary"
+   (the ray within 1e-5 of a triangle edge or a sphere silhouette, where the
+   FP32 rounding of the ray can change the answer).
  * HDRI tables built on the device in FP64: bit-exact with the reference.
  * radiance: the same counter-RNG stream drives the GPU path (FP32) and the
    oracle path (FP64); per-pixel agreement within 1e-3 relative for nearly all
@@ -15,6 +16,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
+import hitcheck
 from conftest import golden
 
 pytestmark = pytest.mark.gpu
@@ -42,23 +44,35 @@ def gpu_ctx(mrt, oracle, scene):
     return ctx
 
 
-def classify_hits(g_prim, g_t, g_p, r_prim, r_t, r_p):
-    """Buckets of the first-hit comparison (gpu vs oracle)."""
-    both = (g_prim >= 0) & (r_prim >= 0)
-    same = g_prim == r_prim
-    t_rel = np.abs(g_t - r_t) / np.maximum(np.abs(r_t), 1e-6)
-    exact = same & ((~both) | (t_rel <= 1e-5))
-    dist = np.linalg.norm(g_p - r_p, axis=1)
-    tie = (~same) & both & (t_rel <= 1e-4) & (dist <= 1e-3 * np.maximum(r_t, 1.0))
-    other = ~(exact | tie)
-    return exact, tie, other
-
-
 def random_rays(rng, vp, n, spread=0.3):
     o = vp["cam"][None] + rng.normal(size=(n, 3)) * spread
     d = rng.normal(size=(n, 3))
     d /= np.linalg.norm(d, axis=1, keepdims=True)
     return o, d
+
+
+def tri_positions(oracle, sc):
+    ro = oracle.Restatement(sc)
+    tp = ro.triangle_positions() if sc.n_triangles else np.zeros((0, 9))
+    ro.close()
+    return tp
+
+
+def assert_hit_parity(name, sc, tp, o, d, h, r):
+    """No real disagreement: every ray is exact, a tie or on a triangle edge /
+    sphere silhouette (tests/hitcheck.py). Quadric grazes are not modelled
+    there, so q0 and t0 (cylinders, cones, hyperboloids) keep a bound of a few
+    rays for them."""
+    exact, tie, boundary, other = hitcheck.classify(sc, tp, o, d, h, r)
+    print(f"{name}: exact {exact.mean():.5f} tie {int(tie.sum())} boundary {int(boundary.sum())} "
+          f"other {int(other.sum())} of {len(h)}")
+    if name in ("q0", "t0"):
+        assert other.sum() <= max(2, int(0.0005 * len(h))), int(other.sum())
+    else:
+        bad = np.nonzero(other)[0][:5]
+        assert not other.any(), [(int(i), int(h["prim"][i]), int(r["prim"][i])) for i in bad]
+    assert exact.mean() >= 0.998
+    return exact
 
 
 @pytest.mark.parametrize("name", ["c0", "c1", "c2", "q0", "t0"])
@@ -67,11 +81,8 @@ def test_first_hit_matches_reference_golden(mrt, oracle, mg, name):
     sc = mg.CASES[name]["make"]()
     ctx = gpu_ctx(mrt, oracle, sc)
     h = ctx.first_hit(g["rays_o"], g["rays_d"])
-    exact, tie, other = classify_hits(h["prim"], h["t"], h["point"], g["hit_prim"], g["hit_t"],
-                                      g["hit_point"])
-    print(f"{name}: exact {exact.mean():.5f} tie {tie.sum()} other {other.sum()} of {len(h)}")
-    assert exact.mean() >= 0.998
-    assert other.sum() <= max(2, int(0.001 * len(h)))
+    ref = {"prim": g["hit_prim"], "t": g["hit_t"], "point": g["hit_point"]}
+    exact = assert_hit_parity(name, sc, tri_positions(oracle, sc), g["rays_o"], g["rays_d"], h, ref)
     hit = (h["prim"] >= 0) & exact
     np.testing.assert_array_equal(h["front_face"][hit], g["hit_front_face"][hit])
     close = np.abs(h["normal"][hit] - g["hit_normal"][hit]).max(axis=1) <= 2e-4
@@ -92,10 +103,8 @@ def test_first_hit_matches_oracle_on_fresh_rays(mrt, oracle, mg, name):
     vp = dict(cam=np.array(sc.camera["position"]))
     o, d = random_rays(rng, vp, 50000)
     h, r = ctx.first_hit(o, d), ro.first_hit(o, d)
-    exact, tie, other = classify_hits(h["prim"], h["t"], h["point"], r["prim"], r["t"], r["point"])
-    print(f"{name}: exact {exact.mean():.5f} tie {tie.sum()} other {other.sum()}")
-    assert exact.mean() >= 0.998
-    assert other.sum() <= max(3, int(0.0005 * len(h)))
+    tp = ro.triangle_positions() if sc.n_triangles else np.zeros((0, 9))
+    assert_hit_parity(name, sc, tp, o, d, h, r)
 
 
 def test_env_tables_bit_exact_with_reference(mrt, oracle, mg):

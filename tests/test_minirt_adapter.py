@@ -2,7 +2,8 @@
 its init_viewport builds it, rendered through the reference-named GPU entry
 points (init_shader, convert_scene_build, convert_scene, compute_frame_gpu,
 calc_one_sample, clean_*) and compared with the reference's CPU render of the
-same structure."""
+same structure: per pixel, from batch means of both renders (image-mean
+bias, per-pixel z-scores and the bias relMSE, 42-minirt_b200/convergence.py)."""
 from __future__ import annotations
 
 import ctypes as C
@@ -35,6 +36,44 @@ def adapter(mrt, oracle):
     return lib
 
 
+def gpu_batches(adapter, ref, m, n, batches):
+    """compute_frame_gpu n times; batch means of the drop-in's float_render."""
+    out, prev = [], ref.accum()
+    for _ in range(batches):
+        for _ in range(n // batches):
+            adapter.compute_frame_gpu(m)
+        cur = ref.accum()
+        out.append((cur - prev) / (n // batches))
+        prev = cur
+    return np.stack(out)
+
+
+def cpu_batches(ref, n, batches):
+    """The reference's calc_one_sample n times; batch means."""
+    out = []
+    for _ in range(batches):
+        ref.clear()
+        ref.render(n // batches)
+        out.append(ref.accum() / (n // batches))
+    return np.stack(out)
+
+
+def assert_same_image(gpu_bm, cpu_bm, what):
+    """Per-pixel agreement of two independent renders of one scene, each
+    given as batch means: no image-mean bias (4 standard errors per channel),
+    at most 1 % of pixels beyond 5 standard errors (a shifted or blurred
+    image fails at its edges), and the bias relMSE (both renders' noise
+    subtracted) within 1e-3 plus 4 standard errors."""
+    import convergence as cv
+    g, r = cv.batch_summary(gpu_bm), cv.batch_summary(cpu_bm)
+    st = cv.compare(g["mean"], g["var_mean"], g["batch_image_mean"], r)
+    print(what, {k: st[k] for k in ("relmse_raw", "relmse_bias", "relmse_bias_se", "image_mean_z",
+                                    "pixel_z_rms", "pixel_z_gt5")})
+    assert np.all(np.abs(st["image_mean_z"]) <= 4.0), st
+    assert st["pixel_z_gt5"] <= 0.01, st
+    assert st["relmse_bias"] <= 1e-3 + 4 * st["relmse_bias_se"], st
+
+
 def counters(ref):
     out = np.zeros(3, np.int32)
     ref.lib.refh_sample_counters(ref.h, out.ctypes.data)
@@ -54,19 +93,12 @@ def test_compute_frame_gpu_matches_reference_render(adapter, oracle, scenes):
     assert cnt[0] == 1 and cnt[1] == len(sc.spheres) and cnt[2] == len(sc.planes)
     adapter.convert_scene(m, scn, vp, g)
     n = 512
-    for _ in range(n):
-        adapter.compute_frame_gpu(m)
+    gpu = gpu_batches(adapter, ref, m, n, 16)
     assert tuple(counters(ref)) == (n, n, n)
-    gpu = ref.accum() / n
     # the reference itself, on a second copy of the same scene
     ref2 = oracle.RefOracle(sc)
     ref2.set_seed(2024)
-    ref2.render(n)
-    cpu = ref2.accum() / n
-    d = (gpu - cpu).mean(axis=2).reshape(-1)
-    se = d.std() / np.sqrt(d.size)
-    print("image mean gpu", gpu.mean(), "cpu", cpu.mean(), "z", d.mean() / se)
-    assert abs(d.mean()) <= 4 * se
+    assert_same_image(gpu, cpu_batches(ref2, n, 16), "c0 drop-in")
     adapter.clean_shaders(sd)
     adapter.clean_scene(g)
 
@@ -102,7 +134,7 @@ def test_unsupported_objects_are_reported(adapter, oracle, scenes):
 
 def test_compute_frame_gpu_with_quadrics_matches_reference_render(adapter, oracle, scenes):
     """Cylinders, cones and hyperboloids of t_scene go through the drop-in
-    too: the image agrees with the reference's own CPU render in the mean."""
+    too: the image agrees with the reference's own CPU render per pixel."""
     sc = scenes.make_quadrics(5, 48, 36, depth=6)
     ref = oracle.RefOracle(sc)
     L = ref.lib
@@ -111,18 +143,11 @@ def test_compute_frame_gpu_with_quadrics_matches_reference_render(adapter, oracl
     assert adapter.init_shader(sd, sc.width, sc.height, scn) == 0
     assert adapter.convert_scene_build(m, scn, vp, g) == 0
     adapter.convert_scene(m, scn, vp, g)
-    n = 256
-    for _ in range(n):
-        adapter.compute_frame_gpu(m)
-    gpu = ref.accum() / n
+    n = 512
+    gpu = gpu_batches(adapter, ref, m, n, 16)
     ref2 = oracle.RefOracle(sc)
     ref2.set_seed(99)
-    ref2.render(n)
-    cpu = ref2.accum() / n
-    d = (gpu - cpu).mean(axis=2).reshape(-1)
-    se = d.std() / np.sqrt(d.size)
-    print("quadrics image mean gpu", gpu.mean(), "cpu", cpu.mean(), "z", d.mean() / se)
-    assert abs(d.mean()) <= 4 * se
+    assert_same_image(gpu, cpu_batches(ref2, n, 16), "quadrics drop-in")
     adapter.clean_shaders(sd)
     adapter.clean_scene(g)
 
@@ -137,17 +162,10 @@ def test_compute_frame_gpu_with_textures_matches_reference_render(adapter, oracl
     assert adapter.init_shader(sd, sc.width, sc.height, scn) == 0
     assert adapter.convert_scene_build(m, scn, vp, g) == 0
     adapter.convert_scene(m, scn, vp, g)
-    n = 256
-    for _ in range(n):
-        adapter.compute_frame_gpu(m)
-    gpu = ref.accum() / n
+    n = 512
+    gpu = gpu_batches(adapter, ref, m, n, 16)
     ref2 = oracle.RefOracle(sc)
     ref2.set_seed(77)
-    ref2.render(n)
-    cpu = ref2.accum() / n
-    d = (gpu - cpu).mean(axis=2).reshape(-1)
-    se = d.std() / np.sqrt(d.size)
-    print("textures image mean gpu", gpu.mean(), "cpu", cpu.mean(), "z", d.mean() / se)
-    assert abs(d.mean()) <= 4 * se
+    assert_same_image(gpu, cpu_batches(ref2, n, 16), "textures drop-in")
     adapter.clean_shaders(sd)
     adapter.clean_scene(g)

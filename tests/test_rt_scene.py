@@ -44,7 +44,7 @@ def test_drop_in_renders_the_parsed_scene_like_the_reference(mrt, oracle):
                             ("clean_shaders", None, [P]), ("clean_scene", None, [P])]:
         f = getattr(lib, name)
         f.restype, f.argtypes = res, args
-    W, H, depth, n = 48, 36, 6, 256
+    W, H, depth, n = 48, 36, 6, 512
     ref = oracle.RefOracle.from_rt(RT, W, H, depth)
     L = ref.lib
     m, scn, vp = L.refh_minirt(ref.h), L.refh_scene_ptr(ref.h), L.refh_viewport_ptr(ref.h)
@@ -52,16 +52,10 @@ def test_drop_in_renders_the_parsed_scene_like_the_reference(mrt, oracle):
     assert lib.init_shader(sd, W, H, scn) == 0
     assert lib.convert_scene_build(m, scn, vp, g) == 0
     lib.convert_scene(m, scn, vp, g)
-    for _ in range(n):
-        lib.compute_frame_gpu(m)
-    gpu = ref.accum() / n
+    from test_minirt_adapter import assert_same_image, cpu_batches, gpu_batches
+    gpu = gpu_batches(lib, ref, m, n, 16)
     cpu_ref = oracle.RefOracle.from_rt(RT, W, H, depth)
     cpu_ref.set_seed(11)
-    cpu_ref.render(n)
-    cpu = cpu_ref.accum() / n
-    d = (gpu - cpu).mean(axis=2).reshape(-1)
-    se = d.std() / np.sqrt(d.size)
-    print("parsed scene: mean gpu", gpu.mean(), "reference", cpu.mean(), "z", d.mean() / se)
-    assert abs(d.mean()) <= 4 * se
+    assert_same_image(gpu, cpu_batches(cpu_ref, n, 16), "parsed .rt scene")
     lib.clean_shaders(sd)
     lib.clean_scene(g)
