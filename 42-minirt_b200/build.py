@@ -35,7 +35,7 @@ UNITS = [("render_inst.cu", f"render_{tag}_g{g}", [f"-DMRT_VIEW={view}", f"-DMRT
          for view, tag in _VIEWS for g in (0, 2, 3, 1)]
 UNITS += [(src, Path(src).stem, []) for src in
           ("api.cu", "adjoint.cu", "wavefront.cu", "photon.cu", "render.cu", "readback.cu", "env.cu",
-           "env_noalloc.cu", "bvh_build.cpp")]
+           "env_noalloc.cu", "bvh_build.cpp", "comm.cpp")]
 REFERENCE_DIR = Path(os.environ.get("MRT_REFERENCE_DIR", "/root/reference"))
 
 
@@ -71,7 +71,7 @@ def build_libmrt(verbose_ptxas: bool = False, jobs: int | None = None) -> Path:
     for o in stale:  # objects of units that no longer exist
         o.unlink()
     if todo or not out.exists():
-        _run([NVCC, *ARCH, "-shared", "-o", str(out), *objs, "-lpthread"])
+        _run([NVCC, *ARCH, "-shared", "-o", str(out), *objs, "-lpthread", "-ldl"])
     return out
 
 

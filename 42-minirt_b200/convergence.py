@@ -14,6 +14,8 @@ Both images are noisy, so E[(x - r)^2] = bias^2 + var_x + var_r per pixel.
                     of E[(x - mu)^2] when r is unbiased for mu);
   relmse_bias       relMSE of the expectations: minus var_x too (an unbiased
                     estimate of the squared bias term, may come out negative).
+Per-pixel z-scores (x - r) / sqrt(var_x + var_r + floor^2), floor =
+Z_FLOOR_REL |r| + Z_FLOOR_ABS (rounding, for pixels without noise).
 The image-mean bias test compares the two image means per channel against
 their standard error, taken from the spread of the batch image means (pixels
 of one reference batch share their sample offsets, so per-pixel variances
@@ -27,6 +29,13 @@ from pathlib import Path
 import numpy as np
 
 EPS = 1e-2
+# Per-pixel z-scores get a precision floor in their denominator: a pixel can
+# have (near) zero variance on both sides (every sample sees the same sky
+# texel or nothing), where the FP32 kernel and the FP64 reference still differ
+# by rounding. 1e-4 relative (about 1,700 FP32 ulps) plus 1e-6 absolute is far
+# below any shading difference a shifted or blurred image would show.
+Z_FLOOR_REL = 1e-4
+Z_FLOOR_ABS = 1e-6
 
 
 def load_fixture(path: str | Path) -> dict:
@@ -82,7 +91,8 @@ def compare(x: np.ndarray, var_x: np.ndarray, batch_means_x: np.ndarray, ref: di
     out["image_mean_ours"] = bx.mean(0).tolist()
     out["image_mean_ref"] = br.mean(0).tolist()
     out["image_mean_z"] = (diff / np.maximum(se, 1e-30)).tolist()
-    z = (x - r) / np.sqrt(np.maximum(var_x + var_r, 1e-30))
+    floor = Z_FLOOR_REL * np.abs(r) + Z_FLOOR_ABS
+    z = (x - r) / np.sqrt(var_x + var_r + floor ** 2)
     out["pixel_z_rms"] = float(np.sqrt(np.mean(z ** 2)))
     out["pixel_z_gt5"] = float(np.mean(np.abs(z) > 5))
     return out

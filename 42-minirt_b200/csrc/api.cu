@@ -21,6 +21,7 @@
 
 #include "../../include/mrt.h"
 #include "bvh_build.h"
+#include "comm.h"
 #include "kernels.h"
 
 using namespace mrt;
@@ -168,6 +169,10 @@ struct mrt_ctx {
   int bvh_depth = 0;
   int auto_form = MRT_FORM_MEGAKERNEL;   // choice of the autotuner for this scene
   int auto_block = 0, auto_capacity = 0, auto_sort = 0;
+  // multi-GPU sample sharding (mrt_comm_init)
+  void* comm = nullptr;
+  int comm_rank = 0, comm_world = 1;
+  DevBuf<long long> comm_count;          // sample count reduced with the frame
 };
 
 namespace {
@@ -382,6 +387,8 @@ void mrt_destroy(mrt_ctx* c) {
   c->mat_tex.release(); c->texs.release(); c->texels.release(); c->rgb_dev.release();
   if (c->rgb_host) cudaFreeHost(c->rgb_host);
   wf_destroy(c->wf);
+  nccl_comm_destroy(c->comm);
+  c->comm_count.release();
   if (c->diff) { c->diff->release(); delete c->diff; }
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
@@ -1774,4 +1781,69 @@ extern "C" int mrt_backward(mrt_ctx* c, const float* theta, const mrt_render_par
   CK(launch_diff_sky_mean(A, c->stream));
   if (n) CK(cudaMemcpyAsync(grad_theta, D.grad.p, sizeof(float) * n, cudaMemcpyDefault, c->stream));
   return diff_finish(c, stats, A.n_paths, launches + (A.n_texels ? 1 : 0));
+}
+
+// ------------------------------------------------------------ multi-GPU
+
+extern "C" int mrt_comm_unique_id(unsigned char* id) {
+  if (!id) return set_err(MRT_ERR_INVALID, "null id buffer");
+  const char* err = nullptr;
+  if (!nccl_unique_id(id, &err)) return set_err(MRT_ERR_CUDA, "ncclGetUniqueId: %s", err);
+  return MRT_OK;
+}
+
+extern "C" int mrt_comm_init(mrt_ctx* c, const unsigned char* id, int32_t rank, int32_t world) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!id || world < 1 || rank < 0 || rank >= world)
+    return set_err(MRT_ERR_INVALID, "mrt_comm_init: rank %d of world %d", rank, world);
+  if (c->comm) return set_err(MRT_ERR_INVALID, "mrt_comm_init: the context already has a communicator");
+  if (c->comm_count.n != 1) CK(c->comm_count.alloc(1));
+  const char* err = nullptr;
+  void* comm = nullptr;
+  if (!nccl_comm_init(&comm, id, rank, world, &err)) return set_err(MRT_ERR_CUDA, "ncclCommInitRank: %s", err);
+  c->comm = comm;
+  c->comm_rank = rank;
+  c->comm_world = world;
+  return MRT_OK;
+}
+
+extern "C" int mrt_reduce_frame(mrt_ctx* c, int32_t root) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!c->comm) return set_err(MRT_ERR_INVALID, "mrt_reduce_frame: no communicator (mrt_comm_init)");
+  if (root < 0 || root >= c->comm_world) return set_err(MRT_ERR_INVALID, "mrt_reduce_frame: root %d", root);
+  const long long mine = c->accum_spp;
+  CK(cudaMemcpyAsync(c->comm_count.p, &mine, sizeof(long long), cudaMemcpyHostToDevice, c->stream));
+  const char* err = nullptr;
+  if (!nccl_reduce_frame(c->comm, reinterpret_cast<float*>(c->accum.p), c->accum.n * 4, c->comm_count.p, root,
+                         c->stream, &err))
+    return set_err(MRT_ERR_CUDA, "mrt_reduce_frame: %s", err);
+  long long total = 0;
+  CK(cudaMemcpyAsync(&total, c->comm_count.p, sizeof(long long), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (c->comm_rank == root) c->accum_spp = (int)total;
+  return MRT_OK;
+}
+
+extern "C" int mrt_comm_destroy(mrt_ctx* c) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (c->stream) CK(cudaStreamSynchronize(c->stream));
+  nccl_comm_destroy(c->comm);
+  c->comm = nullptr;
+  c->comm_rank = 0;
+  c->comm_world = 1;
+  return MRT_OK;
+}
+
+extern "C" void mrt_shard_samples(int64_t total, int32_t world, int32_t rank, int64_t* first, int64_t* count) {
+  if (world < 1 || rank < 0 || rank >= world || total < 0) {
+    if (first) *first = 0;
+    if (count) *count = 0;
+    return;
+  }
+  const int64_t base = total / world, extra = total % world;
+  if (first) *first = rank * base + std::min<int64_t>(rank, extra);
+  if (count) *count = base + (rank < extra ? 1 : 0);
 }

@@ -6,8 +6,10 @@
 // closest_t = 1000 start, hit_register.c:21), then every infinite plane is
 // tested and replaces the BVH hit only with a strictly smaller t
 // (hit_plane.c:43-71, t in [0.001, 1000]). The tree is walked near child
-// first with boxes culled beyond the best t; the stack lives in registers /
-// local memory (64 entries; the builder keeps the depth below that).
+// first with boxes culled beyond the best t; the stack (64 entries; the
+// builder keeps the depth below that) is a per-thread array in the
+// megakernels and a shared-memory short stack in the wavefront's traversal
+// kernels (LocalStack, SharedStack below).
 #pragma once
 #include "device_common.cuh"
 #include "quadric.cuh"
@@ -123,6 +125,33 @@ __device__ __forceinline__ bool prim_hit(const V& S, int i, float3 o, float3 d, 
   return true;
 }
 
+// Traversal stacks. LocalStack: a per-thread array (registers / local
+// memory), used by the megakernels. SharedStack: the first kShared entries of
+// each thread's stack in a [kShared][kThreads] shared-memory array (column =
+// thread, so a warp's pushes at equal depth fall in 32 different banks);
+// deeper entries spill to a per-thread local array. The wavefront's
+// traversal kernels use it, so the common pushes and pops stay out of L1,
+// which then holds more nodes and triangles.
+struct LocalStack {
+  int s[kStackSize];
+  __device__ __forceinline__ void put(int i, int v) { s[i] = v; }
+  __device__ __forceinline__ int get(int i) const { return s[i]; }
+};
+
+template <int kShared, int kThreads>
+struct SharedStack {
+  int* col;
+  int spill[kStackSize - kShared];
+  __device__ __forceinline__ explicit SharedStack(int* smem) : col(smem + threadIdx.x) {}
+  __device__ __forceinline__ void put(int i, int v) {
+    if (i < kShared) col[i * kThreads] = v;
+    else spill[i - kShared] = v;
+  }
+  __device__ __forceinline__ int get(int i) const {
+    return i < kShared ? col[i * kThreads] : spill[i - kShared];
+  }
+};
+
 // Closest hit. `visits` counts node fetches (heat-map / roofline counter).
 // Returns false on a miss. `status` receives ST_BUDGET if the bounded loop
 // ran out (a corrupted tree), never hangs.
@@ -132,16 +161,16 @@ __device__ __forceinline__ bool prim_hit(const V& S, int i, float3 o, float3 d, 
 // megakernels all use this loop: on B200 it measured 5 % faster in the
 // wavefront (c1) than the while-while loop with speculative leaf
 // postponement (Aila & Laine, HPG 2009) that the wavefront used first.
-template <bool kCount, class V>
+template <bool kCount, class V, class Stack>
 __device__ __forceinline__ bool closest_hit_compact(const V& S, float3 o, float3 d, HitInfo& hit,
-                                            int& visits, int* status, uint64_t akey = 0) {
+                                                    int& visits, int* status, Stack& stack,
+                                                    uint64_t akey = 0) {
   float tbest = kTMax;
   int best = kMiss;
   float bu = 0.f, bv = 0.f;
   if (S.has_bvh) {
     float3 inv = f3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
     float3 oi = o * inv;
-    int stack[kStackSize];
     int sp = 0;
     int cur = 0;
     int budget = 4 * S.n_nodes + 4 * S.n_prims + 64;
@@ -161,7 +190,7 @@ __device__ __forceinline__ bool closest_hit_compact(const V& S, float3 o, float3
         if (hl && hr) {
           int nearc = tl <= tr ? ln.x : ln.y;
           int farc = tl <= tr ? ln.y : ln.x;
-          if (sp < kStackSize) stack[sp++] = farc;
+          if (sp < kStackSize) stack.put(sp++, farc);
           else if (status) atomicOr(status, ST_STACK);
           cur = nearc;
           continue;
@@ -177,7 +206,7 @@ __device__ __forceinline__ bool closest_hit_compact(const V& S, float3 o, float3
         }
       }
       if (sp == 0) break;
-      cur = stack[--sp];
+      cur = stack.get(--sp);
     }
   }
   for (int i = 0; i < S.n_planes; ++i) {
@@ -195,9 +224,9 @@ __device__ __forceinline__ bool closest_hit_compact(const V& S, float3 o, float3
 }
 
 // Any hit, compact loop.
-template <class V>
+template <class V, class Stack>
 __device__ __forceinline__ bool any_hit_compact(const V& S, float3 o, float3 d, float tmax,
-                                        int* status, uint64_t akey = 0) {
+                                                int* status, Stack& stack, uint64_t akey = 0) {
   for (int i = 0; i < S.n_planes; ++i) {
     float t;
     if (plane_hit(S.planes[i], o, d, t) && t < tmax) return true;
@@ -205,7 +234,6 @@ __device__ __forceinline__ bool any_hit_compact(const V& S, float3 o, float3 d, 
   if (!S.has_bvh) return false;
   float3 inv = f3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
   float3 oi = o * inv;
-  int stack[kStackSize];
   int sp = 0;
   int cur = 0;
   int budget = 4 * S.n_nodes + 4 * S.n_prims + 64;
@@ -223,7 +251,7 @@ __device__ __forceinline__ bool any_hit_compact(const V& S, float3 o, float3 d, 
       float tr = box_hit(rxy.x, rxy.y, rxy.z, rxy.w, z.z, z.w, oi, inv, tlim);
       bool hl = tl < INFINITY, hr = tr < INFINITY;
       if (hl && hr) {
-        if (sp < kStackSize) stack[sp++] = ln.y;
+        if (sp < kStackSize) stack.put(sp++, ln.y);
         else if (status) atomicOr(status, ST_STACK);
         cur = ln.x;
         continue;
@@ -239,7 +267,7 @@ __device__ __forceinline__ bool any_hit_compact(const V& S, float3 o, float3 d, 
       }
     }
     if (sp == 0) return false;
-    cur = stack[--sp];
+    cur = stack.get(--sp);
   }
 }
 
@@ -248,13 +276,15 @@ __device__ __forceinline__ bool any_hit_compact(const V& S, float3 o, float3 d, 
 template <bool kCount, class V>
 __device__ __forceinline__ bool closest_hit(const V& S, float3 o, float3 d, HitInfo& hit,
                                             int& visits, int* status, uint64_t akey = 0) {
-  return closest_hit_compact<kCount>(S, o, d, hit, visits, status, akey);
+  LocalStack stack;
+  return closest_hit_compact<kCount>(S, o, d, hit, visits, status, stack, akey);
 }
 
 template <class V>
 __device__ __forceinline__ bool any_hit(const V& S, float3 o, float3 d, float tmax, int* status,
                                         uint64_t akey = 0) {
-  return any_hit_compact(S, o, d, tmax, status, akey);
+  LocalStack stack;
+  return any_hit_compact(S, o, d, tmax, status, stack, akey);
 }
 
 }  // namespace mrt

@@ -35,6 +35,41 @@ namespace mrt {
 constexpr int kKinds = 4;   // 0 diffuse/default, 1 metal, 2 dielectric, 3 mixed metallic
 constexpr int kWfBlock = 128;
 
+#ifndef MRT_WF_SMEM_STACK
+#define MRT_WF_SMEM_STACK 24
+#endif
+#ifndef MRT_WF_MINB
+#define MRT_WF_MINB 1
+#endif
+// traversal stack of the extend / connect kernels: the first kTravShared
+// entries in shared memory, the rest in local memory
+constexpr int kTravShared = MRT_WF_SMEM_STACK;
+#if MRT_WF_SMEM_STACK > 0
+#define MRT_TRAV_STACK(name) \
+  __shared__ int name##_smem[kTravShared * kWfBlock]; \
+  SharedStack<kTravShared, kWfBlock> name(name##_smem)
+#else
+#define MRT_TRAV_STACK(name) LocalStack name
+#endif
+#ifndef MRT_WF_SORT
+#define MRT_WF_SORT 1
+#endif
+#ifndef MRT_WF_SORT_SH
+#define MRT_WF_SORT_SH 1
+#endif
+#ifndef MRT_WF_SORT_BITS
+#define MRT_WF_SORT_BITS 5
+#endif
+#ifndef MRT_WF_SORT_ORDER
+#define MRT_WF_SORT_ORDER 0
+#endif
+// Ray reordering before the traversal kernels: a counting sort of the queue
+// on a key of the ray's origin cell (Morton order of a 2^kSortBits-per-axis
+// grid over the scene's bounds) and its direction octant.
+constexpr int kSortBits = MRT_WF_SORT_BITS;
+constexpr int kSortBins = 8 << (3 * kSortBits);
+constexpr int kScanThreads = 1024;
+
 struct WfState {
   // path state, indexed by path slot
   float4* o;          // origin.xyz, pixel (int bits)
@@ -58,19 +93,33 @@ struct WfState {
   float4* sh_d;       // shadow ray dir.xyz, (path << 4 | slot) bits
   int* counters;      // see Cnt
   float4* frame;      // accumulator (W*H)
+  // ray reordering
+  int* q_tmp;         // unsorted copy of the queue being sorted
+  int2* sort_kr;      // per queue entry: (key, rank within its key)
+  unsigned* sort_hist;  // kSortBins counters, then exclusive offsets
+  float4* sh_o2;      // shadow rays in key order
+  float4* sh_d2;
   int capacity;
   int sh_capacity;
   int rays_per_path;  // shadow rays a diffuse event may emit
   int vis_words;      // ceil(n_lights / 4)
+  int slot_bits;      // light-index bits of a shadow ray's tag
 };
 
-// A shadow ray's tag (the int bits of sh_d.w): the path slot above kSlotBits
-// bits of light index; slot kEnvSlot is the HDRI sample. Path slots stay below
-// 2^(31 - kSlotBits) = kMaxWfCapacity.
-constexpr int kSlotBits = 10;
-constexpr int kEnvSlot = (1 << kSlotBits) - 1;
-constexpr int kMaxWfLights = kEnvSlot;
-constexpr int kMaxWfCapacity = 1 << (31 - kSlotBits);
+// A shadow ray's tag (the int bits of sh_d.w): the path slot above
+// WfState::slot_bits bits of light index, the all-ones slot being the HDRI
+// sample. slot_bits is the fewest bits that hold the scene's light indices
+// and that slot (1 with no lights, 10 for the maximum of 1023 lights), so
+// path slots stay below 2^(31 - slot_bits): 2^30 for a scene lit by its sky
+// alone, 2^21 at the light maximum.
+constexpr int kMaxSlotBits = 10;
+constexpr int kMaxWfLights = (1 << kMaxSlotBits) - 1;
+
+__host__ __device__ inline int slot_bits_for(int n_lights) {
+  int b = 1;
+  while ((1 << b) < n_lights + 1) ++b;
+  return b;
+}
 
 enum Cnt : int {
   C_LIVE0 = 0, C_LIVE1 = 1, C_KIND = 2,          // C_KIND..C_KIND+3
@@ -96,6 +145,120 @@ __device__ __forceinline__ int warp_append(int* counter, bool pred) {
   if (lane == leader) base = atomicAdd(counter, __popc(mask));
   base = __shfl_sync(mask, base, leader);
   return base + __popc(mask & ((1u << lane) - 1u));
+}
+
+// ------------------------------------------------------------ reorder
+__device__ __forceinline__ uint32_t spread3(uint32_t x) {
+  // bits b of x to bit 3b (x < 2^10)
+  x &= 0x3ffu;
+  x = (x | (x << 16)) & 0x030000ffu;
+  x = (x | (x << 8)) & 0x0300f00fu;
+  x = (x | (x << 4)) & 0x030c30c3u;
+  x = (x | (x << 2)) & 0x09249249u;
+  return x;
+}
+
+// Sort key of a ray: origin cell in Morton order and direction octant.
+__device__ __forceinline__ uint32_t ray_key(const float3& lo, const float3& scale, float3 o, float3 d) {
+  const float m = (float)((1 << kSortBits) - 1);
+  const uint32_t cx = (uint32_t)fminf(fmaxf((o.x - lo.x) * scale.x, 0.f), m);
+  const uint32_t cy = (uint32_t)fminf(fmaxf((o.y - lo.y) * scale.y, 0.f), m);
+  const uint32_t cz = (uint32_t)fminf(fmaxf((o.z - lo.z) * scale.z, 0.f), m);
+  const uint32_t cell = spread3(cx) | (spread3(cy) << 1) | (spread3(cz) << 2);
+  const uint32_t oct = (d.x < 0.f ? 1u : 0u) | (d.y < 0.f ? 2u : 0u) | (d.z < 0.f ? 4u : 0u);
+  return MRT_WF_SORT_ORDER == 0 ? (oct << (3 * kSortBits)) | cell : (cell << 3) | oct;
+}
+
+// Scene bounds from the root node's two child boxes.
+__device__ __forceinline__ void scene_box(const SceneView& S, float3& lo, float3& scale) {
+  const Node r = S.nodes[0];
+  lo = f3(fminf(r.lxy.x, r.rxy.x), fminf(r.lxy.z, r.rxy.z), fminf(r.z.x, r.z.z));
+  const float3 hi = f3(fmaxf(r.lxy.y, r.rxy.y), fmaxf(r.lxy.w, r.rxy.w), fmaxf(r.z.y, r.z.w));
+  const float cells = (float)(1 << kSortBits);
+  scale = f3(cells / fmaxf(hi.x - lo.x, 1e-20f), cells / fmaxf(hi.y - lo.y, 1e-20f),
+             cells / fmaxf(hi.z - lo.z, 1e-20f));
+}
+
+// Keys and ranks of the live queue (a copy of which goes to q_tmp).
+template <int kBounceParity>
+__global__ void __launch_bounds__(kWfBlock) wf_sort_key(SceneView S, WfState W) {
+  const int n = W.counters[kBounceParity ? C_LIVE1 : C_LIVE0];
+  const int* q = W.q_live[kBounceParity];
+  float3 lo, scale;
+  scene_box(S, lo, scale);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const int i = q[k];
+    const float4 o = W.o[i], d = W.d[i];
+    const uint32_t key = ray_key(lo, scale, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z));
+    const int rank = (int)atomicAdd(W.sort_hist + key, 1u);
+    W.sort_kr[k] = make_int2((int)key, rank);
+    W.q_tmp[k] = i;
+  }
+}
+
+// Keys and ranks of the shadow-ray queue.
+__global__ void __launch_bounds__(kWfBlock) wf_sort_key_sh(SceneView S, WfState W) {
+  const int n = min(W.counters[C_SH], W.sh_capacity);
+  float3 lo, scale;
+  scene_box(S, lo, scale);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const float4 o = W.sh_o[k], d = W.sh_d[k];
+    const uint32_t key = ray_key(lo, scale, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z));
+    const int rank = (int)atomicAdd(W.sort_hist + key, 1u);
+    W.sort_kr[k] = make_int2((int)key, rank);
+  }
+}
+
+// Exclusive scan of the kSortBins counters, in place (one block).
+__global__ void __launch_bounds__(kScanThreads) wf_sort_scan(WfState W) {
+  constexpr int kChunk = kSortBins / kScanThreads;
+  __shared__ unsigned warp_sums[kScanThreads / 32];
+  unsigned* h = W.sort_hist + (size_t)threadIdx.x * kChunk;
+  unsigned sum = 0;
+  for (int j = 0; j < kChunk; ++j) sum += h[j];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned incl = sum;
+  for (int off = 1; off < 32; off <<= 1) {
+    const unsigned v = __shfl_up_sync(0xffffffffu, incl, off);
+    if (lane >= off) incl += v;
+  }
+  if (lane == 31) warp_sums[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    unsigned w = warp_sums[lane];
+    for (int off = 1; off < 32; off <<= 1) {
+      const unsigned v = __shfl_up_sync(0xffffffffu, w, off);
+      if (lane >= off) w += v;
+    }
+    warp_sums[lane] = w;
+  }
+  __syncthreads();
+  unsigned run = incl - sum + (warp ? warp_sums[warp - 1] : 0u);
+  for (int j = 0; j < kChunk; ++j) {
+    const unsigned c = h[j];
+    h[j] = run;
+    run += c;
+  }
+}
+
+template <int kBounceParity>
+__global__ void __launch_bounds__(kWfBlock) wf_sort_scatter(WfState W) {
+  const int n = W.counters[kBounceParity ? C_LIVE1 : C_LIVE0];
+  int* q = W.q_live[kBounceParity];
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const int2 kr = W.sort_kr[k];
+    q[W.sort_hist[kr.x] + kr.y] = W.q_tmp[k];
+  }
+}
+
+__global__ void __launch_bounds__(kWfBlock) wf_sort_scatter_sh(WfState W) {
+  const int n = min(W.counters[C_SH], W.sh_capacity);
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const int2 kr = W.sort_kr[k];
+    const unsigned dst = W.sort_hist[kr.x] + kr.y;
+    W.sh_o2[dst] = W.sh_o[k];
+    W.sh_d2[dst] = W.sh_d[k];
+  }
 }
 
 // ------------------------------------------------------------ generate
@@ -137,10 +300,11 @@ __global__ void __launch_bounds__(kWfBlock) wf_generate(SceneView S, WfState W, 
 
 // --------------------------------------------------------------- extend
 template <int kBounceParity, class V>
-__global__ void __launch_bounds__(kWfBlock) wf_extend(V S, WfState W, int* status) {
+__global__ void __launch_bounds__(kWfBlock, MRT_WF_MINB) wf_extend(V S, WfState W, int* status) {
   const int n = W.counters[kBounceParity ? C_LIVE1 : C_LIVE0];
   const int* q = W.q_live[kBounceParity];
   const int lane = threadIdx.x & 31;
+  MRT_TRAV_STACK(stack);
   while (true) {
     int base = 0;
     if (lane == 0) base = atomicAdd(&W.counters[C_WORK], 32);
@@ -152,7 +316,7 @@ __global__ void __launch_bounds__(kWfBlock) wf_extend(V S, WfState W, int* statu
       const float4 o = W.o[i], d = W.d[i];
       HitInfo h;
       int visits = 0;
-      bool hit = closest_hit_compact<false>(S, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), h, visits, status);
+      bool hit = closest_hit_compact<false>(S, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), h, visits, status, stack);
       W.hit[i] = make_float4(h.t, h.u, h.v, __int_as_float(hit ? h.prim : kMiss));
     }
   }
@@ -221,7 +385,7 @@ __device__ __forceinline__ void emit_shadow(const WfState& W, int path, int slot
     return;
   }
   W.sh_o[s] = make_float4(o.x, o.y, o.z, tmax);
-  W.sh_d[s] = make_float4(d.x, d.y, d.z, __int_as_float((path << kSlotBits) | slot));
+  W.sh_d[s] = make_float4(d.x, d.y, d.z, __int_as_float((path << W.slot_bits) | slot));
 }
 
 template <int kBounceParity, class V>
@@ -321,7 +485,7 @@ __global__ void __launch_bounds__(kWfBlock) wf_sample(V S, WfState W, const WfPa
           const float4 r = __ldg(S.env_rec1 + kk);
           env_rad = f3(r.x, r.y, r.z);
           if (s.mat >= 0) env_rad = env_rad * S.mats[s.mat].ao;
-          emit_shadow(W, i, kEnvSlot, s.p, dir, INFINITY, status);
+          emit_shadow(W, i, (1 << W.slot_bits) - 1, s.p, dir, INFINITY, status);
         }
         ps.d = cos_hemisphere(ps.rng, s.n);
         W.sp[i] = make_float4(s.p.x, s.p.y, s.p.z, __int_as_float(s.mat));
@@ -350,10 +514,11 @@ __global__ void __launch_bounds__(kWfBlock) wf_sample(V S, WfState W, const WfPa
 }
 
 // -------------------------------------------------------------- connect
-template <class V>
-__global__ void __launch_bounds__(kWfBlock) wf_connect(V S, WfState W, int* status) {
+template <bool kSortedShadow, class V>
+__global__ void __launch_bounds__(kWfBlock, MRT_WF_MINB) wf_connect(V S, WfState W, int* status) {
   const int n = min(W.counters[C_SH], W.sh_capacity);
   const int lane = threadIdx.x & 31;
+  MRT_TRAV_STACK(stack);
   while (true) {
     int base = 0;
     if (lane == 0) base = atomicAdd(&W.counters[C_WORK], 32);
@@ -361,12 +526,14 @@ __global__ void __launch_bounds__(kWfBlock) wf_connect(V S, WfState W, int* stat
     if (base >= n) break;
     const int k = base + lane;
     if (k < n) {
-      const float4 o = W.sh_o[k], d = W.sh_d[k];
-      const bool blocked = any_hit_compact(S, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), o.w, status);
+      const float4 o = kSortedShadow ? W.sh_o2[k] : W.sh_o[k];
+      const float4 d = kSortedShadow ? W.sh_d2[k] : W.sh_d[k];
+      const bool blocked = any_hit_compact(S, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), o.w, status, stack);
       if (!blocked) {
         const int tag = __float_as_int(d.w);
-        const int path = tag >> kSlotBits, slot = tag & kEnvSlot;
-        if (slot == kEnvSlot) W.vis_env[path] = 1u;
+        const int env_slot = (1 << W.slot_bits) - 1;
+        const int path = tag >> W.slot_bits, slot = tag & env_slot;
+        if (slot == env_slot) W.vis_env[path] = 1u;
         else atomicAdd(&W.vis[(size_t)(slot >> 2) * W.capacity + path], 1u << (8 * (slot & 3)));
       }
     }
@@ -504,6 +671,7 @@ struct WfHost {
   std::vector<void*> allocs;
   cudaGraphExec_t graph = nullptr;
   int graph_bounces = -1;
+  unsigned graph_launches = 0;   // kernels per replay of the graph
   uint64_t graph_key = 0;
 };
 
@@ -535,7 +703,9 @@ static cudaError_t wf_alloc(WfHost* H, int capacity, int n_lights, bool env) {
   AL(vis, n * 4 * vis_words); AL(vis_env, n * 4);
   AL(q_live[0], n * 4); AL(q_live[1], n * 4); AL(q_kind, n * 4 * kKinds); AL(q_def, n * 4);
   AL(counters, sizeof(int) * C_COUNT);
+  AL(q_tmp, n * 4); AL(sort_hist, sizeof(unsigned) * kSortBins);
   if ((e = A((void**)&H->dparams, sizeof(WfParams))) != cudaSuccess) return e;
+  if ((e = cudaMemset(s.sort_hist, 0, sizeof(unsigned) * kSortBins)) != cudaSuccess) return e;
 #undef AL
   return cudaMemset(s.counters, 0, sizeof(int) * C_COUNT);
 }
@@ -543,17 +713,69 @@ static cudaError_t wf_alloc(WfHost* H, int capacity, int n_lights, bool env) {
 static cudaError_t wf_shadow_alloc(WfHost* H, size_t sh_cap) {
   if ((size_t)H->sh_capacity >= sh_cap) return cudaSuccess;
   cudaError_t e;
-  float4 *o = nullptr, *d = nullptr;
+  float4 *o = nullptr, *d = nullptr, *o2 = nullptr, *d2 = nullptr;
+  int2* kr = nullptr;
+  const size_t kr_n = std::max(sh_cap, (size_t)H->capacity);
   if ((e = cudaMalloc(&o, sh_cap * 16)) != cudaSuccess) return e;
-  if ((e = cudaMalloc(&d, sh_cap * 16)) != cudaSuccess) { cudaFree(o); return e; }
   H->allocs.push_back(o);
+  if ((e = cudaMalloc(&d, sh_cap * 16)) != cudaSuccess) return e;
   H->allocs.push_back(d);
+  if ((e = cudaMalloc(&o2, sh_cap * 16)) != cudaSuccess) return e;
+  H->allocs.push_back(o2);
+  if ((e = cudaMalloc(&d2, sh_cap * 16)) != cudaSuccess) return e;
+  H->allocs.push_back(d2);
+  if ((e = cudaMalloc(&kr, kr_n * sizeof(int2))) != cudaSuccess) return e;
+  H->allocs.push_back(kr);
   H->st.sh_o = o;
   H->st.sh_d = d;
+  H->st.sh_o2 = o2;
+  H->st.sh_d2 = d2;
+  H->st.sort_kr = kr;
   H->st.sh_capacity = (int)sh_cap;
   H->sh_capacity = (int)sh_cap;
   if (H->graph) { cudaGraphExecDestroy(H->graph); H->graph = nullptr; }
   return cudaSuccess;
+}
+
+// One bounce of the wave: [reorder] extend, classify, sample, [reorder]
+// connect, finish, reset. Returns the number of kernels launched.
+template <int kPar, class VT>
+static unsigned wf_enqueue_bounce(const WfHost* H, const VT& v, const WfState& s, const WfParams* dP,
+                                  int* status, int bounce, cudaStream_t st) {
+  const int sms = H->sms;
+  const int gen_blocks = std::max(1, std::min((H->capacity + kWfBlock - 1) / kWfBlock, sms * 16));
+  const int sh_blocks = std::max(1, std::min((H->sh_capacity + kWfBlock - 1) / kWfBlock, sms * 16));
+  const int pers = sms * 12;
+  unsigned n = 0;
+  const size_t hist_bytes = sizeof(unsigned) * kSortBins;
+  const bool sort_live = MRT_WF_SORT && bounce > 0 && v.has_bvh;
+  if (sort_live) {
+    // counting sort of the live queue by ray key (the counters start at zero)
+    wf_sort_key<kPar><<<gen_blocks, kWfBlock, 0, st>>>(v, s);
+    wf_sort_scan<<<1, kScanThreads, 0, st>>>(s);
+    wf_sort_scatter<kPar><<<gen_blocks, kWfBlock, 0, st>>>(s);
+    cudaMemsetAsync(s.sort_hist, 0, hist_bytes, st);
+    n += 3;
+  }
+  wf_extend<kPar, VT><<<pers, kWfBlock, 0, st>>>(v, s, status);
+  wf_classify<kPar><<<gen_blocks, kWfBlock, 0, st>>>(v, s, dP);
+  wf_sample<kPar, VT><<<gen_blocks, kWfBlock, 0, st>>>(v, s, dP, status);
+  wf_work_reset<<<1, 32, 0, st>>>(s);
+  n += 4;
+  if (MRT_WF_SORT_SH && v.has_bvh) {
+    wf_sort_key_sh<<<sh_blocks, kWfBlock, 0, st>>>(v, s);
+    wf_sort_scan<<<1, kScanThreads, 0, st>>>(s);
+    wf_sort_scatter_sh<<<sh_blocks, kWfBlock, 0, st>>>(s);
+    cudaMemsetAsync(s.sort_hist, 0, hist_bytes, st);
+    wf_connect<true, VT><<<pers, kWfBlock, 0, st>>>(v, s, status);
+    n += 4;
+  } else {
+    wf_connect<false, VT><<<pers, kWfBlock, 0, st>>>(v, s, status);
+    n += 1;
+  }
+  wf_finish<kPar><<<gen_blocks, kWfBlock, 0, st>>>(v, s);
+  wf_reset<kPar><<<1, 32, 0, st>>>(s);
+  return n + 2;
 }
 
 // Enqueues one wave (generate + max_bounces x stages) on `st`; the
@@ -562,33 +784,14 @@ template <class VT>
 static void wf_enqueue_wave_t(WfHost* H, const VT& v, const WfParams& P, int* status,
                               cudaStream_t st, unsigned* launches) {
   const WfParams* dP = H->dparams;
-  const int sms = H->sms;
-  const int gen_blocks = std::max(1, std::min((H->capacity + kWfBlock - 1) / kWfBlock, sms * 16));
-  const int pers = sms * 12;
+  const int gen_blocks = std::max(1, std::min((H->capacity + kWfBlock - 1) / kWfBlock, H->sms * 16));
   WfState s = H->st;
   wf_wave_begin<<<1, 32, 0, st>>>(s);
   wf_generate<<<gen_blocks, kWfBlock, 0, st>>>(v, s, dP);
   unsigned n = 2;
-  for (int b = 0; b < P.max_bounces; ++b) {
-    if ((b & 1) == 0) {
-      wf_extend<0, VT><<<pers, kWfBlock, 0, st>>>(v, s, status);
-      wf_classify<0><<<gen_blocks, kWfBlock, 0, st>>>(v, s, dP);
-      wf_sample<0, VT><<<gen_blocks, kWfBlock, 0, st>>>(v, s, dP, status);
-      wf_work_reset<<<1, 32, 0, st>>>(s);
-      wf_connect<VT><<<pers, kWfBlock, 0, st>>>(v, s, status);
-      wf_finish<0><<<gen_blocks, kWfBlock, 0, st>>>(v, s);
-      wf_reset<0><<<1, 32, 0, st>>>(s);
-    } else {
-      wf_extend<1, VT><<<pers, kWfBlock, 0, st>>>(v, s, status);
-      wf_classify<1><<<gen_blocks, kWfBlock, 0, st>>>(v, s, dP);
-      wf_sample<1, VT><<<gen_blocks, kWfBlock, 0, st>>>(v, s, dP, status);
-      wf_work_reset<<<1, 32, 0, st>>>(s);
-      wf_connect<VT><<<pers, kWfBlock, 0, st>>>(v, s, status);
-      wf_finish<1><<<gen_blocks, kWfBlock, 0, st>>>(v, s);
-      wf_reset<1><<<1, 32, 0, st>>>(s);
-    }
-    n += 7;
-  }
+  for (int b = 0; b < P.max_bounces; ++b)
+    n += (b & 1) ? wf_enqueue_bounce<1>(H, v, s, dP, status, b, st)
+                 : wf_enqueue_bounce<0>(H, v, s, dP, status, b, st);
   // paths still live after the last bounce retire with what they gathered
   wf_wave_end<<<1, 32, 0, st>>>(s);
   n += 1;
@@ -626,7 +829,8 @@ int wf_render(WfHost* H, const SceneView& v, const LaunchParams& L, int spp, int
     return MRT_ERR_INVALID;
   }
   if (capacity <= 0) capacity = 1 << 22;
-  capacity = std::min(capacity, kMaxWfCapacity);
+  const int slot_bits = slot_bits_for(v.n_lights);
+  capacity = std::min(capacity, 1 << (31 - slot_bits));
   capacity = (int)std::min<uint64_t>((uint64_t)capacity, std::max<uint64_t>(total, 1024));
   cudaError_t e;
   if (H->capacity != capacity || H->vis_words != std::max(1, (v.n_lights + 3) / 4)) {
@@ -648,6 +852,7 @@ int wf_render(WfHost* H, const SceneView& v, const LaunchParams& L, int spp, int
     return MRT_ERR_OOM;
   }
   H->st.frame = frame;
+  H->st.slot_bits = slot_bits;
   WfParams P{};
   P.seed = L.seed;
   P.sample_base = L.sample_base;
@@ -677,8 +882,8 @@ int wf_render(WfHost* H, const SceneView& v, const LaunchParams& L, int spp, int
       if (H->graph) { cudaGraphExecDestroy(H->graph); H->graph = nullptr; }
       cudaGraph_t g;
       if ((e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) { *err = cudaGetErrorString(e); return MRT_ERR_CUDA; }
-      unsigned dummy = 0;
-      wf_enqueue_wave(H, v, P, status, st, &dummy);
+      unsigned count = 1;   // wf_retire_remaining below
+      wf_enqueue_wave(H, v, P, status, st, &count);
       // the paths alive after max_bounces retire (parity of the last bounce)
       const int par = P.max_bounces & 1;
       wf_retire_remaining<<<H->sms * 4, kWfBlock, 0, st>>>(H->st, par ? C_LIVE1 : C_LIVE0, par);
@@ -688,10 +893,11 @@ int wf_render(WfHost* H, const SceneView& v, const LaunchParams& L, int spp, int
       if (e != cudaSuccess) { *err = cudaGetErrorString(e); return MRT_ERR_CUDA; }
       H->graph_key = key;
       H->graph_bounces = P.max_bounces;
+      H->graph_launches = count;
     }
     for (uint64_t w = 0; w < waves; ++w) {
       if ((e = cudaGraphLaunch(H->graph, st)) != cudaSuccess) { *err = cudaGetErrorString(e); return MRT_ERR_CUDA; }
-      if (launches) *launches += 1 + 7 * P.max_bounces + 3;
+      if (launches) *launches += H->graph_launches;
     }
   } else {
     for (uint64_t w = 0; w < waves; ++w) {
@@ -708,8 +914,10 @@ int wf_render(WfHost* H, const SceneView& v, const LaunchParams& L, int spp, int
 WfHost* wf_create() { return new WfHost(); }
 
 size_t wf_device_bytes(const WfHost* H) {
-  return H ? (size_t)H->capacity * (16 * 10 + 8 + 4 * (4 + H->vis_words) + 4 * kKinds) + (size_t)H->sh_capacity * 32
-           : 0;
+  if (!H) return 0;
+  const size_t cap = (size_t)H->capacity, sh = (size_t)H->sh_capacity;
+  return cap * (16 * 10 + 8 + 4 * (4 + H->vis_words) + 4 * kKinds + 4) + sh * 64 + std::max(cap, sh) * 8 +
+         sizeof(unsigned) * kSortBins;
 }
 
 void wf_destroy(WfHost* H) {

@@ -197,6 +197,11 @@ SIGNATURES = {
     "mrt_read_depth": (C.c_int, [_P, _P]),
     "mrt_render_state_save": (C.c_int, [_P, C.c_char_p]),
     "mrt_render_state_load": (C.c_int, [_P, C.c_char_p]),
+    "mrt_comm_unique_id": (C.c_int, [_P]),
+    "mrt_comm_init": (C.c_int, [_P, _P, C.c_int32, C.c_int32]),
+    "mrt_reduce_frame": (C.c_int, [_P, C.c_int32]),
+    "mrt_comm_destroy": (C.c_int, [_P]),
+    "mrt_shard_samples": (None, [C.c_int64, C.c_int32, C.c_int32, _P, _P]),
     "mrt_trace_first_hit": (C.c_int, [_P, _P, C.c_int64, _P]),
     "mrt_trace_paths": (C.c_int, [_P, C.POINTER(RenderParams), _P, _P, C.c_int32, _P, _P]),
     "mrt_read_env_tables": (C.c_int, [_P, _P, _P, _P]),
@@ -233,6 +238,22 @@ def render_batch(ctxs: list, params: list[dict], block_size: int = 0) -> "Render
 
 
 _lib = None
+
+COMM_ID_BYTES = 128
+
+
+def comm_unique_id() -> bytes:
+    """A new NCCL communicator id (mrt_comm_unique_id), to be sent to every rank."""
+    buf = (C.c_ubyte * COMM_ID_BYTES)()
+    check(load().mrt_comm_unique_id(buf), "mrt_comm_unique_id")
+    return bytes(buf)
+
+
+def shard_samples(total: int, world: int, rank: int) -> tuple[int, int]:
+    """(first, count) of rank's contiguous sample shard (mrt_shard_samples)."""
+    first, count = C.c_int64(), C.c_int64()
+    load().mrt_shard_samples(total, world, rank, C.byref(first), C.byref(count))
+    return first.value, count.value
 
 
 def load(path: str | os.PathLike | None = None) -> C.CDLL:
@@ -352,6 +373,20 @@ class Context:
 
     def load_state(self, path) -> None:
         check(self.lib.mrt_render_state_load(self.h, str(path).encode()), "mrt_render_state_load")
+
+    # multi-GPU sample sharding (one process per GPU, NCCL)
+    def comm_init(self, comm_id: bytes, rank: int, world: int) -> None:
+        """Joins the communicator made by comm_unique_id() on one rank."""
+        assert len(comm_id) == COMM_ID_BYTES
+        buf = (C.c_ubyte * COMM_ID_BYTES).from_buffer_copy(comm_id)
+        check(self.lib.mrt_comm_init(self.h, buf, rank, world), "mrt_comm_init")
+
+    def reduce_frame(self, root: int = 0) -> None:
+        """Sums every rank's accumulator and sample count into root's."""
+        check(self.lib.mrt_reduce_frame(self.h, root), "mrt_reduce_frame")
+
+    def comm_destroy(self) -> None:
+        check(self.lib.mrt_comm_destroy(self.h), "mrt_comm_destroy")
 
     def read_depth(self) -> np.ndarray:
         out = np.zeros((self.height, self.width), np.int32)

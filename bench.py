@@ -35,7 +35,9 @@ samples per pixel (16 steps = the 256 spp render).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 Under torchrun each rank renders its own sample range (weak scaling); the
-frames are summed with one NCCL reduce at the end of the timed region.
+frames are summed on rank 0 by the library's mrt_reduce_frame (NCCL) inside
+the timed regions: once after the timed steps of each form, and after every
+step of the end-to-end run.
 """
 from __future__ import annotations
 
@@ -401,6 +403,12 @@ def main() -> int:
     t0 = time.perf_counter()
     ctx.build(sc)
     build_s = time.perf_counter() - t0
+    if dist:
+        # the library's own communicator (mrt_comm_init, NCCL): the frames of
+        # all ranks are summed on rank 0 by mrt_reduce_frame
+        cid = [mrt.comm_unique_id() if rank == 0 else None]
+        dist.broadcast_object_list(cid, src=0)
+        ctx.comm_init(cid[0], rank, world)
     npix = sc.width * sc.height
     spp = a.spp_per_step
     paths_per_step = npix * spp
@@ -442,6 +450,11 @@ def main() -> int:
             st = ctx.render(spp, seed=1, sample_base=base + s * spp, form=fid)
             ms += st.ms
             launches += st.kernel_launches
+        if dist:
+            # the frame of the job: one sum-reduce of the accumulators onto rank 0
+            t_r = time.perf_counter()
+            ctx.reduce_frame(0)
+            ms += 1000.0 * (time.perf_counter() - t_r)
         barrier()
         t_max = ms
         if dist:
@@ -471,7 +484,16 @@ def main() -> int:
     for s in range(a.steps):
         ctx.set_camera(cam, sc.ior_all, sc.ambient_ratio)
         ctx.render(spp, seed=2, sample_base=rank * a.steps * spp + s * spp, form=fid)
-        ctx.accumulate_double(host)
+        if dist:
+            # every step's frame summed on rank 0 (mrt_reduce_frame), read
+            # back there; the other ranks drop their consumed partial frame
+            ctx.reduce_frame(0)
+            if rank == 0:
+                ctx.accumulate_double(host)
+            else:
+                ctx.clear()
+        else:
+            ctx.accumulate_double(host)
     barrier()
     e2e_s = time.perf_counter() - t0
     if dist:
@@ -479,9 +501,6 @@ def main() -> int:
         t = torch.tensor([e2e_s], device=f"cuda:{local}")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-        # the frames of all ranks summed on rank 0 (one NCCL reduce)
-        frame = torch.from_numpy(host.astype(np.float32)).cuda(local)
-        D.reduce_frame(frame, dist)
     e2e = paths_per_step * a.steps * world / e2e_s / 1e6
 
     relmse = None
@@ -526,6 +545,8 @@ def main() -> int:
                                 "kind": "reference", "sample": cpu["sample"]}
     if rank == 0:
         print(json.dumps(line), flush=True)
+    if dist:
+        ctx.comm_destroy()
     ctx.close()
     if dist:
         dist.destroy_process_group()

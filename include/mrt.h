@@ -400,6 +400,34 @@ MRT_API int			mrt_read_depth(mrt_ctx *ctx, int32_t *depth);
 MRT_API int			mrt_render_state_save(mrt_ctx *ctx, const char *path);
 MRT_API int			mrt_render_state_load(mrt_ctx *ctx, const char *path);
 
+/* --------------------------------------------------- multi-GPU sharding
+ * Replaces the render farm (src/network/handle_client.c:67-75: clients
+ * render samples, the server adds their float_render buffers) with one
+ * process per GPU over NCCL (NVLink / NVSwitch). Every rank builds the same
+ * scene, renders its own contiguous sample range (mrt_shard_samples) with
+ * render params sample_base = first, spp = count and the same seed, then
+ * mrt_reduce_frame sums the accumulators: the root's frame equals a
+ * single-GPU render of all samples up to summation order. libnccl.so.2 is
+ * loaded on the first call; without it these calls return MRT_ERR_CUDA. */
+# define MRT_COMM_ID_BYTES 128
+/* A new communicator id (ncclGetUniqueId) on one rank; the caller sends its
+ * MRT_COMM_ID_BYTES bytes to the other ranks by its own means. */
+MRT_API int			mrt_comm_unique_id(unsigned char *id);
+/* Joins ctx to the communicator `id` as `rank` of `world` (collective: every
+ * rank calls it). One communicator per context, released by
+ * mrt_comm_destroy or mrt_destroy. */
+MRT_API int			mrt_comm_init(mrt_ctx *ctx, const unsigned char *id,
+				int32_t rank, int32_t world);
+/* Collective: sums every rank's device accumulator into root's (in place)
+ * and every rank's accumulated sample count into root's, on the context's
+ * stream; the other ranks' accumulators are left as they were. */
+MRT_API int			mrt_reduce_frame(mrt_ctx *ctx, int32_t root);
+MRT_API int			mrt_comm_destroy(mrt_ctx *ctx);
+/* Contiguous shard of `total` samples for `rank` of `world`, balanced to
+ * within one sample: [*first, *first + *count). */
+MRT_API void		mrt_shard_samples(int64_t total, int32_t world, int32_t rank,
+				int64_t *first, int64_t *count);
+
 /* ------------------------------------------------------------ autotuner */
 
 # define MRT_TUNE_MAX 32

@@ -2,7 +2,11 @@
 
 Buckets, per ray:
   exact     same primitive (flat id) and, when both hit, t within 1e-5
-            relative;
+            relative, or within the FP32 rounding of the ray origin carried
+            to the hit (origin_rounding below: rays leaving a surface
+            have a short t, and at grazing incidence the rounding of their
+            origin, ~6e-8 of its coordinates, moves the hit along the ray
+            by that over the cosine of the incidence angle);
   tie       different primitives whose hits are within 1e-4 relative in t
             and 1e-3 apart: two surfaces at the same depth (a shared mesh
             edge, coincident surfaces), where either answer is the closest
@@ -80,14 +84,27 @@ def near_boundary(scene, tri_pos, o, d, prim):
     return out
 
 
+def origin_rounding(o, d, normal):
+    """Bound on |t_fp32 - t_fp64| from rounding the ray origin to FP32:
+    4 ulps of the largest origin coordinate per axis, over |cos| between the
+    unit direction and the surface normal (floored at 1e-3)."""
+    ulp = 2.0 ** -23 * np.max(np.abs(o), axis=1)
+    dn = d / np.linalg.norm(d, axis=1, keepdims=True)
+    nn = normal / np.maximum(np.linalg.norm(normal, axis=1, keepdims=True), 1e-300)
+    cos = np.abs(np.einsum("ij,ij->i", dn, nn))
+    return 4.0 * np.sqrt(3.0) * ulp / np.maximum(cos, 1e-3) / np.linalg.norm(d, axis=1)
+
+
 def classify(scene, tri_pos, o, d, g, r):
     """Buckets of the GPU hits g against the oracle hits r (record arrays
     with prim, t, point)."""
     g_prim, r_prim = g["prim"].astype(np.int64), r["prim"].astype(np.int64)
     both = (g_prim >= 0) & (r_prim >= 0)
     same = g_prim == r_prim
-    t_rel = np.abs(g["t"] - r["t"]) / np.maximum(np.abs(r["t"]), 1e-6)
-    exact = same & ((~both) | (t_rel <= 1e-5))
+    dt = np.abs(g["t"] - r["t"])
+    t_rel = dt / np.maximum(np.abs(r["t"]), 1e-6)
+    t_ok = (t_rel <= 1e-5) | (dt <= origin_rounding(o, d, r["normal"]))
+    exact = same & ((~both) | t_ok)
     dist = np.linalg.norm(g["point"] - r["point"], axis=1)
     tie = (~same) & both & (t_rel <= 1e-4) & (dist <= 1e-3 * np.maximum(r["t"], 1.0))
     rest = ~(exact | tie)

@@ -12,10 +12,11 @@ the two are compared with the statistics of 42-minirt_b200/convergence.py:
     subtracted), i.e. no bias beyond the metric's bar;
   * relmse_converged <= 1e-3 where the GPU render has enough samples for its
     own noise to be below the bar (all configurations but c2, whose caustics
-    need ~15k samples per pixel);
+    need more than 16k samples per pixel);
   * image-mean bias test: |mean difference| <= 4 standard errors per channel,
     the standard error from the batch image means of both sides;
-  * per-pixel z-scores: at most 0.5 % of pixels beyond 5 standard errors.
+  * per-pixel z-scores: at most 0.5 % of pixels beyond 5 standard errors
+    (with a rounding floor for pixels without noise, convergence.Z_FLOOR_*).
 
 c2 is the reference's single-pass kNN mode (k = 15, 2 M photons). A kNN image
 depends on its photon set, so the GPU is given the reference's own photon
@@ -35,8 +36,12 @@ from conftest import GOLDEN
 
 pytestmark = pytest.mark.gpu
 
-# samples per pixel of the GPU render, in 16 batches
-GPU_SPP = {"c0": 16384, "c1": 4096, "c2": 4096, "c4": 16384}
+# samples per pixel of the GPU render, in 16 batches. c2 is heavy-tailed
+# (paths trapped between the floor and the underside of the glass slab by
+# total internal reflection reach dense caustic regions, where the kNN
+# estimate is large): 16,384 samples keep the GPU side's noise, and the
+# uncertainty of the subtracted variances, well below the bar.
+GPU_SPP = {"c0": 16384, "c1": 4096, "c2": 16384, "c4": 16384}
 BATCHES = 16
 
 

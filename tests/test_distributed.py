@@ -100,3 +100,14 @@ def test_two_rank_sample_sharding_reproduces_single_render():
         assert len(gp) == 2 + 3
         np.testing.assert_array_equal(gp[:2], 0.0)
         np.testing.assert_array_equal(gw[2:], 11.0)
+
+
+def test_c_abi_shard_samples_matches_host_helper(mrt):
+    """mrt_shard_samples (the C host's sharding arithmetic) equals
+    distributed.shard_samples; no device needed."""
+    import distributed as D
+    for total in (0, 1, 7, 64, 1000, 4096):
+        for world in (1, 2, 3, 8):
+            for r in range(world):
+                assert mrt.shard_samples(total, world, r) == D.shard_samples(total, world, r)
+    assert mrt.shard_samples(10, 2, 5) == (0, 0)
