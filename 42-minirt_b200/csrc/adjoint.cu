@@ -322,29 +322,41 @@ __device__ __forceinline__ void material_rec(const V& S, PathState& P, const Sur
   }
 }
 
+// Gradient sums are 64-bit fixed point (AdjointArgs::q_scale): each value is
+// rounded to an integer once, and integer additions give the same total in
+// any order, so the result does not depend on thread scheduling.
+__device__ __forceinline__ long long fx_q(float v, double scale) {
+  double x = (double)v * scale;
+  if (!(x == x)) x = 0.0;                      // NaN contributes nothing
+  x = fmin(fmax(x, -4.0e18), 4.0e18);
+  return __double2ll_rn(x);
+}
+
 // atomicAdd with the lanes of a warp that target the same address summed
 // first (one atomic per distinct address): HDRI NEE concentrates on the few
 // texels of a sun, and a warp's paths often share a material.
-__device__ __forceinline__ void agg_add(float* addr, float v) {
+__device__ __forceinline__ void agg_add_q(long long* addr, long long q) {
   const unsigned active = __activemask();
   const unsigned peers = __match_any_sync(active, (unsigned long long)addr);
   const int leader = __ffs(peers) - 1;
-  float sum = 0.f;
-  for (unsigned m = peers; m; m &= m - 1) sum += __shfl_sync(peers, v, __ffs(m) - 1);
-  if ((int)(threadIdx.x & 31) == leader && sum != 0.f) atomicAdd(addr, sum);
+  long long sum = 0;
+  for (unsigned m = peers; m; m &= m - 1) sum += __shfl_sync(peers, q, __ffs(m) - 1);
+  if ((int)(threadIdx.x & 31) == leader && sum != 0)
+    atomicAdd(reinterpret_cast<unsigned long long*>(addr), (unsigned long long)sum);
 }
 
 __device__ __forceinline__ void add_sky_grad(const AdjointArgs& A, int texel, int c, float v) {
-  agg_add(A.g_sky + 3 * (size_t)texel + c, v);
+  agg_add_q(A.q_sky + 3 * (size_t)texel + c, fx_q(v, A.q_scale));
 }
 
 // Shared-memory accumulators of the per-material gradients of one block.
 struct MatGrad {
-  float* s;     // [albedo M*3 | roughness M | emission M]
+  long long* s;   // [albedo M*3 | roughness M | emission M], fixed point
   int M;
-  __device__ __forceinline__ void albedo(int m, int c, float v) { agg_add(s + 3 * m + c, v); }
-  __device__ __forceinline__ void rough(int m, float v) { agg_add(s + 3 * M + m, v); }
-  __device__ __forceinline__ void emis(int m, float v) { agg_add(s + 4 * M + m, v); }
+  double scale;
+  __device__ __forceinline__ void albedo(int m, int c, float v) { agg_add_q(s + 3 * m + c, fx_q(v, scale)); }
+  __device__ __forceinline__ void rough(int m, float v) { agg_add_q(s + 3 * M + m, fx_q(v, scale)); }
+  __device__ __forceinline__ void emis(int m, float v) { agg_add_q(s + 4 * M + m, fx_q(v, scale)); }
 };
 
 // One reverse step: the adjoint state (Pb, ob, db) after bounce k becomes
@@ -567,9 +579,9 @@ __global__ void __launch_bounds__(kBlock) adj_replay_kernel(V S, AdjointArgs A, 
 template <int kBlock, class V>
 __global__ void __launch_bounds__(kBlock) adj_level_kernel(V S, AdjointArgs A, const TapeEntry* tape,
                                                            float4* state, int k) {
-  extern __shared__ float smem[];
-  MatGrad G{smem, A.n_mats};
-  for (int i = threadIdx.x; i < 5 * A.n_mats; i += kBlock) smem[i] = 0.f;
+  extern __shared__ long long smem_q[];
+  MatGrad G{smem_q, A.n_mats, A.q_scale};
+  for (int i = threadIdx.x; i < 5 * A.n_mats; i += kBlock) smem_q[i] = 0;
   __syncthreads();
   const float inv_col = A.col ? (float)(1.0 / *A.col) : 0.f;
   float gcol = 0.f;
@@ -587,11 +599,13 @@ __global__ void __launch_bounds__(kBlock) adj_level_kernel(V S, AdjointArgs A, c
       state[4 * idx + 3] = make_float4(db.x, db.y, db.z, 0.f);
     }
   }
-  for (int off = 16; off > 0; off >>= 1) gcol += __shfl_down_sync(0xffffffffu, gcol, off);
-  if ((threadIdx.x & 31) == 0 && gcol != 0.f) atomicAdd(A.g_col, gcol);
+  long long qcol = fx_q(gcol, A.q_scale);
+  for (int off = 16; off > 0; off >>= 1) qcol += __shfl_down_sync(0xffffffffu, qcol, off);
+  if ((threadIdx.x & 31) == 0 && qcol != 0)
+    atomicAdd(reinterpret_cast<unsigned long long*>(A.q_col), (unsigned long long)qcol);
   __syncthreads();
   for (int i = threadIdx.x; i < 5 * A.n_mats; i += kBlock)
-    if (smem[i] != 0.f) atomicAdd(A.g_mats + i, smem[i]);
+    if (smem_q[i] != 0) atomicAdd(reinterpret_cast<unsigned long long*>(A.q_mats + i), (unsigned long long)smem_q[i]);
 }
 
 // theta -> MaterialD array (colour, roughness, alpha4, emission strength
@@ -643,24 +657,37 @@ __global__ void diff_env_records_kernel(DiffEnvRecords E) {
   E.aux[k] = ax;
 }
 
-__global__ void diff_image_kernel(const float4* accum, float* img, int npix, float inv_spp) {
+__global__ void diff_image_kernel(const unsigned long long* q, float* img, int npix, double inv) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= npix) return;
-  const float4 a = accum[i];
-  img[3 * i] = a.x * inv_spp;
-  img[3 * i + 1] = a.y * inv_spp;
-  img[3 * i + 2] = a.z * inv_spp;
+  for (int c = 0; c < 3; ++c) img[3 * i + c] = (float)((double)(long long)q[3 * i + c] * inv);
 }
 
-// The dense part of the pdf_joint gradient: every texel's luminance enters
-// the column average that divides every pdf.
-__global__ void diff_sky_mean_kernel(float* g_sky, const float* g_col, int n_texels, float scale) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n_texels) return;
-  const float s = *g_col * scale;
-  g_sky[3 * i] += s * 0.2126f;
-  g_sky[3 * i + 1] += s * 0.7152f;
-  g_sky[3 * i + 2] += s * 0.0722f;
+__global__ void abs_max_kernel(const float* x, size_t n, float* out) {
+  float m = 0.f;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const float a = fabsf(x[i]);
+    if (a > m && a < INFINITY) m = a;
+  }
+  for (int off = 16; off > 0; off >>= 1) m = fmaxf(m, __shfl_down_sync(0xffffffffu, m, off));
+  // non-negative floats order like their bit patterns
+  if ((threadIdx.x & 31) == 0 && m > 0.f) atomicMax(reinterpret_cast<int*>(out), __float_as_int(m));
+}
+
+// Fixed-point sums to the float gradient, with the dense part of the
+// pdf_joint gradient: every texel's luminance enters the column average that
+// divides every pdf (d column_average / d texel channel c = 255 * lum[c] /
+// (W * H)).
+__global__ void diff_grad_out_kernel(AdjointArgs A, float* out_mats, float* out_sky, int64_t n_mats5,
+                                     float dense) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const double inv = 1.0 / A.q_scale;
+  if (i < n_mats5) out_mats[i] = (float)((double)A.q_mats[i] * inv);
+  if (i < A.n_texels) {
+    const float s = (float)((double)*A.q_col * inv) * dense;
+    const float lw[3] = {0.2126f, 0.7152f, 0.0722f};
+    for (int c = 0; c < 3; ++c) out_sky[3 * i + c] = (float)((double)A.q_sky[3 * i + c] * inv) + s * lw[c];
+  }
 }
 
 // Linear sky radiance of every texel as the renderer decodes it (RGBE,
@@ -697,8 +724,26 @@ cudaError_t launch_diff_env_records(const DiffEnvRecords& E, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_diff_image(const float4* accum, float* img, int npix, float inv_spp, cudaStream_t st) {
-  diff_image_kernel<<<(npix + 255) / 256, 256, 0, st>>>(accum, img, npix, inv_spp);
+cudaError_t launch_diff_image(const unsigned long long* accum_fx, float* img, int npix, int spp,
+                              cudaStream_t st) {
+  diff_image_kernel<<<(npix + 255) / 256, 256, 0, st>>>(accum_fx, img, npix,
+                                                       1.0 / (kFrameFxScale * (double)std::max(spp, 1)));
+  return cudaGetLastError();
+}
+
+cudaError_t launch_abs_max(const float* x, size_t n, float* out, cudaStream_t st) {
+  if (n == 0) return cudaSuccess;
+  const unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, 1184);
+  abs_max_kernel<<<blocks, 256, 0, st>>>(x, n, out);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_diff_grad_out(const AdjointArgs& A, float* out_mats, float* out_sky, int64_t n_mats5,
+                                 cudaStream_t st) {
+  const int64_t n = std::max<int64_t>(n_mats5, A.n_texels);
+  if (n == 0) return cudaSuccess;
+  const float dense = A.n_texels ? A.pdf_dgray / (float)A.n_texels : 0.f;
+  diff_grad_out_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(A, out_mats, out_sky, n_mats5, dense);
   return cudaGetLastError();
 }
 
@@ -722,7 +767,7 @@ cudaError_t launch_adjoint_chunk(const SceneView& S, const AdjointArgs& A, TapeE
     unsigned grid = (unsigned)std::min<uint64_t>((uint64_t)sms * std::max(occ, 1), want);
     adj_replay_kernel<kBlock, VT><<<grid, kBlock, 0, st>>>(v, A, tape, state, status, work);
     if ((e2 = cudaGetLastError()) != cudaSuccess) return e2;
-    const size_t smem = (size_t)5 * A.n_mats * sizeof(float);
+    const size_t smem = (size_t)5 * A.n_mats * sizeof(long long);
     e2 = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, adj_level_kernel<kBlock, VT>, kBlock, smem);
     if (e2 != cudaSuccess) return e2;
     grid = (unsigned)std::min<uint64_t>((uint64_t)sms * std::max(occ, 1), want);
@@ -733,14 +778,6 @@ cudaError_t launch_adjoint_chunk(const SceneView& S, const AdjointArgs& A, TapeE
     return cudaSuccess;
     }
   });
-}
-
-cudaError_t launch_diff_sky_mean(const AdjointArgs& A, cudaStream_t st) {
-  if (A.n_texels == 0) return cudaSuccess;
-  // d column_average / d sky texel channel c = 255 * lum_weight[c] / (W * H)
-  diff_sky_mean_kernel<<<(A.n_texels + 255) / 256, 256, 0, st>>>(A.g_sky, A.g_col, A.n_texels,
-                                                               A.pdf_dgray / (float)A.n_texels);
-  return cudaGetLastError();
 }
 
 }  // namespace mrt

@@ -111,14 +111,18 @@ struct DiffState {
   bool tables = false;                 // HDRI NEE tables are rebuilt from theta
   DevBuf<float> theta, grad, img, dimg;
   DevBuf<MaterialD> mats;
-  DevBuf<float4> accum, grid, rec0, rec1, state;
+  DevBuf<float4> grid, rec0, rec1, state;
   DevBuf<TapeEntry> tape;
   DevBuf<int2> aux;
   DevBuf<float> pdf, cm, cc;
   DevBuf<double> gray, raw, rowcdf, scal, cdfh;
+  DevBuf<unsigned long long> accum_fx;   // forward image, fixed point (3 per pixel)
+  DevBuf<long long> gq;                  // backward sums, fixed point (as grad)
+  DevBuf<float> wmax;                    // max |d loss / d image|
   void release() {
+    accum_fx.release(); gq.release(); wmax.release();
     theta.release(); grad.release(); img.release(); dimg.release(); mats.release();
-    accum.release(); grid.release(); rec0.release(); rec1.release(); aux.release();
+    grid.release(); rec0.release(); rec1.release(); aux.release();
     state.release(); tape.release();
     pdf.release(); cm.release(); cc.release();
     gray.release(); raw.release(); rowcdf.release(); scal.release(); cdfh.release();
@@ -1592,9 +1596,11 @@ int diff_prepare(mrt_ctx* c, const float* theta, SceneView& v) {
     D.tables = c->view.env_nee && W >= 2 && H >= 2;
     CK(D.theta.alloc(std::max<int64_t>(n, 1)));
     CK(D.grad.alloc(n + 1));   // + d loss / d column average
+    CK(D.gq.alloc(n + 1));
+    CK(D.wmax.alloc(1));
     CK(D.img.alloc(3 * npix));
     CK(D.dimg.alloc(3 * npix));
-    CK(D.accum.alloc(npix));
+    CK(D.accum_fx.alloc(3 * npix));
     CK(D.mats.alloc(std::max(M, 1)));
     if (D.tables) {
       const size_t t = (size_t)W * H, no = (size_t)(H - 1) * W;
@@ -1707,21 +1713,22 @@ extern "C" int mrt_forward(mrt_ctx* c, const float* theta, const mrt_render_para
   DiffState& D = *c->diff;
   const uint64_t npix = (uint64_t)c->W * c->H;
   CK(cudaMemsetAsync(c->status.p, 0, sizeof(int), c->stream));
-  CK(cudaMemsetAsync(D.accum.p, 0, D.accum.bytes(), c->stream));
+  CK(cudaMemsetAsync(D.accum_fx.p, 0, D.accum_fx.bytes(), c->stream));
   LaunchParams L{};
   L.seed = p->seed;
   L.max_bounces = p->max_bounces > 0 ? p->max_bounces : v.max_bounces;
   L.jitter = p->jitter;
+  L.accum_fx = D.accum_fx.p;        // order-independent sums: the same image on every run
   const int spp_chunk = (int)std::max<uint64_t>(1, (1ull << 26) / std::max<uint64_t>(npix, 1));
   int launches = 0;
   for (int s = 0; s < p->spp; s += spp_chunk) {
     const int k = std::min(spp_chunk, p->spp - s);
     L.sample_base = (uint32_t)(p->sample_base + s);
     L.n_paths = npix * (uint64_t)k;
-    CK(launch_megakernel_regen(v, L, D.accum.p, c->status.p, c->counters.p + 7, 0, 0, c->stream));
+    CK(launch_megakernel_regen(v, L, nullptr, c->status.p, c->counters.p + 7, 0, 0, c->stream));
     launches++;
   }
-  CK(launch_diff_image(D.accum.p, D.img.p, (int)npix, 1.0f / (float)p->spp, c->stream));
+  CK(launch_diff_image(D.accum_fx.p, D.img.p, (int)npix, p->spp, c->stream));
   CK(cudaMemcpyAsync(image, D.img.p, sizeof(float) * 3 * npix, cudaMemcpyDefault, c->stream));
   return diff_finish(c, stats, npix * (uint64_t)p->spp, launches + 1);
 }
@@ -1741,7 +1748,17 @@ extern "C" int mrt_backward(mrt_ctx* c, const float* theta, const mrt_render_par
   const uint64_t npix = (uint64_t)c->W * c->H;
   CK(cudaMemsetAsync(c->status.p, 0, sizeof(int), c->stream));
   CK(cudaMemcpyAsync(D.dimg.p, grad_image, sizeof(float) * 3 * npix, cudaMemcpyDefault, c->stream));
-  CK(cudaMemsetAsync(D.grad.p, 0, D.grad.bytes(), c->stream));
+  CK(cudaMemsetAsync(D.gq.p, 0, D.gq.bytes(), c->stream));
+  // fixed-point scale of the gradient sums: 2^36 / max |d loss / d image|
+  // (rounded to a power of two), so a single path's contribution, which is
+  // d loss / d image / spp times factors of order 1 to 1e3, keeps about 30
+  // significant bits, and sums stay below 2^63 up to 2^27 max |d loss / d image|
+  CK(cudaMemsetAsync(D.wmax.p, 0, sizeof(float), c->stream));
+  CK(launch_abs_max(D.dimg.p, 3 * npix, D.wmax.p, c->stream));
+  float wmax = 0.f;
+  CK(cudaMemcpyAsync(&wmax, D.wmax.p, sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  const int wexp = wmax > 0.f ? (int)std::ceil(std::log2((double)wmax)) : 0;
   AdjointArgs A{};
   A.n_paths = npix * (uint64_t)p->spp;
   A.seed = p->seed;
@@ -1755,9 +1772,10 @@ extern "C" int mrt_backward(mrt_ctx* c, const float* theta, const mrt_render_par
   A.col = D.tables ? D.scal.p : nullptr;
   A.dimg = D.dimg.p;
   A.env_aux = D.tables ? D.aux.p : nullptr;
-  A.g_mats = D.grad.p;
-  A.g_sky = D.grad.p + 5 * (size_t)D.M;
-  A.g_col = D.grad.p + n;
+  A.q_mats = D.gq.p;
+  A.q_sky = D.gq.p + 5 * (size_t)D.M;
+  A.q_col = D.gq.p + n;
+  A.q_scale = std::ldexp(1.0, std::max(-60, std::min(100, 36 - wexp)));
   // samples per chunk: the tape (80 B per bounce) stays within a budget of
   // device memory, at most 16 GiB or a quarter of what is free
   size_t free_b = 0, total_b = 0;
@@ -1778,9 +1796,9 @@ extern "C" int mrt_backward(mrt_ctx* c, const float* theta, const mrt_render_par
     CK(launch_adjoint_chunk(v, Ac, D.tape.p, D.state.p, c->counters.p + 7, c->status.p, c->stream));
     launches += 1 + A.max_bounces;
   }
-  CK(launch_diff_sky_mean(A, c->stream));
+  CK(launch_diff_grad_out(A, D.grad.p, D.grad.p + 5 * (size_t)D.M, 5 * (int64_t)D.M, c->stream));
   if (n) CK(cudaMemcpyAsync(grad_theta, D.grad.p, sizeof(float) * n, cudaMemcpyDefault, c->stream));
-  return diff_finish(c, stats, A.n_paths, launches + (A.n_texels ? 1 : 0));
+  return diff_finish(c, stats, A.n_paths, launches + 2);   // + abs max, fixed point -> float
 }
 
 // ------------------------------------------------------------ multi-GPU

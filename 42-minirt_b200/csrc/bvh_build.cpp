@@ -50,8 +50,15 @@ struct BNode {
 
 constexpr int kBins = 32;
 constexpr int kMedianDepth = 40;
+#ifndef MRT_SAH_ISECT
+#define MRT_SAH_ISECT 1.0f
+#endif
+#ifndef MRT_BUILD_LEAF_MAX
+#define MRT_BUILD_LEAF_MAX kLeafMax
+#endif
 constexpr float kTraversalCost = 1.0f;
-constexpr float kIsectCost = 1.0f;
+constexpr float kIsectCost = MRT_SAH_ISECT;
+constexpr int kBuildLeafMax = MRT_BUILD_LEAF_MAX;
 
 struct Builder {
   const std::vector<PrimBox>& prims;
@@ -87,7 +94,7 @@ struct Builder {
     if (ext[1] > ext[axis]) axis = 1;
     if (ext[2] > ext[axis]) axis = 2;
     if (depth >= kMedianDepth || ext[axis] <= 0.0f) {
-      if (n <= (uint32_t)kLeafMax && depth < kMedianDepth) return 0;
+      if (n <= (uint32_t)kBuildLeafMax && depth < kMedianDepth) return 0;
       uint32_t mid = b + n / 2;
       std::nth_element(order.begin() + b, order.begin() + mid, order.begin() + e,
                        [&](uint32_t x, uint32_t y) { return prims[x].c[axis] < prims[y].c[axis]; });
@@ -135,8 +142,8 @@ struct Builder {
     const float parent_area = std::max(box.area(), 1e-30f);
     const float split_cost = kTraversalCost + kIsectCost * best_cost / parent_area;
     const float leaf_cost = kIsectCost * n;
-    if (best_axis < 0 || (n <= (uint32_t)kLeafMax && leaf_cost <= split_cost)) {
-      if (n <= (uint32_t)kLeafMax) return 0;
+    if (best_axis < 0 || (n <= (uint32_t)kBuildLeafMax && leaf_cost <= split_cost)) {
+      if (n <= (uint32_t)kBuildLeafMax) return 0;
       uint32_t mid = b + n / 2;
       std::nth_element(order.begin() + b, order.begin() + mid, order.begin() + e,
                        [&](uint32_t x, uint32_t y) { return prims[x].c[axis] < prims[y].c[axis]; });

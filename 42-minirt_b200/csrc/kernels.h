@@ -16,7 +16,16 @@ struct LaunchParams {
   int render_mode;
   int has_offset;        // explicit shared offset (compute_frame / calc_one_sample)
   float ox, oy;
+  // when set (the differentiable forward), path radiance is added here as
+  // 64-bit fixed point (kFrameFxScale), 3 per pixel, instead of into the
+  // float4 accumulator: integer sums do not depend on the order in which
+  // paths finish, so the image is the same on every run
+  unsigned long long* accum_fx;
 };
+
+// Fixed-point scale of accum_fx: 2^32 per unit radiance (resolution
+// 2.3e-10; a pixel sum stays below 2^63 up to 2^31 units).
+constexpr double kFrameFxScale = 4294967296.0;
 
 // One scene of a multi-scene batch launch.
 struct BatchItem {
@@ -112,9 +121,13 @@ struct AdjointArgs {
   const double* col;       // column average of the grey values (device)
   const float* dimg;       // d loss / d image, W*H*3
   const int2* env_aux;
-  float* g_mats;           // [albedo M*3 | roughness M | emission M]
-  float* g_sky;            // W*H*3
-  float* g_col;            // one float
+  // gradient sums as 64-bit fixed point (value * q_scale): integer
+  // additions are associative, so the sums do not depend on the order in
+  // which threads add, and one seed gives one gradient
+  long long* q_mats;       // [albedo M*3 | roughness M | emission M]
+  long long* q_sky;        // W*H*3
+  long long* q_col;        // one value
+  double q_scale;          // 2^S with S chosen from max |d loss / d image|
 };
 
 // Tape of the backward: one entry per bounce, tape[k * n_paths + path].
@@ -129,7 +142,13 @@ struct __align__(16) TapeEntry {   // 80 B
 cudaError_t launch_diff_mats(const MaterialD* base, const float* theta, int M, MaterialD* out,
                              cudaStream_t st);
 cudaError_t launch_diff_env_records(const DiffEnvRecords& E, cudaStream_t st);
-cudaError_t launch_diff_image(const float4* accum, float* img, int npix, float inv_spp, cudaStream_t st);
+cudaError_t launch_diff_image(const unsigned long long* accum_fx, float* img, int npix, int spp,
+                              cudaStream_t st);
+// max |x| over n floats into *out (device), which must start at 0
+cudaError_t launch_abs_max(const float* x, size_t n, float* out, cudaStream_t st);
+// out[i] = q[i] / scale for i < n; then the dense pdf term of the sky
+cudaError_t launch_diff_grad_out(const AdjointArgs& A, float* out_mats, float* out_sky, int64_t n_mats5,
+                                 cudaStream_t st);
 cudaError_t launch_diff_sky_init(const SceneView& S, float* out, cudaStream_t st);
 // Backward of the paths [sample_base, sample_base + n_paths / W*H) of one
 // chunk: replay writing the tape (n_paths * max_bounces entries) and the
@@ -138,7 +157,6 @@ cudaError_t launch_diff_sky_init(const SceneView& S, float* out, cudaStream_t st
 cudaError_t launch_adjoint_chunk(const SceneView& S, const AdjointArgs& A, TapeEntry* tape, float4* state,
                                  unsigned long long* work, int* status, cudaStream_t st);
 // The dense term of the pdf gradient (after all chunks).
-cudaError_t launch_diff_sky_mean(const AdjointArgs& A, cudaStream_t st);
 
 // Photons (photon.cu)
 struct PhotonEmit {

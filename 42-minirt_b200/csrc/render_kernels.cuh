@@ -59,6 +59,24 @@ __global__ void __launch_bounds__(kBlock) megakernel(V S, LaunchParams L, float4
   }
 }
 
+// A finished path's radiance into the frame: the float4 accumulator, or the
+// fixed-point one of the differentiable forward (LaunchParams::accum_fx).
+__device__ __forceinline__ void add_path(const LaunchParams& L, float4* accum, uint32_t pixel, float3 c) {
+  if (L.accum_fx) {
+    unsigned long long* q = L.accum_fx + 3 * (size_t)pixel;
+    const float v[3] = {c.x, c.y, c.z};
+    for (int k = 0; k < 3; ++k) {
+      double x = (double)v[k] * kFrameFxScale;
+      if (!(x == x)) x = 0.0;
+      x = fmin(fmax(x, -4.0e18), 4.0e18);
+      const long long iq = __double2ll_rn(x);
+      if (iq) atomicAdd(q + k, (unsigned long long)iq);
+    }
+  } else {
+    atomicAdd(accum + pixel, make_float4(c.x, c.y, c.z, 1.0f));
+  }
+}
+
 // Persistent megakernel with path regeneration: every lane advances its path
 // by one bounce per loop iteration; lanes whose path ended take the next path
 // index (one atomic per warp for all idle lanes), so warps stay full until
@@ -98,7 +116,7 @@ __global__ void __launch_bounds__(kBlock) megakernel_regen(V S, LaunchParams L, 
           P.last_mat = -1;
           depth_left = L.max_bounces;
           active = depth_left > 0;
-          if (!active) atomicAdd(accum + pixel, make_float4(0.f, 0.f, 0.f, 1.0f));
+          if (!active) add_path(L, accum, pixel, f3(0.f, 0.f, 0.f));
         }
       }
     }
@@ -106,7 +124,7 @@ __global__ void __launch_bounds__(kBlock) megakernel_regen(V S, LaunchParams L, 
     if (active) {
       if (!bounce(S, P, depth_left, status, C)) {
         active = false;
-        atomicAdd(accum + pixel, make_float4(P.acc.x, P.acc.y, P.acc.z, 1.0f));
+        add_path(L, accum, pixel, P.acc);
       }
     }
   }

@@ -36,7 +36,7 @@ constexpr int kKinds = 4;   // 0 diffuse/default, 1 metal, 2 dielectric, 3 mixed
 constexpr int kWfBlock = 128;
 
 #ifndef MRT_WF_SMEM_STACK
-#define MRT_WF_SMEM_STACK 24
+#define MRT_WF_SMEM_STACK 0
 #endif
 #ifndef MRT_WF_MINB
 #define MRT_WF_MINB 1
@@ -52,10 +52,10 @@ constexpr int kTravShared = MRT_WF_SMEM_STACK;
 #define MRT_TRAV_STACK(name) LocalStack name
 #endif
 #ifndef MRT_WF_SORT
-#define MRT_WF_SORT 1
+#define MRT_WF_SORT 0
 #endif
 #ifndef MRT_WF_SORT_SH
-#define MRT_WF_SORT_SH 1
+#define MRT_WF_SORT_SH 0
 #endif
 #ifndef MRT_WF_SORT_BITS
 #define MRT_WF_SORT_BITS 5
@@ -258,6 +258,86 @@ __global__ void __launch_bounds__(kWfBlock) wf_sort_scatter_sh(WfState W) {
     const unsigned dst = W.sort_hist[kr.x] + kr.y;
     W.sh_o2[dst] = W.sh_o[k];
     W.sh_d2[dst] = W.sh_d[k];
+  }
+}
+
+// Block-local reordering: each block sorts 1024 consecutive queue entries by
+// ray key in shared memory (bitonic network) and writes them back in place;
+// no global histogram or scan. Entries beyond n sort last with key ~0u.
+constexpr int kLocalSort = 1024;
+
+__device__ __forceinline__ void bitonic_1024(uint32_t* key, uint16_t* idx) {
+  const int t = threadIdx.x;
+  for (int k = 2; k <= kLocalSort; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      const int u = t ^ j;
+      if (u > t) {
+        const bool up = (t & k) == 0;
+        const uint32_t a = key[t], b = key[u];
+        if ((a > b) == up) {
+          key[t] = b; key[u] = a;
+          const uint16_t x = idx[t]; idx[t] = idx[u]; idx[u] = x;
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+template <int kBounceParity>
+__global__ void __launch_bounds__(kLocalSort) wf_sort_local(SceneView S, WfState W) {
+  __shared__ uint32_t key[kLocalSort];
+  __shared__ uint16_t idx[kLocalSort];
+  __shared__ int val[kLocalSort];
+  const int n = W.counters[kBounceParity ? C_LIVE1 : C_LIVE0];
+  int* q = W.q_live[kBounceParity];
+  float3 lo, scale;
+  scene_box(S, lo, scale);
+  for (int base = blockIdx.x * kLocalSort; base < n; base += gridDim.x * kLocalSort) {
+    const int k = base + threadIdx.x;
+    uint32_t kk = 0xffffffffu;
+    int v = -1;
+    if (k < n) {
+      v = q[k];
+      const float4 o = W.o[v], d = W.d[v];
+      kk = ray_key(lo, scale, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z));
+    }
+    key[threadIdx.x] = kk;
+    idx[threadIdx.x] = (uint16_t)threadIdx.x;
+    val[threadIdx.x] = v;
+    __syncthreads();
+    bitonic_1024(key, idx);
+    if (k < n) q[k] = val[idx[threadIdx.x]];
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(kLocalSort) wf_sort_local_sh(SceneView S, WfState W) {
+  __shared__ uint32_t key[kLocalSort];
+  __shared__ uint16_t idx[kLocalSort];
+  __shared__ float4 ro[kLocalSort], rd[kLocalSort];
+  const int n = min(W.counters[C_SH], W.sh_capacity);
+  float3 lo, scale;
+  scene_box(S, lo, scale);
+  for (int base = blockIdx.x * kLocalSort; base < n; base += gridDim.x * kLocalSort) {
+    const int k = base + threadIdx.x;
+    uint32_t kk = 0xffffffffu;
+    if (k < n) {
+      const float4 o = W.sh_o[k], d = W.sh_d[k];
+      ro[threadIdx.x] = o;
+      rd[threadIdx.x] = d;
+      kk = ray_key(lo, scale, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z));
+    }
+    key[threadIdx.x] = kk;
+    idx[threadIdx.x] = (uint16_t)threadIdx.x;
+    __syncthreads();
+    bitonic_1024(key, idx);
+    if (k < n) {
+      const int src = idx[threadIdx.x];
+      W.sh_o2[k] = ro[src];
+      W.sh_d2[k] = rd[src];
+    }
+    __syncthreads();
   }
 }
 
@@ -749,7 +829,12 @@ static unsigned wf_enqueue_bounce(const WfHost* H, const VT& v, const WfState& s
   unsigned n = 0;
   const size_t hist_bytes = sizeof(unsigned) * kSortBins;
   const bool sort_live = MRT_WF_SORT && bounce > 0 && v.has_bvh;
-  if (sort_live) {
+  const int local_blocks = std::max(1, std::min((H->capacity + kLocalSort - 1) / kLocalSort, sms * 2));
+  const int local_sh_blocks = std::max(1, std::min((H->sh_capacity + kLocalSort - 1) / kLocalSort, sms * 2));
+  if (sort_live && MRT_WF_SORT == 2) {
+    wf_sort_local<kPar><<<local_blocks, kLocalSort, 0, st>>>(v, s);
+    n += 1;
+  } else if (sort_live) {
     // counting sort of the live queue by ray key (the counters start at zero)
     wf_sort_key<kPar><<<gen_blocks, kWfBlock, 0, st>>>(v, s);
     wf_sort_scan<<<1, kScanThreads, 0, st>>>(s);
@@ -762,7 +847,11 @@ static unsigned wf_enqueue_bounce(const WfHost* H, const VT& v, const WfState& s
   wf_sample<kPar, VT><<<gen_blocks, kWfBlock, 0, st>>>(v, s, dP, status);
   wf_work_reset<<<1, 32, 0, st>>>(s);
   n += 4;
-  if (MRT_WF_SORT_SH && v.has_bvh) {
+  if (MRT_WF_SORT_SH == 2 && v.has_bvh) {
+    wf_sort_local_sh<<<local_sh_blocks, kLocalSort, 0, st>>>(v, s);
+    wf_connect<true, VT><<<pers, kWfBlock, 0, st>>>(v, s, status);
+    n += 2;
+  } else if (MRT_WF_SORT_SH && v.has_bvh) {
     wf_sort_key_sh<<<sh_blocks, kWfBlock, 0, st>>>(v, s);
     wf_sort_scan<<<1, kScanThreads, 0, st>>>(s);
     wf_sort_scatter_sh<<<sh_blocks, kWfBlock, 0, st>>>(s);

@@ -91,7 +91,7 @@ def perturb(theta0: np.ndarray, layout: dict, rel: float, seed: int) -> np.ndarr
 
 def fit(ctx: mrt.Context, theta_init, target, steps: int = 100, lr: float = 1e-2, spp: int = 64,
         seed: int = 1000, decorrelate: bool = True, mask=None, residual_spp: int | None = None,
-        lr_decay: bool = False, callback=None):
+        lr_decay: bool = False, callback=None, sky_log: bool = False, sky_lr: float | None = None):
     """Projected Adam on the mean squared error between render(theta) and
     target (an (H, W, 3) CUDA tensor); each step draws fresh samples. With
     decorrelate, the gradient replays samples independent of those of the
@@ -101,32 +101,60 @@ def fit(ctx: mrt.Context, theta_init, target, steps: int = 100, lr: float = 1e-2
     entry of theta) restricts the fit to a subset. residual_spp (decorrelated
     only) renders the image that sets the residual with more samples than
     the gradient replays (a forward costs about half a backward); lr_decay
-    anneals the rate along a cosine to 1% of lr. Returns (theta, losses)."""
+    anneals the rate along a cosine to 1% of lr.
+
+    sky_log optimises the sky texels in log space (theta_sky = exp(phi)):
+    Adam's steps have a fixed size in the parameter, and sky radiance spans
+    five orders of magnitude (0.2 to 5e4 at a sun), so equal steps in
+    log-radiance are equal relative changes of every texel, and the texels
+    stay positive. sky_lr (default lr) is the rate of that group. Returns
+    (theta, losses)."""
     torch = _torch()
     layout = ctx.diff_layout()
-    theta = torch.as_tensor(theta_init, dtype=torch.float32, device=target.device).clone().requires_grad_(True)
-    lo, hi = bounds(layout, target.device)
-    opt = torch.optim.Adam([theta], lr=lr)
-    keep = None if mask is None else torch.as_tensor(mask, dtype=torch.float32, device=target.device)
+    dev = target.device
+    th0 = torch.as_tensor(theta_init, dtype=torch.float32, device=dev).clone()
+    n_mat = layout["albedo"] + layout["roughness"] + layout["emission"]
+    lo, hi = bounds(layout, dev)
+    keep = None if mask is None else torch.as_tensor(mask, dtype=torch.float32, device=dev)
+    use_log = sky_log and layout["sky"] > 0
+    if use_log:
+        mat = th0[:n_mat].clone().requires_grad_(True)
+        phi = torch.log(torch.clamp(th0[n_mat:], min=1e-6)).requires_grad_(True)
+        groups = [{"params": [mat], "lr": lr}, {"params": [phi], "lr": sky_lr or lr}]
+    else:
+        mat = th0.clone().requires_grad_(True)
+        phi = None
+        groups = [{"params": [mat], "lr": lr}]
+    opt = torch.optim.Adam(groups)
+    base_lrs = [g["lr"] for g in opt.param_groups]
+
+    def full():
+        return torch.cat([mat, torch.exp(phi)]) if use_log else mat
+
     losses = []
     rspp = spp if (residual_spp is None or not decorrelate) else residual_spp
     stride = rspp + spp
     for step in range(steps):
         if lr_decay:
-            for grp in opt.param_groups:
-                grp["lr"] = lr * (0.01 + 0.99 * 0.5 * (1 + np.cos(np.pi * step / max(steps - 1, 1))))
+            f = 0.01 + 0.99 * 0.5 * (1 + np.cos(np.pi * step / max(steps - 1, 1)))
+            for grp, b in zip(opt.param_groups, base_lrs):
+                grp["lr"] = b * f
         opt.zero_grad(set_to_none=True)
         base = step * stride
+        theta = full()
         img = render(theta, ctx, rspp, seed, base, base + rspp if decorrelate else base, spp)
         loss = torch.mean((img - target) ** 2)
         loss.backward()
         if keep is not None:
-            theta.grad.mul_(keep)
+            mat.grad.mul_(keep[:mat.numel()])
+            if use_log:
+                phi.grad.mul_(keep[n_mat:])
         opt.step()
         with torch.no_grad():
-            boxed = torch.maximum(torch.minimum(theta, hi), lo)
-            theta.copy_(boxed if keep is None else torch.where(keep > 0, boxed, theta))
+            m_lo, m_hi = lo[:mat.numel()], hi[:mat.numel()]
+            boxed = torch.maximum(torch.minimum(mat, m_hi), m_lo)
+            mat.copy_(boxed if keep is None else torch.where(keep[:mat.numel()] > 0, boxed, mat))
         losses.append(float(loss.detach()))
         if callback:
             callback(step, losses[-1])
-    return theta.detach(), losses
+    return full().detach(), losses

@@ -8,8 +8,13 @@ rendering random pixel batches through calc_one_sample_task
 (oracle/_ref/liboracle_ref.so). Scene preparation (the reference's BVH build,
 HDRI tables, photon map) happens once before forking and is not timed.
 
+Two builds of the same sources (oracle/Makefile): "parity" (-O2, the build
+the parity tests pin against) and "fast" (-O3 -march=x86-64-v3, no
+-ffast-math), the stronger of the two CPU baselines.
+
 Run as a separate process (it forks; it must not share a process with CUDA):
   python oracle/cpu_baseline.py --config c1 --seconds 10 [--procs N] [--steps K --warmup W]
+                                [--build parity|fast]
 Prints one JSON object.
 """
 from __future__ import annotations
@@ -82,9 +87,14 @@ def timed_step(ref, seconds: float, procs: int, seed: int, batch: int) -> dict:
     return {"paths": paths, "seconds": secs, "mpaths_s": paths / secs / 1e6}
 
 
+BUILDS = {"parity": ("_ref/liboracle_ref.so", "-O2"),
+          "fast": ("_ref/fast/liboracle_ref.so", "-O3 -march=x86-64-v3")}
+
+
 def run(config: str, seconds: float, procs: int, steps: int = 1, warmup: int = 0,
-        batch: int = 64) -> dict:
+        batch: int = 64, build: str = "parity") -> dict:
     import oracle
+    oracle.REF_LIB = HERE / BUILDS[build][0]
     sc = make_scene(config)
     t0 = time.perf_counter()
     oracle.ref_lib().refh_set_seed(12345)
@@ -99,6 +109,7 @@ def run(config: str, seconds: float, procs: int, steps: int = 1, warmup: int = 0
             "seconds": secs, "mpaths_s": paths / secs / 1e6,
             "per_core_mpaths_s": paths / secs / 1e6 / procs, "steps": steps,
             "step_mpaths_s": [r["mpaths_s"] for r in rates],
+            "build": f"{build} ({BUILDS[build][1]}, no -ffast-math)",
             "sample": f"{config} full scene, random pixels in batches of {batch} at 1 spp, "
                       f"{procs} forked processes x {seconds:g} s per step"}
 
@@ -110,8 +121,9 @@ def main() -> int:
     ap.add_argument("--procs", type=int, default=os.cpu_count() or 1)
     ap.add_argument("--steps", type=int, default=1)
     ap.add_argument("--warmup", type=int, default=0)
+    ap.add_argument("--build", default="parity", choices=sorted(BUILDS))
     a = ap.parse_args()
-    print(json.dumps(run(a.config, a.seconds, a.procs, a.steps, a.warmup)), flush=True)
+    print(json.dumps(run(a.config, a.seconds, a.procs, a.steps, a.warmup, build=a.build)), flush=True)
     return 0
 
 

@@ -81,7 +81,7 @@ def test_first_hit_matches_reference_golden(mrt, oracle, mg, name):
     sc = mg.CASES[name]["make"]()
     ctx = gpu_ctx(mrt, oracle, sc)
     h = ctx.first_hit(g["rays_o"], g["rays_d"])
-    ref = {"prim": g["hit_prim"], "t": g["hit_t"], "point": g["hit_point"]}
+    ref = {"prim": g["hit_prim"], "t": g["hit_t"], "point": g["hit_point"], "normal": g["hit_normal"]}
     exact = assert_hit_parity(name, sc, tri_positions(oracle, sc), g["rays_o"], g["rays_d"], h, ref)
     hit = (h["prim"] >= 0) & exact
     np.testing.assert_array_equal(h["front_face"][hit], g["hit_front_face"][hit])
