@@ -177,6 +177,12 @@ struct mrt_ctx {
   void* comm = nullptr;
   int comm_rank = 0, comm_world = 1;
   DevBuf<long long> comm_count;          // sample count reduced with the frame
+  // BVH build options (mrt_set_bvh_options), applied by mrt_scene_build
+  int bvh_mode = MRT_BVH_SAH;
+  std::vector<int32_t> bvh_list;         // reference object-list order (flat ids), empty = flat order
+  std::vector<double> bvh_pos;           // positions the reference's split sorts by, empty = computed
+  DevBuf<double> ref_boxes;
+  std::vector<uint32_t> leaf_order;      // flat primitive id of each leaf slot (last build)
 };
 
 namespace {
@@ -556,6 +562,14 @@ extern "C" int mrt_scene_build(mrt_ctx* c, const mrt_scene_desc* d) {
   const size_t q_hyp = q_cone + d->n_cones, tri_base = q_hyp + d->n_hyperboloids;
   const size_t n_prims = tri_base + n_tris;
   std::vector<PrimBox> boxes(n_prims);
+  // double bounds and split positions for the reference-topology tree
+  const bool ref_tree = c->bvh_mode == MRT_BVH_REFERENCE;
+  std::vector<RefPrim> refp(ref_tree ? n_prims : 0);
+  auto set_box = [&](size_t idx, const double* mn, const double* mx, const double* pos) {
+    prim_box_from_double(boxes[idx], mn, mx);
+    if (!ref_tree) return;
+    for (int k = 0; k < 3; ++k) { refp[idx].mn[k] = mn[k]; refp[idx].mx[k] = mx[k]; refp[idx].pos[k] = pos[k]; }
+  };
   struct TriRef { const mrt_mesh* m; uint32_t t; };
   std::vector<TriRef> tris;
   tris.reserve(n_tris);
@@ -567,7 +581,7 @@ extern "C" int mrt_scene_build(mrt_ctx* c, const mrt_scene_desc* d) {
     double mn[3], mx[3];
     const double r = (s.radius * 2.0) * 0.5;
     for (int k = 0; k < 3; ++k) { mn[k] = s.center[k] - r; mx[k] = s.center[k] + r; }
-    prim_box_from_double(boxes[i], mn, mx);
+    set_box(i, mn, mx, s.center);
   }
   // quadric bounds as bvh_obj_bounds.c computes them (axis-aligned extents of
   // the end discs, :41-96); a zero orientation takes the default the hit
@@ -578,14 +592,14 @@ extern "C" int mrt_scene_build(mrt_ctx* c, const mrt_scene_desc* d) {
     if (a.x == 0 && a.y == 0 && a.z == 0) a = dz ? V3{0, 0, 1} : V3{0, 1, 0};
     axis = unitv(a);
   };
-  auto disc_box = [&](size_t idx, const V3& p0, const V3& p1, const V3& a, double r) {
+  auto disc_box = [&](size_t idx, const V3& p0, const V3& p1, const V3& a, double r, const double* pos) {
     const double e[3] = {r * std::sqrt(std::max(0.0, 1.0 - a.x * a.x)), r * std::sqrt(std::max(0.0, 1.0 - a.y * a.y)),
                          r * std::sqrt(std::max(0.0, 1.0 - a.z * a.z))};
     const double lo[3] = {std::min(p0.x, p1.x), std::min(p0.y, p1.y), std::min(p0.z, p1.z)};
     const double hi[3] = {std::max(p0.x, p1.x), std::max(p0.y, p1.y), std::max(p0.z, p1.z)};
     double mn[3], mx[3];
     for (int k = 0; k < 3; ++k) { mn[k] = lo[k] - e[k]; mx[k] = hi[k] + e[k]; }
-    prim_box_from_double(boxes[idx], mn, mx);
+    set_box(idx, mn, mx, pos);
   };
   for (int i = 0; i < d->n_cylinders; ++i) {
     const mrt_cylinder& q = d->cylinders[i];
@@ -595,7 +609,7 @@ extern "C" int mrt_scene_build(mrt_ctx* c, const mrt_scene_desc* d) {
     V3 a;
     axis_of(q.orientation, 0, a);
     const V3 c = v3(q.position), h = mul(a, q.height * 0.5);
-    disc_box(q_cyl + i, sub(c, h), add(c, h), a, q.diameter * 0.5);
+    disc_box(q_cyl + i, sub(c, h), add(c, h), a, q.diameter * 0.5, q.position);
   }
   for (int i = 0; i < d->n_cones; ++i) {
     const mrt_cone& q = d->cones[i];
@@ -605,7 +619,7 @@ extern "C" int mrt_scene_build(mrt_ctx* c, const mrt_scene_desc* d) {
     V3 a;
     axis_of(q.orientation, 0, a);
     const V3 c = v3(q.position);
-    disc_box(q_cone + i, c, add(c, mul(a, q.height)), a, q.diameter * 0.5);
+    disc_box(q_cone + i, c, add(c, mul(a, q.height)), a, q.diameter * 0.5, q.position);
   }
   for (int i = 0; i < d->n_hyperboloids; ++i) {
     const mrt_hyperboloid& q = d->hyperboloids[i];
@@ -619,7 +633,7 @@ extern "C" int mrt_scene_build(mrt_ctx* c, const mrt_scene_desc* d) {
     const double hh = q.height * 0.5;
     const double rmax = std::max(std::fabs(q.a), std::fabs(q.b)) *
                         std::sqrt(std::max(0.0, q.shape + (hh * hh) / (q.c * q.c)));
-    disc_box(q_hyp + i, sub(c, h), add(c, h), a, rmax);
+    disc_box(q_hyp + i, sub(c, h), add(c, h), a, rmax, q.position);
   }
   {
     size_t p = tri_base;
@@ -627,6 +641,7 @@ extern "C" int mrt_scene_build(mrt_ctx* c, const mrt_scene_desc* d) {
       const mrt_mesh& me = d->meshes[i];
       for (uint32_t t = 0; t < me.n_triangles; ++t, ++p) {
         double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+        double sum[3] = {0, 0, 0};      // (v0 + v1) + v2, the centre's order of additions
         for (int cidx = 0; cidx < 3; ++cidx) {
           uint32_t vi = me.indices ? me.indices[3 * (size_t)t + cidx] : 3 * t + cidx;
           const double* q = me.positions + 3 * (size_t)vi;
@@ -635,17 +650,49 @@ extern "C" int mrt_scene_build(mrt_ctx* c, const mrt_scene_desc* d) {
               return set_err(MRT_ERR_INVALID, "mesh %d triangle %u has a non-finite vertex", i, t);
             mn[k] = std::min(mn[k], q[k]);
             mx[k] = std::max(mx[k], q[k]);
+            sum[k] += q[k];
           }
         }
-        prim_box_from_double(boxes[p], mn, mx);
+        // triangle centre as the loaders compute it (obj_finilizer.c:54)
+        const double centre[3] = {sum[0] / 3.0, sum[1] / 3.0, sum[2] / 3.0};
+        set_box(p, mn, mx, centre);
         tris.push_back({&me, t});
       }
     }
   }
   BvhResult bvh;
   std::string err;
-  if (!build_bvh(boxes, bvh, err)) return set_err(MRT_ERR_INVALID, "BVH: %s", err.c_str());
+  std::vector<double> dboxes;
+  if (ref_tree) {
+    std::vector<uint32_t> list(n_prims);
+    if (!c->bvh_list.empty()) {
+      if (c->bvh_list.size() != n_prims)
+        return set_err(MRT_ERR_INVALID, "BVH options: object list of %zu entries for %zu primitives",
+                       c->bvh_list.size(), n_prims);
+      std::vector<char> seen(n_prims, 0);
+      for (size_t i = 0; i < n_prims; ++i) {
+        const int32_t f = c->bvh_list[i];
+        if (f < 0 || (size_t)f >= n_prims || seen[f])
+          return set_err(MRT_ERR_INVALID, "BVH options: object list entry %zu (%d) is not a permutation", i, f);
+        seen[f] = 1;
+        list[i] = (uint32_t)f;
+      }
+    } else {
+      for (size_t i = 0; i < n_prims; ++i) list[i] = (uint32_t)i;
+    }
+    if (!c->bvh_pos.empty()) {
+      if (c->bvh_pos.size() != 3 * n_prims)
+        return set_err(MRT_ERR_INVALID, "BVH options: %zu positions for %zu primitives", c->bvh_pos.size() / 3, n_prims);
+      for (size_t i = 0; i < n_prims; ++i)
+        for (int k = 0; k < 3; ++k) refp[i].pos[k] = c->bvh_pos[3 * i + k];
+    }
+    if (!build_bvh_reference(refp, list, bvh, dboxes, err))
+      return set_err(MRT_ERR_INVALID, "BVH: %s", err.c_str());
+  } else if (!build_bvh(boxes, bvh, err)) {
+    return set_err(MRT_ERR_INVALID, "BVH: %s", err.c_str());
+  }
   c->bvh_depth = bvh.max_depth;
+  c->leaf_order = bvh.order;
 
   // leaf-order geometry, metadata and shading records
   std::vector<float4> geom(3 * std::max<size_t>(n_prims, 1));
@@ -828,6 +875,13 @@ extern "C" int mrt_scene_build(mrt_ctx* c, const mrt_scene_desc* d) {
   v.has_bvh = n_prims > 0;
   v.has_quadrics = (d->n_cylinders + d->n_cones + d->n_hyperboloids) > 0;
   v.root_leaf = bvh.root_leaf;
+  v.left_first = ref_tree ? 1 : 0;
+  v.ref_boxes = nullptr;
+  c->ref_boxes.release();
+  if (ref_tree && !dboxes.empty()) {
+    CK(c->ref_boxes.upload(dboxes.data(), dboxes.size(), st));
+    v.ref_boxes = c->ref_boxes.p;
+  }
   set_viewport(v, d->camera, c->W, c->H);
 
   // sky and importance-sampling tables
@@ -1864,4 +1918,23 @@ extern "C" void mrt_shard_samples(int64_t total, int32_t world, int32_t rank, in
   const int64_t base = total / world, extra = total % world;
   if (first) *first = rank * base + std::min<int64_t>(rank, extra);
   if (count) *count = base + (rank < extra ? 1 : 0);
+}
+
+extern "C" int mrt_set_bvh_options(mrt_ctx* c, const mrt_bvh_options* o) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!o || (o->mode != MRT_BVH_SAH && o->mode != MRT_BVH_REFERENCE) || o->n_prims < 0)
+    return set_err(MRT_ERR_INVALID, "mrt_set_bvh_options: mode %d", o ? o->mode : -1);
+  c->bvh_mode = o->mode;
+  c->bvh_list.assign(o->order ? o->order : nullptr, o->order ? o->order + o->n_prims : nullptr);
+  c->bvh_pos.assign(o->positions ? o->positions : nullptr, o->positions ? o->positions + 3 * o->n_prims : nullptr);
+  return MRT_OK;
+}
+
+extern "C" int64_t mrt_read_bvh_leaves(mrt_ctx* c, int32_t* flat, int64_t cap) {
+  if (!c || !c->has_scene) return set_err(MRT_ERR_INVALID, "mrt_read_bvh_leaves: no scene");
+  const int64_t n = (int64_t)c->leaf_order.size();
+  if (flat)
+    for (int64_t i = 0; i < std::min(n, cap); ++i) flat[i] = (int32_t)c->leaf_order[i];
+  return n;
 }

@@ -50,15 +50,10 @@ struct BNode {
 
 constexpr int kBins = 32;
 constexpr int kMedianDepth = 40;
-#ifndef MRT_SAH_ISECT
-#define MRT_SAH_ISECT 1.0f
-#endif
-#ifndef MRT_BUILD_LEAF_MAX
-#define MRT_BUILD_LEAF_MAX kLeafMax
-#endif
+// Intersection cost 1.5 and leaves of at most 4 primitives were measured
+// against these (c1, c4): within 1 % either way.
 constexpr float kTraversalCost = 1.0f;
-constexpr float kIsectCost = MRT_SAH_ISECT;
-constexpr int kBuildLeafMax = MRT_BUILD_LEAF_MAX;
+constexpr float kIsectCost = 1.0f;
 
 struct Builder {
   const std::vector<PrimBox>& prims;
@@ -94,7 +89,7 @@ struct Builder {
     if (ext[1] > ext[axis]) axis = 1;
     if (ext[2] > ext[axis]) axis = 2;
     if (depth >= kMedianDepth || ext[axis] <= 0.0f) {
-      if (n <= (uint32_t)kBuildLeafMax && depth < kMedianDepth) return 0;
+      if (n <= (uint32_t)kLeafMax && depth < kMedianDepth) return 0;
       uint32_t mid = b + n / 2;
       std::nth_element(order.begin() + b, order.begin() + mid, order.begin() + e,
                        [&](uint32_t x, uint32_t y) { return prims[x].c[axis] < prims[y].c[axis]; });
@@ -142,8 +137,8 @@ struct Builder {
     const float parent_area = std::max(box.area(), 1e-30f);
     const float split_cost = kTraversalCost + kIsectCost * best_cost / parent_area;
     const float leaf_cost = kIsectCost * n;
-    if (best_axis < 0 || (n <= (uint32_t)kBuildLeafMax && leaf_cost <= split_cost)) {
-      if (n <= (uint32_t)kBuildLeafMax) return 0;
+    if (best_axis < 0 || (n <= (uint32_t)kLeafMax && leaf_cost <= split_cost)) {
+      if (n <= (uint32_t)kLeafMax) return 0;
       uint32_t mid = b + n / 2;
       std::nth_element(order.begin() + b, order.begin() + mid, order.begin() + e,
                        [&](uint32_t x, uint32_t y) { return prims[x].c[axis] < prims[y].c[axis]; });
@@ -211,6 +206,54 @@ void prim_box_from_double(PrimBox& p, const double* mn, const double* mx) {
     p.mx[k] = round_up(mx[k]);
     p.c[k] = (float)(0.5 * (mn[k] + mx[k]));
   }
+}
+
+// Flattens a tree of BNodes (root 0) to dual-child device nodes in
+// depth-first order; dev_index_out (optional) receives each internal
+// node's device index.
+static bool flatten(const std::vector<BNode>& nodes, BvhResult& out, std::vector<int>* dev_index_out) {
+  if (nodes[0].left < 0) {
+    out.root_leaf = leaf_link(nodes[0].first, nodes[0].count);
+    Node dn;
+    const BNode& r = nodes[0];
+    dn.lxy = make_float4(r.box.mn[0], r.box.mx[0], r.box.mn[1], r.box.mx[1]);
+    dn.rxy = make_float4(INFINITY, -INFINITY, INFINITY, -INFINITY);
+    dn.z = make_float4(r.box.mn[2], r.box.mx[2], INFINITY, -INFINITY);
+    dn.link = make_int4(out.root_leaf, out.root_leaf, 0, 0);
+    out.nodes.push_back(dn);
+    out.leaves = 1;
+    return true;
+  }
+  std::vector<int> local_index;
+  std::vector<int>& dev_index = dev_index_out ? *dev_index_out : local_index;
+  dev_index.assign(nodes.size(), -1);
+  std::vector<int> stack{0};
+  std::vector<int> order_nodes;
+  while (!stack.empty()) {
+    int i = stack.back();
+    stack.pop_back();
+    dev_index[i] = (int)order_nodes.size();
+    order_nodes.push_back(i);
+    if (nodes[nodes[i].right].left >= 0) stack.push_back(nodes[i].right);
+    if (nodes[nodes[i].left].left >= 0) stack.push_back(nodes[i].left);
+  }
+  out.nodes.resize(order_nodes.size());
+  for (size_t k = 0; k < order_nodes.size(); ++k) {
+    const BNode& p = nodes[order_nodes[k]];
+    const BNode& L = nodes[p.left];
+    const BNode& R = nodes[p.right];
+    Node dn;
+    dn.lxy = make_float4(L.box.mn[0], L.box.mx[0], L.box.mn[1], L.box.mx[1]);
+    dn.rxy = make_float4(R.box.mn[0], R.box.mx[0], R.box.mn[1], R.box.mx[1]);
+    dn.z = make_float4(L.box.mn[2], L.box.mx[2], R.box.mn[2], R.box.mx[2]);
+    int ll = L.left >= 0 ? dev_index[p.left] : leaf_link(L.first, L.count);
+    int rl = R.left >= 0 ? dev_index[p.right] : leaf_link(R.first, R.count);
+    if (L.left < 0) out.leaves++;
+    if (R.left < 0) out.leaves++;
+    dn.link = make_int4(ll, rl, 0, 0);
+    out.nodes[k] = dn;
+  }
+  return true;
 }
 
 bool build_bvh(const std::vector<PrimBox>& prims, BvhResult& out, std::string& err) {
@@ -297,45 +340,153 @@ bool build_bvh(const std::vector<PrimBox>& prims, BvhResult& out, std::string& e
     return false;
   }
 
-  // Flatten to dual-child device nodes in depth-first order.
-  if (nodes[0].left < 0) {
-    out.root_leaf = leaf_link(nodes[0].first, nodes[0].count);
-    Node dn;
-    const BNode& r = nodes[0];
-    dn.lxy = make_float4(r.box.mn[0], r.box.mx[0], r.box.mn[1], r.box.mx[1]);
-    dn.rxy = make_float4(INFINITY, -INFINITY, INFINITY, -INFINITY);
-    dn.z = make_float4(r.box.mn[2], r.box.mx[2], INFINITY, -INFINITY);
-    dn.link = make_int4(out.root_leaf, out.root_leaf, 0, 0);
-    out.nodes.push_back(dn);
-    out.leaves = 1;
+  return flatten(nodes, out, nullptr);
+}
+
+
+// ---------------------------------------------------------------------------
+// The reference's median-split tree, for parity runs (MRT_BVH_REFERENCE).
+// Its steps are restated, not redesigned, because the topology must come out
+// identical: node bounds are the union of the primitives' double bounds; a
+// node of more than one primitive is split on the longest axis of its bounds
+// (choose_axis, bvh_build.c:44) at count / 2 after sorting its primitives by
+// their position on that axis compared as float (compare_obj_axis_with_bvh,
+// bvh_math.c:34); the sort is the reference's (qshort_axis.c: insertion sort
+// below 16 elements, else median-of-three quicksort recursing on the smaller
+// side), whose handling of equal keys decides the order of ties.
+namespace {
+
+struct RefSort {
+  const std::vector<RefPrim>& prims;
+  const std::vector<uint32_t>& list;
+  int axis;
+  int cmp(uint32_t a, uint32_t b) const {
+    const float va = (float)prims[list[a]].pos[axis], vb = (float)prims[list[b]].pos[axis];
+    return va < vb ? -1 : (va > vb ? 1 : 0);
+  }
+  void insertion(uint32_t* arr, int lo, int hi) const {
+    for (int i = lo + 1; i <= hi; ++i) {
+      const uint32_t key = arr[i];
+      int j = i - 1;
+      while (j >= lo && cmp(arr[j], key) > 0) {
+        arr[j + 1] = arr[j];
+        --j;
+      }
+      arr[j + 1] = key;
+    }
+  }
+  int partition(uint32_t* arr, int lo, int hi) const {
+    const int mid = lo + (hi - lo) / 2;
+    if (cmp(arr[lo], arr[mid]) > 0) std::swap(arr[lo], arr[mid]);
+    if (cmp(arr[lo], arr[hi]) > 0) std::swap(arr[lo], arr[hi]);
+    if (cmp(arr[mid], arr[hi]) > 0) std::swap(arr[mid], arr[hi]);
+    std::swap(arr[mid], arr[hi - 1]);
+    const uint32_t pivot = arr[hi - 1];
+    int i = lo, j = hi - 1;
+    while (true) {
+      while (cmp(arr[++i], pivot) < 0) {}
+      while (cmp(arr[--j], pivot) > 0) {}
+      if (i >= j) break;
+      std::swap(arr[i], arr[j]);
+    }
+    std::swap(arr[i], arr[hi - 1]);
+    return i;
+  }
+  void sort(uint32_t* arr, int lo, int hi) const {
+    while (lo < hi) {
+      if (hi - lo < 16) {
+        insertion(arr, lo, hi);
+        return;
+      }
+      const int p = partition(arr, lo, hi);
+      if (p - lo < hi - p) {
+        sort(arr, lo, p - 1);
+        lo = p + 1;
+      } else {
+        sort(arr, p + 1, hi);
+        hi = p - 1;
+      }
+    }
+  }
+};
+
+}  // namespace
+
+
+bool build_bvh_reference(const std::vector<RefPrim>& prims, const std::vector<uint32_t>& list,
+                         BvhResult& out, std::vector<double>& dboxes, std::string& err) {
+  out = BvhResult();
+  dboxes.clear();
+  const uint32_t n = (uint32_t)list.size();
+  if (n == 0) return true;
+  if (n >= (1u << 28) || list.size() != prims.size()) {
+    err = n >= (1u << 28) ? "too many primitives for the leaf encoding (max 2^28)"
+                          : "reference BVH: object list does not cover the primitives";
+    return false;
+  }
+  std::vector<uint32_t> idx(n);            // prim_indices: positions in the object list
+  for (uint32_t i = 0; i < n; ++i) idx[i] = i;
+  std::vector<BNode> nodes;
+  std::vector<double> dbl;                 // 6 per BNode
+  RefSort sorter{prims, list, 0};
+  auto make_node = [&](uint32_t start, uint32_t count, int depth) {
+    double mn[3], mx[3];
+    const RefPrim& f = prims[list[idx[start]]];
+    for (int k = 0; k < 3; ++k) { mn[k] = f.mn[k]; mx[k] = f.mx[k]; }
+    for (uint32_t i = 0; i < count; ++i) {
+      const RefPrim& p = prims[list[idx[start + i]]];
+      for (int k = 0; k < 3; ++k) { mn[k] = std::fmin(mn[k], p.mn[k]); mx[k] = std::fmax(mx[k], p.mx[k]); }
+    }
+    BNode b;
+    for (int k = 0; k < 3; ++k) { b.box.mn[k] = round_down(mn[k]); b.box.mx[k] = round_up(mx[k]); }
+    b.first = start;
+    b.count = count;
+    b.depth = depth;
+    nodes.push_back(b);
+    dbl.insert(dbl.end(), {mn[0], mn[1], mn[2], mx[0], mx[1], mx[2]});
+    return (int)nodes.size() - 1;
+  };
+  struct Task { uint32_t start, count; int node; };
+  std::vector<Task> stack;
+  stack.push_back({0, n, make_node(0, n, 0)});
+  while (!stack.empty()) {
+    const Task t = stack.back();
+    stack.pop_back();
+    if (t.count <= 1) continue;
+    const double* b = &dbl[6 * (size_t)t.node];
+    const double ex = b[3] - b[0], ey = b[4] - b[1], ez = b[5] - b[2];
+    sorter.axis = (ex > ey && ex > ez) ? 0 : (ey > ez ? 1 : 2);
+    sorter.sort(idx.data() + t.start, 0, (int)t.count - 1);
+    const uint32_t mid = t.start + t.count / 2;
+    const int depth = nodes[t.node].depth + 1;
+    const int l = make_node(t.start, mid - t.start, depth);
+    const int r = make_node(mid, t.start + t.count - mid, depth);
+    nodes[t.node].left = l;
+    nodes[t.node].right = r;
+    stack.push_back({mid, t.start + t.count - mid, r});
+    stack.push_back({t.start, mid - t.start, l});
+  }
+  for (const BNode& q : nodes) out.max_depth = std::max(out.max_depth, q.depth);
+  if (out.max_depth >= kMaxTreeDepth) {
+    err = "reference BVH deeper than the traversal stack";
+    return false;
+  }
+  // leaves hold one primitive each: leaf order = the sorted object list
+  out.order.resize(n);
+  for (uint32_t i = 0; i < n; ++i) out.order[i] = list[idx[i]];
+  std::vector<int> dev_index;
+  if (!flatten(nodes, out, &dev_index)) return false;
+  dboxes.assign(6 + 12 * out.nodes.size(), 0.0);
+  std::copy(dbl.begin(), dbl.begin() + 6, dboxes.begin());
+  if (nodes[0].left < 0) {                 // a single primitive: the root is the leaf
+    std::copy(dbl.begin(), dbl.begin() + 6, dboxes.begin() + 6);
     return true;
   }
-  std::vector<int> dev_index(nodes.size(), -1);
-  std::vector<int> stack{0};
-  std::vector<int> order_nodes;
-  while (!stack.empty()) {
-    int i = stack.back();
-    stack.pop_back();
-    dev_index[i] = (int)order_nodes.size();
-    order_nodes.push_back(i);
-    if (nodes[nodes[i].right].left >= 0) stack.push_back(nodes[i].right);
-    if (nodes[nodes[i].left].left >= 0) stack.push_back(nodes[i].left);
-  }
-  out.nodes.resize(order_nodes.size());
-  for (size_t k = 0; k < order_nodes.size(); ++k) {
-    const BNode& p = nodes[order_nodes[k]];
-    const BNode& L = nodes[p.left];
-    const BNode& R = nodes[p.right];
-    Node dn;
-    dn.lxy = make_float4(L.box.mn[0], L.box.mx[0], L.box.mn[1], L.box.mx[1]);
-    dn.rxy = make_float4(R.box.mn[0], R.box.mx[0], R.box.mn[1], R.box.mx[1]);
-    dn.z = make_float4(L.box.mn[2], L.box.mx[2], R.box.mn[2], R.box.mx[2]);
-    int ll = L.left >= 0 ? dev_index[p.left] : leaf_link(L.first, L.count);
-    int rl = R.left >= 0 ? dev_index[p.right] : leaf_link(R.first, R.count);
-    if (L.left < 0) out.leaves++;
-    if (R.left < 0) out.leaves++;
-    dn.link = make_int4(ll, rl, 0, 0);
-    out.nodes[k] = dn;
+  for (size_t i = 0; i < nodes.size(); ++i) {
+    if (nodes[i].left < 0) continue;
+    double* d = &dboxes[6 + 12 * (size_t)dev_index[i]];
+    std::copy(dbl.begin() + 6 * nodes[i].left, dbl.begin() + 6 * nodes[i].left + 6, d);
+    std::copy(dbl.begin() + 6 * nodes[i].right, dbl.begin() + 6 * nodes[i].right + 6, d + 6);
   }
   return true;
 }

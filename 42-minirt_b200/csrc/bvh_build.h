@@ -24,4 +24,20 @@ struct BvhResult {
 void prim_box_from_double(PrimBox& p, const double* mn, const double* mx);
 bool build_bvh(const std::vector<PrimBox>& prims, BvhResult& out, std::string& err);
 
+// A primitive of the reference-topology build: its bounds as the reference
+// computes them (compute_object_bounds, bvh_math.c:17) and the position its
+// median split sorts by (get_obj_position, bvh_utils.c:88).
+struct RefPrim {
+  double mn[3], mx[3];
+  double pos[3];
+};
+
+// The reference's own tree (bvh_build.c:16-127): list[i] is the input
+// primitive at position i of the reference's object list (bvh_make_lst.c).
+// dboxes receives the double-precision boxes for the reference's node-visit
+// count: 6 for the root, then 12 per device node (left child, right child),
+// each as min xyz, max xyz.
+bool build_bvh_reference(const std::vector<RefPrim>& prims, const std::vector<uint32_t>& list,
+                         BvhResult& out, std::vector<double>& dboxes, std::string& err);
+
 }  // namespace mrt

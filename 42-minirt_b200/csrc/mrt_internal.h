@@ -124,6 +124,8 @@ struct SceneView {
   int has_bvh;
   int has_quadrics;      // launch the SceneViewQ instantiation
   int has_textures;      // launch the SceneViewT instantiation
+  int left_first;        // traverse the left child first (reference-topology tree), else the nearer
+  const double* ref_boxes;  // reference-topology tree: double child boxes for its node-visit count
   const MatTexD* mat_tex;    // per material
   const TexD* texs;
   const uchar4* texels;

@@ -143,7 +143,14 @@ __device__ __forceinline__ float3 trace_path(const V& S, PathState& P, int max_d
     bool hit = closest_hit<true>(S, P.o, P.d, h, visits, status, P.rng.s);
     C.segments++;
     C.visits += visits;
-    if (render_mode == 1) return f3(hit ? (float)visits : -1.0f, 0.f, 0.f);
+    if (render_mode == 1) {
+      if (S.ref_boxes) {          // the reference's count on its own tree
+        bool any_leaf;
+        const int cnt = ref_visit_count(S, P.o, P.d, any_leaf, status);
+        return f3(hit ? (any_leaf ? (float)cnt : 0.0f) : -1.0f, 0.f, 0.f);
+      }
+      return f3(hit ? (float)visits : -1.0f, 0.f, 0.f);
+    }
     if (!hit) return f3(0.f, 0.f, 0.f);
     return make_surf(S, h, P.o, P.d, 2).color;
   }

@@ -7,9 +7,7 @@
 // tested and replaces the BVH hit only with a strictly smaller t
 // (hit_plane.c:43-71, t in [0.001, 1000]). The tree is walked near child
 // first with boxes culled beyond the best t; the stack (64 entries; the
-// builder keeps the depth below that) is a per-thread array in the
-// megakernels and a shared-memory short stack in the wavefront's traversal
-// kernels (LocalStack, SharedStack below).
+// builder keeps the depth below that) is a per-thread array (LocalStack).
 #pragma once
 #include "device_common.cuh"
 #include "quadric.cuh"
@@ -125,31 +123,15 @@ __device__ __forceinline__ bool prim_hit(const V& S, int i, float3 o, float3 d, 
   return true;
 }
 
-// Traversal stacks. LocalStack: a per-thread array (registers / local
-// memory), used by the megakernels. SharedStack: the first kShared entries of
-// each thread's stack in a [kShared][kThreads] shared-memory array (column =
-// thread, so a warp's pushes at equal depth fall in 32 different banks);
-// deeper entries spill to a per-thread local array. The wavefront's
-// traversal kernels use it, so the common pushes and pops stay out of L1,
-// which then holds more nodes and triangles.
+// The traversal stack: a per-thread array (registers / local memory, which
+// L1 caches). A shared-memory short stack (24 entries per thread, spilling
+// to local memory) measured 2.7 % slower in the wavefront on c1, so the
+// traversal loops take the stack as a parameter and every caller passes this
+// one.
 struct LocalStack {
   int s[kStackSize];
   __device__ __forceinline__ void put(int i, int v) { s[i] = v; }
   __device__ __forceinline__ int get(int i) const { return s[i]; }
-};
-
-template <int kShared, int kThreads>
-struct SharedStack {
-  int* col;
-  int spill[kStackSize - kShared];
-  __device__ __forceinline__ explicit SharedStack(int* smem) : col(smem + threadIdx.x) {}
-  __device__ __forceinline__ void put(int i, int v) {
-    if (i < kShared) col[i * kThreads] = v;
-    else spill[i - kShared] = v;
-  }
-  __device__ __forceinline__ int get(int i) const {
-    return i < kShared ? col[i * kThreads] : spill[i - kShared];
-  }
 };
 
 // Closest hit. `visits` counts node fetches (heat-map / roofline counter).
@@ -188,8 +170,11 @@ __device__ __forceinline__ bool closest_hit_compact(const V& S, float3 o, float3
         float tr = box_hit(rxy.x, rxy.y, rxy.z, rxy.w, z.z, z.w, oi, inv, tbest);
         bool hl = tl < INFINITY, hr = tr < INFINITY;
         if (hl && hr) {
-          int nearc = tl <= tr ? ln.x : ln.y;
-          int farc = tl <= tr ? ln.y : ln.x;
+          // nearer child first; the reference-topology tree keeps the
+          // reference's left-first order, so exact-t ties resolve as there
+          const bool left_near = S.left_first || tl <= tr;
+          int nearc = left_near ? ln.x : ln.y;
+          int farc = left_near ? ln.y : ln.x;
           if (sp < kStackSize) stack.put(sp++, farc);
           else if (status) atomicOr(status, ST_STACK);
           cur = nearc;
@@ -269,6 +254,58 @@ __device__ __forceinline__ bool any_hit_compact(const V& S, float3 o, float3 d, 
     if (sp == 0) return false;
     cur = stack.get(--sp);
   }
+}
+
+// The reference's node-visit count for render_mode 1 on the reference-topology
+// tree (S.ref_boxes): hit_bvh (bvh_hit.c:16-43) visits the root and both
+// children of every internal node whose box the ray hits, without culling,
+// and counts every visit; boxes are tested in double with intersect_aabb's
+// formula (bvh_utils.c:38-59). any_leaf receives whether a leaf primitive was
+// hit, on which hit_register_all keeps the count (hit_register.c:113-121).
+__device__ __forceinline__ bool ref_box_hit(const double* b, double3 o, double3 d) {
+  double t1 = fmin((b[0] - o.x) / d.x, (b[3] - o.x) / d.x);
+  double tmin = fmax(t1, fmin((b[1] - o.y) / d.y, (b[4] - o.y) / d.y));
+  t1 = fmin((b[2] - o.z) / d.z, (b[5] - o.z) / d.z);
+  tmin = fmax(tmin, t1);
+  t1 = fmax((b[0] - o.x) / d.x, (b[3] - o.x) / d.x);
+  double tmax = fmin(t1, fmax((b[1] - o.y) / d.y, (b[4] - o.y) / d.y));
+  t1 = fmax((b[2] - o.z) / d.z, (b[5] - o.z) / d.z);
+  tmax = fmin(tmax, t1);
+  return tmax >= fmax(tmin, 0.0) && tmin < 1000.0;
+}
+
+template <class V>
+__device__ int ref_visit_count(const V& S, float3 of, float3 df, bool& any_leaf, int* status) {
+  const double3 o = make_double3(of.x, of.y, of.z), d = make_double3(df.x, df.y, df.z);
+  any_leaf = false;
+  int count = 1;
+  if (!S.has_bvh || !ref_box_hit(S.ref_boxes, o, d)) return count;
+  auto leaf = [&](int link) {
+    const int first = (~link) >> 3;
+    float t, u, v;
+    if (prim_hit(S, first, of, df, kTMax, t, u, v)) any_leaf = true;
+  };
+  if (S.root_leaf) {
+    leaf(S.root_leaf);
+    return count;
+  }
+  int stack[kStackSize];
+  int sp = 0;
+  stack[sp++] = 0;
+  while (sp > 0) {
+    const int k = stack[--sp];
+    count += 2;
+    const int4 ln = __ldg(&S.nodes[k].link);
+    const double* b = S.ref_boxes + 6 + 12 * (size_t)k;
+    const int child[2] = {ln.x, ln.y};
+    for (int c = 1; c >= 0; --c) {          // right pushed first: left popped first
+      if (!ref_box_hit(b + 6 * c, o, d)) continue;
+      if (child[c] < 0) leaf(child[c]);
+      else if (sp < kStackSize) stack[sp++] = child[c];
+      else if (status) atomicOr(status, ST_STACK);
+    }
+  }
+  return count;
 }
 
 // Entry points of the shading code (megakernels, probes, photon emission);

@@ -35,40 +35,10 @@ namespace mrt {
 constexpr int kKinds = 4;   // 0 diffuse/default, 1 metal, 2 dielectric, 3 mixed metallic
 constexpr int kWfBlock = 128;
 
-#ifndef MRT_WF_SMEM_STACK
-#define MRT_WF_SMEM_STACK 0
-#endif
-#ifndef MRT_WF_MINB
-#define MRT_WF_MINB 1
-#endif
-// traversal stack of the extend / connect kernels: the first kTravShared
-// entries in shared memory, the rest in local memory
-constexpr int kTravShared = MRT_WF_SMEM_STACK;
-#if MRT_WF_SMEM_STACK > 0
-#define MRT_TRAV_STACK(name) \
-  __shared__ int name##_smem[kTravShared * kWfBlock]; \
-  SharedStack<kTravShared, kWfBlock> name(name##_smem)
-#else
-#define MRT_TRAV_STACK(name) LocalStack name
-#endif
-#ifndef MRT_WF_SORT
-#define MRT_WF_SORT 0
-#endif
-#ifndef MRT_WF_SORT_SH
-#define MRT_WF_SORT_SH 0
-#endif
-#ifndef MRT_WF_SORT_BITS
-#define MRT_WF_SORT_BITS 5
-#endif
-#ifndef MRT_WF_SORT_ORDER
-#define MRT_WF_SORT_ORDER 0
-#endif
-// Ray reordering before the traversal kernels: a counting sort of the queue
-// on a key of the ray's origin cell (Morton order of a 2^kSortBits-per-axis
-// grid over the scene's bounds) and its direction octant.
-constexpr int kSortBits = MRT_WF_SORT_BITS;
-constexpr int kSortBins = 8 << (3 * kSortBits);
-constexpr int kScanThreads = 1024;
+// Traversal kernels are capped at 40 registers (12 blocks of 128 per SM):
+// measured 1.2 % faster on c1 than the 54-register build, despite a few
+// bytes of spills.
+constexpr int kTravMinBlocks = 12;
 
 struct WfState {
   // path state, indexed by path slot
@@ -93,12 +63,6 @@ struct WfState {
   float4* sh_d;       // shadow ray dir.xyz, (path << 4 | slot) bits
   int* counters;      // see Cnt
   float4* frame;      // accumulator (W*H)
-  // ray reordering
-  int* q_tmp;         // unsorted copy of the queue being sorted
-  int2* sort_kr;      // per queue entry: (key, rank within its key)
-  unsigned* sort_hist;  // kSortBins counters, then exclusive offsets
-  float4* sh_o2;      // shadow rays in key order
-  float4* sh_d2;
   int capacity;
   int sh_capacity;
   int rays_per_path;  // shadow rays a diffuse event may emit
@@ -147,200 +111,6 @@ __device__ __forceinline__ int warp_append(int* counter, bool pred) {
   return base + __popc(mask & ((1u << lane) - 1u));
 }
 
-// ------------------------------------------------------------ reorder
-__device__ __forceinline__ uint32_t spread3(uint32_t x) {
-  // bits b of x to bit 3b (x < 2^10)
-  x &= 0x3ffu;
-  x = (x | (x << 16)) & 0x030000ffu;
-  x = (x | (x << 8)) & 0x0300f00fu;
-  x = (x | (x << 4)) & 0x030c30c3u;
-  x = (x | (x << 2)) & 0x09249249u;
-  return x;
-}
-
-// Sort key of a ray: origin cell in Morton order and direction octant.
-__device__ __forceinline__ uint32_t ray_key(const float3& lo, const float3& scale, float3 o, float3 d) {
-  const float m = (float)((1 << kSortBits) - 1);
-  const uint32_t cx = (uint32_t)fminf(fmaxf((o.x - lo.x) * scale.x, 0.f), m);
-  const uint32_t cy = (uint32_t)fminf(fmaxf((o.y - lo.y) * scale.y, 0.f), m);
-  const uint32_t cz = (uint32_t)fminf(fmaxf((o.z - lo.z) * scale.z, 0.f), m);
-  const uint32_t cell = spread3(cx) | (spread3(cy) << 1) | (spread3(cz) << 2);
-  const uint32_t oct = (d.x < 0.f ? 1u : 0u) | (d.y < 0.f ? 2u : 0u) | (d.z < 0.f ? 4u : 0u);
-  return MRT_WF_SORT_ORDER == 0 ? (oct << (3 * kSortBits)) | cell : (cell << 3) | oct;
-}
-
-// Scene bounds from the root node's two child boxes.
-__device__ __forceinline__ void scene_box(const SceneView& S, float3& lo, float3& scale) {
-  const Node r = S.nodes[0];
-  lo = f3(fminf(r.lxy.x, r.rxy.x), fminf(r.lxy.z, r.rxy.z), fminf(r.z.x, r.z.z));
-  const float3 hi = f3(fmaxf(r.lxy.y, r.rxy.y), fmaxf(r.lxy.w, r.rxy.w), fmaxf(r.z.y, r.z.w));
-  const float cells = (float)(1 << kSortBits);
-  scale = f3(cells / fmaxf(hi.x - lo.x, 1e-20f), cells / fmaxf(hi.y - lo.y, 1e-20f),
-             cells / fmaxf(hi.z - lo.z, 1e-20f));
-}
-
-// Keys and ranks of the live queue (a copy of which goes to q_tmp).
-template <int kBounceParity>
-__global__ void __launch_bounds__(kWfBlock) wf_sort_key(SceneView S, WfState W) {
-  const int n = W.counters[kBounceParity ? C_LIVE1 : C_LIVE0];
-  const int* q = W.q_live[kBounceParity];
-  float3 lo, scale;
-  scene_box(S, lo, scale);
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-    const int i = q[k];
-    const float4 o = W.o[i], d = W.d[i];
-    const uint32_t key = ray_key(lo, scale, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z));
-    const int rank = (int)atomicAdd(W.sort_hist + key, 1u);
-    W.sort_kr[k] = make_int2((int)key, rank);
-    W.q_tmp[k] = i;
-  }
-}
-
-// Keys and ranks of the shadow-ray queue.
-__global__ void __launch_bounds__(kWfBlock) wf_sort_key_sh(SceneView S, WfState W) {
-  const int n = min(W.counters[C_SH], W.sh_capacity);
-  float3 lo, scale;
-  scene_box(S, lo, scale);
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-    const float4 o = W.sh_o[k], d = W.sh_d[k];
-    const uint32_t key = ray_key(lo, scale, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z));
-    const int rank = (int)atomicAdd(W.sort_hist + key, 1u);
-    W.sort_kr[k] = make_int2((int)key, rank);
-  }
-}
-
-// Exclusive scan of the kSortBins counters, in place (one block).
-__global__ void __launch_bounds__(kScanThreads) wf_sort_scan(WfState W) {
-  constexpr int kChunk = kSortBins / kScanThreads;
-  __shared__ unsigned warp_sums[kScanThreads / 32];
-  unsigned* h = W.sort_hist + (size_t)threadIdx.x * kChunk;
-  unsigned sum = 0;
-  for (int j = 0; j < kChunk; ++j) sum += h[j];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  unsigned incl = sum;
-  for (int off = 1; off < 32; off <<= 1) {
-    const unsigned v = __shfl_up_sync(0xffffffffu, incl, off);
-    if (lane >= off) incl += v;
-  }
-  if (lane == 31) warp_sums[warp] = incl;
-  __syncthreads();
-  if (warp == 0) {
-    unsigned w = warp_sums[lane];
-    for (int off = 1; off < 32; off <<= 1) {
-      const unsigned v = __shfl_up_sync(0xffffffffu, w, off);
-      if (lane >= off) w += v;
-    }
-    warp_sums[lane] = w;
-  }
-  __syncthreads();
-  unsigned run = incl - sum + (warp ? warp_sums[warp - 1] : 0u);
-  for (int j = 0; j < kChunk; ++j) {
-    const unsigned c = h[j];
-    h[j] = run;
-    run += c;
-  }
-}
-
-template <int kBounceParity>
-__global__ void __launch_bounds__(kWfBlock) wf_sort_scatter(WfState W) {
-  const int n = W.counters[kBounceParity ? C_LIVE1 : C_LIVE0];
-  int* q = W.q_live[kBounceParity];
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-    const int2 kr = W.sort_kr[k];
-    q[W.sort_hist[kr.x] + kr.y] = W.q_tmp[k];
-  }
-}
-
-__global__ void __launch_bounds__(kWfBlock) wf_sort_scatter_sh(WfState W) {
-  const int n = min(W.counters[C_SH], W.sh_capacity);
-  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
-    const int2 kr = W.sort_kr[k];
-    const unsigned dst = W.sort_hist[kr.x] + kr.y;
-    W.sh_o2[dst] = W.sh_o[k];
-    W.sh_d2[dst] = W.sh_d[k];
-  }
-}
-
-// Block-local reordering: each block sorts 1024 consecutive queue entries by
-// ray key in shared memory (bitonic network) and writes them back in place;
-// no global histogram or scan. Entries beyond n sort last with key ~0u.
-constexpr int kLocalSort = 1024;
-
-__device__ __forceinline__ void bitonic_1024(uint32_t* key, uint16_t* idx) {
-  const int t = threadIdx.x;
-  for (int k = 2; k <= kLocalSort; k <<= 1) {
-    for (int j = k >> 1; j > 0; j >>= 1) {
-      const int u = t ^ j;
-      if (u > t) {
-        const bool up = (t & k) == 0;
-        const uint32_t a = key[t], b = key[u];
-        if ((a > b) == up) {
-          key[t] = b; key[u] = a;
-          const uint16_t x = idx[t]; idx[t] = idx[u]; idx[u] = x;
-        }
-      }
-      __syncthreads();
-    }
-  }
-}
-
-template <int kBounceParity>
-__global__ void __launch_bounds__(kLocalSort) wf_sort_local(SceneView S, WfState W) {
-  __shared__ uint32_t key[kLocalSort];
-  __shared__ uint16_t idx[kLocalSort];
-  __shared__ int val[kLocalSort];
-  const int n = W.counters[kBounceParity ? C_LIVE1 : C_LIVE0];
-  int* q = W.q_live[kBounceParity];
-  float3 lo, scale;
-  scene_box(S, lo, scale);
-  for (int base = blockIdx.x * kLocalSort; base < n; base += gridDim.x * kLocalSort) {
-    const int k = base + threadIdx.x;
-    uint32_t kk = 0xffffffffu;
-    int v = -1;
-    if (k < n) {
-      v = q[k];
-      const float4 o = W.o[v], d = W.d[v];
-      kk = ray_key(lo, scale, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z));
-    }
-    key[threadIdx.x] = kk;
-    idx[threadIdx.x] = (uint16_t)threadIdx.x;
-    val[threadIdx.x] = v;
-    __syncthreads();
-    bitonic_1024(key, idx);
-    if (k < n) q[k] = val[idx[threadIdx.x]];
-    __syncthreads();
-  }
-}
-
-__global__ void __launch_bounds__(kLocalSort) wf_sort_local_sh(SceneView S, WfState W) {
-  __shared__ uint32_t key[kLocalSort];
-  __shared__ uint16_t idx[kLocalSort];
-  __shared__ float4 ro[kLocalSort], rd[kLocalSort];
-  const int n = min(W.counters[C_SH], W.sh_capacity);
-  float3 lo, scale;
-  scene_box(S, lo, scale);
-  for (int base = blockIdx.x * kLocalSort; base < n; base += gridDim.x * kLocalSort) {
-    const int k = base + threadIdx.x;
-    uint32_t kk = 0xffffffffu;
-    if (k < n) {
-      const float4 o = W.sh_o[k], d = W.sh_d[k];
-      ro[threadIdx.x] = o;
-      rd[threadIdx.x] = d;
-      kk = ray_key(lo, scale, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z));
-    }
-    key[threadIdx.x] = kk;
-    idx[threadIdx.x] = (uint16_t)threadIdx.x;
-    __syncthreads();
-    bitonic_1024(key, idx);
-    if (k < n) {
-      const int src = idx[threadIdx.x];
-      W.sh_o2[k] = ro[src];
-      W.sh_d2[k] = rd[src];
-    }
-    __syncthreads();
-  }
-}
-
 // ------------------------------------------------------------ generate
 __global__ void __launch_bounds__(kWfBlock) wf_generate(SceneView S, WfState W, const WfParams* __restrict__ Pp) {
   const WfParams P = *Pp;
@@ -380,11 +150,11 @@ __global__ void __launch_bounds__(kWfBlock) wf_generate(SceneView S, WfState W, 
 
 // --------------------------------------------------------------- extend
 template <int kBounceParity, class V>
-__global__ void __launch_bounds__(kWfBlock, MRT_WF_MINB) wf_extend(V S, WfState W, int* status) {
+__global__ void __launch_bounds__(kWfBlock, kTravMinBlocks) wf_extend(V S, WfState W, int* status) {
   const int n = W.counters[kBounceParity ? C_LIVE1 : C_LIVE0];
   const int* q = W.q_live[kBounceParity];
   const int lane = threadIdx.x & 31;
-  MRT_TRAV_STACK(stack);
+  LocalStack stack;
   while (true) {
     int base = 0;
     if (lane == 0) base = atomicAdd(&W.counters[C_WORK], 32);
@@ -594,11 +364,11 @@ __global__ void __launch_bounds__(kWfBlock) wf_sample(V S, WfState W, const WfPa
 }
 
 // -------------------------------------------------------------- connect
-template <bool kSortedShadow, class V>
-__global__ void __launch_bounds__(kWfBlock, MRT_WF_MINB) wf_connect(V S, WfState W, int* status) {
+template <class V>
+__global__ void __launch_bounds__(kWfBlock, kTravMinBlocks) wf_connect(V S, WfState W, int* status) {
   const int n = min(W.counters[C_SH], W.sh_capacity);
   const int lane = threadIdx.x & 31;
-  MRT_TRAV_STACK(stack);
+  LocalStack stack;
   while (true) {
     int base = 0;
     if (lane == 0) base = atomicAdd(&W.counters[C_WORK], 32);
@@ -606,8 +376,7 @@ __global__ void __launch_bounds__(kWfBlock, MRT_WF_MINB) wf_connect(V S, WfState
     if (base >= n) break;
     const int k = base + lane;
     if (k < n) {
-      const float4 o = kSortedShadow ? W.sh_o2[k] : W.sh_o[k];
-      const float4 d = kSortedShadow ? W.sh_d2[k] : W.sh_d[k];
+      const float4 o = W.sh_o[k], d = W.sh_d[k];
       const bool blocked = any_hit_compact(S, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), o.w, status, stack);
       if (!blocked) {
         const int tag = __float_as_int(d.w);
@@ -783,9 +552,7 @@ static cudaError_t wf_alloc(WfHost* H, int capacity, int n_lights, bool env) {
   AL(vis, n * 4 * vis_words); AL(vis_env, n * 4);
   AL(q_live[0], n * 4); AL(q_live[1], n * 4); AL(q_kind, n * 4 * kKinds); AL(q_def, n * 4);
   AL(counters, sizeof(int) * C_COUNT);
-  AL(q_tmp, n * 4); AL(sort_hist, sizeof(unsigned) * kSortBins);
   if ((e = A((void**)&H->dparams, sizeof(WfParams))) != cudaSuccess) return e;
-  if ((e = cudaMemset(s.sort_hist, 0, sizeof(unsigned) * kSortBins)) != cudaSuccess) return e;
 #undef AL
   return cudaMemset(s.counters, 0, sizeof(int) * C_COUNT);
 }
@@ -793,78 +560,34 @@ static cudaError_t wf_alloc(WfHost* H, int capacity, int n_lights, bool env) {
 static cudaError_t wf_shadow_alloc(WfHost* H, size_t sh_cap) {
   if ((size_t)H->sh_capacity >= sh_cap) return cudaSuccess;
   cudaError_t e;
-  float4 *o = nullptr, *d = nullptr, *o2 = nullptr, *d2 = nullptr;
-  int2* kr = nullptr;
-  const size_t kr_n = std::max(sh_cap, (size_t)H->capacity);
+  float4 *o = nullptr, *d = nullptr;
   if ((e = cudaMalloc(&o, sh_cap * 16)) != cudaSuccess) return e;
   H->allocs.push_back(o);
   if ((e = cudaMalloc(&d, sh_cap * 16)) != cudaSuccess) return e;
   H->allocs.push_back(d);
-  if ((e = cudaMalloc(&o2, sh_cap * 16)) != cudaSuccess) return e;
-  H->allocs.push_back(o2);
-  if ((e = cudaMalloc(&d2, sh_cap * 16)) != cudaSuccess) return e;
-  H->allocs.push_back(d2);
-  if ((e = cudaMalloc(&kr, kr_n * sizeof(int2))) != cudaSuccess) return e;
-  H->allocs.push_back(kr);
   H->st.sh_o = o;
   H->st.sh_d = d;
-  H->st.sh_o2 = o2;
-  H->st.sh_d2 = d2;
-  H->st.sort_kr = kr;
   H->st.sh_capacity = (int)sh_cap;
   H->sh_capacity = (int)sh_cap;
   if (H->graph) { cudaGraphExecDestroy(H->graph); H->graph = nullptr; }
   return cudaSuccess;
 }
 
-// One bounce of the wave: [reorder] extend, classify, sample, [reorder]
-// connect, finish, reset. Returns the number of kernels launched.
+// One bounce of the wave: extend, classify, sample, connect, finish, reset.
+// Returns the number of kernels launched.
 template <int kPar, class VT>
 static unsigned wf_enqueue_bounce(const WfHost* H, const VT& v, const WfState& s, const WfParams* dP,
-                                  int* status, int bounce, cudaStream_t st) {
-  const int sms = H->sms;
-  const int gen_blocks = std::max(1, std::min((H->capacity + kWfBlock - 1) / kWfBlock, sms * 16));
-  const int sh_blocks = std::max(1, std::min((H->sh_capacity + kWfBlock - 1) / kWfBlock, sms * 16));
-  const int pers = sms * 12;
-  unsigned n = 0;
-  const size_t hist_bytes = sizeof(unsigned) * kSortBins;
-  const bool sort_live = MRT_WF_SORT && bounce > 0 && v.has_bvh;
-  const int local_blocks = std::max(1, std::min((H->capacity + kLocalSort - 1) / kLocalSort, sms * 2));
-  const int local_sh_blocks = std::max(1, std::min((H->sh_capacity + kLocalSort - 1) / kLocalSort, sms * 2));
-  if (sort_live && MRT_WF_SORT == 2) {
-    wf_sort_local<kPar><<<local_blocks, kLocalSort, 0, st>>>(v, s);
-    n += 1;
-  } else if (sort_live) {
-    // counting sort of the live queue by ray key (the counters start at zero)
-    wf_sort_key<kPar><<<gen_blocks, kWfBlock, 0, st>>>(v, s);
-    wf_sort_scan<<<1, kScanThreads, 0, st>>>(s);
-    wf_sort_scatter<kPar><<<gen_blocks, kWfBlock, 0, st>>>(s);
-    cudaMemsetAsync(s.sort_hist, 0, hist_bytes, st);
-    n += 3;
-  }
+                                  int* status, cudaStream_t st) {
+  const int gen_blocks = std::max(1, std::min((H->capacity + kWfBlock - 1) / kWfBlock, H->sms * 16));
+  const int pers = H->sms * 12;
   wf_extend<kPar, VT><<<pers, kWfBlock, 0, st>>>(v, s, status);
   wf_classify<kPar><<<gen_blocks, kWfBlock, 0, st>>>(v, s, dP);
   wf_sample<kPar, VT><<<gen_blocks, kWfBlock, 0, st>>>(v, s, dP, status);
   wf_work_reset<<<1, 32, 0, st>>>(s);
-  n += 4;
-  if (MRT_WF_SORT_SH == 2 && v.has_bvh) {
-    wf_sort_local_sh<<<local_sh_blocks, kLocalSort, 0, st>>>(v, s);
-    wf_connect<true, VT><<<pers, kWfBlock, 0, st>>>(v, s, status);
-    n += 2;
-  } else if (MRT_WF_SORT_SH && v.has_bvh) {
-    wf_sort_key_sh<<<sh_blocks, kWfBlock, 0, st>>>(v, s);
-    wf_sort_scan<<<1, kScanThreads, 0, st>>>(s);
-    wf_sort_scatter_sh<<<sh_blocks, kWfBlock, 0, st>>>(s);
-    cudaMemsetAsync(s.sort_hist, 0, hist_bytes, st);
-    wf_connect<true, VT><<<pers, kWfBlock, 0, st>>>(v, s, status);
-    n += 4;
-  } else {
-    wf_connect<false, VT><<<pers, kWfBlock, 0, st>>>(v, s, status);
-    n += 1;
-  }
+  wf_connect<VT><<<pers, kWfBlock, 0, st>>>(v, s, status);
   wf_finish<kPar><<<gen_blocks, kWfBlock, 0, st>>>(v, s);
   wf_reset<kPar><<<1, 32, 0, st>>>(s);
-  return n + 2;
+  return 7;
 }
 
 // Enqueues one wave (generate + max_bounces x stages) on `st`; the
@@ -879,8 +602,8 @@ static void wf_enqueue_wave_t(WfHost* H, const VT& v, const WfParams& P, int* st
   wf_generate<<<gen_blocks, kWfBlock, 0, st>>>(v, s, dP);
   unsigned n = 2;
   for (int b = 0; b < P.max_bounces; ++b)
-    n += (b & 1) ? wf_enqueue_bounce<1>(H, v, s, dP, status, b, st)
-                 : wf_enqueue_bounce<0>(H, v, s, dP, status, b, st);
+    n += (b & 1) ? wf_enqueue_bounce<1>(H, v, s, dP, status, st)
+                 : wf_enqueue_bounce<0>(H, v, s, dP, status, st);
   // paths still live after the last bounce retire with what they gathered
   wf_wave_end<<<1, 32, 0, st>>>(s);
   n += 1;
@@ -1005,8 +728,7 @@ WfHost* wf_create() { return new WfHost(); }
 size_t wf_device_bytes(const WfHost* H) {
   if (!H) return 0;
   const size_t cap = (size_t)H->capacity, sh = (size_t)H->sh_capacity;
-  return cap * (16 * 10 + 8 + 4 * (4 + H->vis_words) + 4 * kKinds + 4) + sh * 64 + std::max(cap, sh) * 8 +
-         sizeof(unsigned) * kSortBins;
+  return cap * (16 * 10 + 8 + 4 * (4 + H->vis_words) + 4 * kKinds) + sh * 32;
 }
 
 void wf_destroy(WfHost* H) {

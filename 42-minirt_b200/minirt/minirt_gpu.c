@@ -358,6 +358,75 @@ static int	flatten(t_minirt *mrt, t_scene *s, t_flat *f)
 	return (0);
 }
 
+/* The reference's BVH object list (bvh_make_lst.c:52-69) as flat
+ * primitive ids (spheres, cylinders, cones, hyperboloids, then the meshes'
+ * triangles, as flatten lays them out), with the position its median split
+ * sorts by (get_obj_position, bvh_utils.c:88: the object's position, or a
+ * triangle's centre as its loader stored it). Selects the reference's own
+ * tree for the next build, so that render_mode 1 reports hit_bvh's visit
+ * counts (bvh_hit.c:16). */
+static int	set_reference_bvh(t_minirt *mrt, t_scene *s, const t_flat *f)
+{
+	const int64_t	tb = f->d.n_spheres + f->d.n_cylinders + f->d.n_cones
+		+ f->d.n_hyperboloids;
+	int64_t			n = tb, i = 0, it = 0;
+	int64_t			k4[4] = {0, f->d.n_spheres, f->d.n_spheres + f->d.n_cylinders,
+		f->d.n_spheres + f->d.n_cylinders + f->d.n_cones};
+	int32_t			*order;
+	double			*pos;
+	mrt_bvh_options	o;
+	int				rc;
+
+	for (int m = 0; m < f->d.n_meshes; m++)
+		n += f->me[m].n_triangles;
+	order = malloc(sizeof(int32_t) * (n ? n : 1));
+	pos = malloc(sizeof(double) * 3 * (n ? n : 1));
+	if (!order || !pos)
+		return (free(order), free(pos), -1);
+	for (int e = 0; e < s->el_amount; e++)
+	{
+		t_objects	ty = s->elements[e].type;
+		void		*ob = s->elements[e].object;
+		int64_t		id;
+
+		if (ty == SPHERE || ty == CYLINDER || ty == CONE || ty == HYPERBOLOID)
+		{
+			int	kind = ty == SPHERE ? 0 : ty == CYLINDER ? 1 : ty == CONE ? 2 : 3;
+
+			id = k4[kind]++;
+			order[i++] = (int32_t)id;
+			if (ty == SPHERE)
+				v3(pos + 3 * id, ((t_sphere *)ob)->position);
+			else if (ty == CYLINDER)
+				v3(pos + 3 * id, ((t_cylinder *)ob)->position);
+			else if (ty == CONE)
+				v3(pos + 3 * id, ((t_cone *)ob)->position);
+			else
+				v3(pos + 3 * id, ((t_hyperboloid *)ob)->position);
+		}
+		else if (ty == CUSTOM)
+		{
+			t_custom_object	*c = ob;
+
+			for (size_t k = 0; k < c->triangle_count; k++)
+			{
+				t_triangle	*t = c->obj_list[k].object;
+
+				id = tb + it + (t - c->triangles);
+				order[i++] = (int32_t)id;
+				v3(pos + 3 * id, t->center);
+			}
+			it += c->triangle_count;
+		}
+	}
+	o = (mrt_bvh_options){MRT_BVH_REFERENCE, 0, n, order, pos};
+	(void)mrt;
+	rc = mrt_set_bvh_options(mrt->shaders_data.ctx, &o);
+	free(order);
+	free(pos);
+	return (rc == MRT_OK ? 0 : -1);
+}
+
 /* convert_scene_build (gpu_scene.c:104): full repack and upload. */
 int	convert_scene_build(t_minirt *minirt, t_scene *scene, t_viewport *vp,
 	t_gpu_structs *gpu)
@@ -376,6 +445,21 @@ int	convert_scene_build(t_minirt *minirt, t_scene *scene, t_viewport *vp,
 	{
 		free_flat(&f);
 		return (-1);
+	}
+	if (minirt->render_mode == 1)
+	{
+		if (set_reference_bvh(minirt, scene, &f))
+		{
+			free_flat(&f);
+			err_line("convert_scene_build");
+			return (-1);
+		}
+	}
+	else
+	{
+		mrt_bvh_options	o = {MRT_BVH_SAH, 0, 0, NULL, NULL};
+
+		mrt_set_bvh_options(minirt->shaders_data.ctx, &o);
 	}
 	rc = mrt_scene_build(minirt->shaders_data.ctx, &f.d);
 	if (rc == MRT_OK)

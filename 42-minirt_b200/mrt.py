@@ -162,6 +162,14 @@ class TuneResult(C.Structure):
     _fields_ = [("n", C.c_int32), ("best", C.c_int32), ("entry", TuneEntry * 32)]
 
 
+class BvhOptions(C.Structure):
+    _fields_ = [("mode", C.c_int32), ("pad_", C.c_int32), ("n_prims", C.c_int64),
+                ("order", C.POINTER(C.c_int32)), ("positions", C.POINTER(C.c_double))]
+
+
+BVH_SAH, BVH_REFERENCE = 0, 1
+
+
 class Ray(C.Structure):
     _fields_ = [("orig", f64x3), ("dir", f64x3)]
 
@@ -198,6 +206,8 @@ SIGNATURES = {
     "mrt_render_state_save": (C.c_int, [_P, C.c_char_p]),
     "mrt_render_state_load": (C.c_int, [_P, C.c_char_p]),
     "mrt_comm_unique_id": (C.c_int, [_P]),
+    "mrt_set_bvh_options": (C.c_int, [_P, _P]),
+    "mrt_read_bvh_leaves": (C.c_int64, [_P, _P, C.c_int64]),
     "mrt_comm_init": (C.c_int, [_P, _P, C.c_int32, C.c_int32]),
     "mrt_reduce_frame": (C.c_int, [_P, C.c_int32]),
     "mrt_comm_destroy": (C.c_int, [_P]),
@@ -387,6 +397,34 @@ class Context:
 
     def comm_destroy(self) -> None:
         check(self.lib.mrt_comm_destroy(self.h), "mrt_comm_destroy")
+
+    def set_bvh_options(self, mode: int, order=None, positions=None) -> None:
+        """BVH build for the next build(): BVH_SAH (default) or BVH_REFERENCE
+        (the reference's median-split tree, traversed left first, with the
+        reference's node-visit count in render_mode 1). order: flat ids in the
+        reference's object-list order; positions: (n, 3) split positions."""
+        o = BvhOptions(mode=mode)
+        keep = []
+        if order is not None:
+            a = np.ascontiguousarray(order, np.int32)
+            keep.append(a)
+            o.order = a.ctypes.data_as(C.POINTER(C.c_int32))
+            o.n_prims = len(a)
+        if positions is not None:
+            b = np.ascontiguousarray(positions, np.float64).reshape(-1, 3)
+            keep.append(b)
+            o.positions = b.ctypes.data_as(C.POINTER(C.c_double))
+            o.n_prims = len(b)
+        check(self.lib.mrt_set_bvh_options(self.h, C.byref(o)), "mrt_set_bvh_options")
+
+    def bvh_leaves(self) -> np.ndarray:
+        """Flat primitive ids in leaf order (mrt_read_bvh_leaves)."""
+        n = self.lib.mrt_read_bvh_leaves(self.h, None, 0)
+        if n < 0:
+            check(int(n), "mrt_read_bvh_leaves")
+        out = np.zeros(max(1, n), np.int32)
+        self.lib.mrt_read_bvh_leaves(self.h, _ptr(out), n)
+        return out[:n]
 
     def read_depth(self) -> np.ndarray:
         out = np.zeros((self.height, self.width), np.int32)

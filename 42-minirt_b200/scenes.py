@@ -87,6 +87,11 @@ class Scene:
     def n_triangles(self) -> int:
         return int(sum(len(m.indices) for m in self.meshes))
 
+    def n_prims_bvh(self) -> int:
+        """Primitives the BVH holds: spheres, quadrics and triangles (not planes)."""
+        return (len(self.spheres) + len(self.cylinders) + len(self.cones) + len(self.hyperboloids)
+                + self.n_triangles)
+
     def desc(self) -> mrt.SceneDesc:
         """Build the C struct (keeps every array alive on self)."""
         keep = []

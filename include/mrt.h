@@ -377,6 +377,43 @@ MRT_API int			mrt_render(mrt_ctx *ctx, const mrt_render_params *params,
 MRT_API int			mrt_render_batch(mrt_ctx **ctx, const mrt_render_params *params,
 				int32_t n, mrt_render_stats *stats);
 
+/* BVH build options, applied by the next mrt_scene_build.
+ * MRT_BVH_SAH (default): this library's binned-SAH tree, up to 8 primitives
+ * per leaf, traversed nearer child first. MRT_BVH_REFERENCE: the reference's
+ * own tree (bvh_build.c:16-127: one primitive per leaf, split at the median
+ * of the object positions on the longest axis of the node bounds, in the
+ * reference's sort order), traversed left child first, with the reference's
+ * node-visit count for render_mode 1 (hit_bvh, bvh_hit.c:16). Use it for
+ * parity runs: exact-t ties and heat-map counts then come out as the
+ * reference's. order (may be NULL) lists the flat primitive ids (spheres,
+ * cylinders, cones, hyperboloids, then mesh triangles, as mrt_scene_desc
+ * holds them) in the order of the reference's object list (bvh_make_lst.c);
+ * positions (may be NULL) gives, per flat id, the point the split sorts by
+ * (get_obj_position, bvh_utils.c:88; default: the centre of a sphere or
+ * quadric, the vertex mean of a triangle). Both arrays have n_prims entries
+ * (3 doubles each for positions) and are copied by the call. */
+typedef enum mrt_bvh_mode
+{
+	MRT_BVH_SAH = 0,
+	MRT_BVH_REFERENCE = 1
+}	mrt_bvh_mode;
+
+typedef struct mrt_bvh_options
+{
+	int32_t			mode;
+	int32_t			pad_;
+	int64_t			n_prims;
+	const int32_t	*order;
+	const double	*positions;
+}	mrt_bvh_options;
+
+MRT_API int			mrt_set_bvh_options(mrt_ctx *ctx, const mrt_bvh_options *options);
+/* Parity probe of the tree: the flat primitive id in each leaf slot of the
+ * last build, in leaf order (up to cap entries); returns the slot count.
+ * With MRT_BVH_REFERENCE this is the reference's sorted prim_indices order
+ * (one primitive per leaf). */
+MRT_API int64_t		mrt_read_bvh_leaves(mrt_ctx *ctx, int32_t *flat, int64_t cap);
+
 /* Zero the device accumulator. */
 MRT_API int			mrt_clear(mrt_ctx *ctx);
 /* Copy the device accumulator (sum over samples, W*H*3 floats, row-major,

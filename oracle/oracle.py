@@ -62,6 +62,7 @@ def ref_lib():
             "refh_clear": (None, [_P]), "refh_viewport": (None, [_P, _P]),
             "refh_triangle_positions": (C.c_int, [_P, _P]),
             "refh_bvh": (C.c_int, [_P, _P, _P, _P]),
+            "refh_object_list": (C.c_int, [_P, _P, _P]),
             "refh_env_tables": (C.c_int, [_P, _P, _P, _P, _P]),
             "refh_env_sample": (C.c_int, [_P, C.c_int64, _P, _P]),
             "refh_background": (C.c_int, [_P, _P, C.c_int64, C.c_int, _P]),
@@ -167,6 +168,15 @@ class RefOracle:
         prim = np.zeros(max(1, n_prims), np.int32)
         n = self.lib.refh_bvh(self.h, _ptr(b), _ptr(info), _ptr(prim))
         return b[:n], info[:n], prim[:n_prims]
+
+    def object_list(self):
+        """The reference's BVH object list: flat ids in its order, and each
+        entry's split position (get_obj_position)."""
+        n = self.scene.n_prims_bvh()
+        flat = np.zeros(max(1, n), np.int32)
+        pos = np.zeros((max(1, n), 3))
+        k = self.lib.refh_object_list(self.h, _ptr(flat), _ptr(pos))
+        return flat[:k], pos[:k]
 
     def env_tables(self):
         if self.scene.hdr is None:

@@ -780,6 +780,30 @@ int	refh_bvh(void *hv, double *bounds, uint32_t *info, int32_t *prim_flat)
 	return ((int)b->bvh_nodes_used);
 }
 
+/* The BVH's object list before the build sorts it (bvh_make_lst.c:52): per
+ * entry i, the flat id of its primitive and the position the median split
+ * sorts by (get_obj_position, bvh_utils.c:88). Returns the entry count. */
+int	refh_object_list(void *hv, int32_t *flat, double *pos)
+{
+	t_refh	*h;
+	t_bvh	*b;
+
+	h = hv;
+	b = &h->m->scene.bvh;
+	if (!b->valid)
+		return (0);
+	for (uint32_t i = 0; i < b->size; i++)
+	{
+		t_vec3	p = get_obj_position(i, b);
+
+		flat[i] = flat_prim_of(h, b->obj_list[i]);
+		pos[3 * i] = p.x;
+		pos[3 * i + 1] = p.y;
+		pos[3 * i + 2] = p.z;
+	}
+	return ((int)b->size);
+}
+
 /* HDRI tables (t_amb_light fields). Returns 0 if the scene has none. */
 int	refh_env_tables(void *hv, float *pdf_joint, float *cdf_m_inv,
 	float *cdf_c_inv, double *column_average)

@@ -124,7 +124,9 @@ def test_forward_matches_render_with_sky(c4ctx, mrt):
     ctx.render(8, seed=5, form=mrt.FORM_MEGAKERNEL, env_sampler=1)
     acc, _ = ctx.read_accum()
     ref = acc / 8.0
-    assert np.mean(img == ref) > 0.8
+    # fixed-point pixel sums (forward) against float atomic sums (render)
+    close = np.abs(img - ref) <= 2e-6 * np.maximum(np.abs(ref), 1e-3)
+    assert close.mean() > 0.999, close.mean()
     assert np.abs(img - ref).mean() <= 1e-6 * np.abs(ref).mean()
 
 
@@ -284,7 +286,7 @@ def test_roughness_gradient_matches_fd_crn(mrt, scenes, oracle):
     ctx = mrt.Context(64, 64)
     ctx.build(oracle.canonical_scene(sc))
     th = ctx.diff_params()
-    M, seed, spp = len(sc.materials), 5, 16
+    M, seed, spp = len(sc.materials), 5, 64
     rng = np.random.default_rng(2)
     thp = th.copy()
     thp[:5 * M] *= (1 + 0.2 * rng.uniform(-1, 1, 5 * M)).astype(np.float32)
@@ -314,7 +316,8 @@ def test_roughness_gradient_matches_fd_crn(mrt, scenes, oracle):
         checked += 1
         if abs(g[i] - f2) > 1e-2 * abs(f2) + 2e-5 * scale:
             bad.append((i - 3 * M, g[i], f1, f2))
-    print(f"roughness: {len(idx)} materials with a gradient, {checked} checked, mismatches {bad}")
+    print(f"roughness: {len(idx)} materials with a gradient, {checked} checked, mismatches {bad}; "
+          + ", ".join(f"m{i - 3 * M}: ad {g[i]:.4g} fd {fd[(1e-3, i)]:.4g} / {fd[(5e-4, i)]:.4g}" for i in idx))
     assert checked >= max(3, len(idx) // 2), (checked, len(idx))
     assert not bad, bad
     ctx.close()
