@@ -183,7 +183,15 @@ struct mrt_ctx {
   std::vector<double> bvh_pos;           // positions the reference's split sorts by, empty = computed
   DevBuf<double> ref_boxes;
   std::vector<uint32_t> leaf_order;      // flat primitive id of each leaf slot (last build)
+  // mrt_render_batch (when this context leads a batch): device arrays of the
+  // megakernel groups per view type, and the streams the batch's jobs use
+  DevBuf<SceneView> batch_views[3];
+  DevBuf<BatchItem> batch_items[3];
+  cudaStream_t batch_stream[4] = {};
+  cudaEvent_t batch_event[4] = {};
 };
+
+constexpr int kBatchStreams = 4;
 
 namespace {
 
@@ -400,6 +408,11 @@ void mrt_destroy(mrt_ctx* c) {
   nccl_comm_destroy(c->comm);
   c->comm_count.release();
   if (c->diff) { c->diff->release(); delete c->diff; }
+  for (int k = 0; k < 3; ++k) { c->batch_views[k].release(); c->batch_items[k].release(); }
+  for (int k = 0; k < kBatchStreams; ++k) {
+    if (c->batch_stream[k]) cudaStreamDestroy(c->batch_stream[k]);
+    if (c->batch_event[k]) cudaEventDestroy(c->batch_event[k]);
+  }
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   if (c->stream) cudaStreamDestroy(c->stream);
@@ -1089,10 +1102,6 @@ extern "C" int mrt_render(mrt_ctx* c, const mrt_render_params* p, mrt_render_sta
   const int block_size = p->block_size ? p->block_size : (tuned ? c->auto_block : 0);
   const int queue_capacity = p->queue_capacity ? p->queue_capacity : (tuned ? c->auto_capacity : 0);
   const int sort_threshold = p->sort_threshold ? p->sort_threshold : (tuned ? c->auto_sort : 0);
-  if (form == MRT_FORM_WAVEFRONT && v.has_textures) {
-    if (!tuned) return set_err(MRT_ERR_INVALID, "textured scenes render with the megakernel forms");
-    form = MRT_FORM_MEGAKERNEL;
-  }
   if (form == MRT_FORM_WAVEFRONT && p->render_mode == 0) {
     L.sample_base = (uint32_t)p->sample_base;
     if (!c->wf) c->wf = wf_create();
@@ -1158,64 +1167,138 @@ extern "C" int mrt_render_batch(mrt_ctx** ctxs, const mrt_render_params* params,
                      ctxs[0]->device);
     if (params[i].spp < 0 || params[i].sample_base < 0 || params[i].offset || params[i].render_mode != 0)
       return set_err(MRT_ERR_INVALID, "batch entry %d: spp / sample_base / offset / render_mode", i);
+    if (params[i].form < 0 || params[i].form > 3) return set_err(MRT_ERR_INVALID, "batch entry %d: form", i);
+    for (int j = 0; j < i; ++j)
+      if (ctxs[j] == ctxs[i]) return set_err(MRT_ERR_INVALID, "batch entry %d repeats entry %d", i, j);
   }
   mrt_ctx* c0 = ctxs[0];
   int rc = check_ctx(c0);
   if (rc) return rc;
   if (params[0].block_size && (params[0].block_size % 32 || params[0].block_size > 256))
     return set_err(MRT_ERR_INVALID, "block_size %d", params[0].block_size);
-  // longest-first order by predicted cost
-  std::vector<int> order(n);
+  // each scene's form: its own, or its tuned choice (FORM_AUTO); textured
+  // scenes render with the megakernel
+  std::vector<int> form(n);
   std::vector<double> cost(n);
   for (int i = 0; i < n; ++i) {
-    order[i] = i;
-    const double paths = (double)ctxs[i]->W * ctxs[i]->H * params[i].spp;
-    const int depth = params[i].max_bounces > 0 ? params[i].max_bounces : ctxs[i]->view.max_bounces;
-    cost[i] = paths * depth * std::log2(2.0 + ctxs[i]->view.n_prims);
+    const mrt_ctx* c = ctxs[i];
+    form[i] = params[i].form == MRT_FORM_AUTO ? c->auto_form : params[i].form;
+    const double paths = (double)c->W * c->H * params[i].spp;
+    const int depth = params[i].max_bounces > 0 ? params[i].max_bounces : c->view.max_bounces;
+    cost[i] = paths * depth * std::log2(2.0 + c->view.n_prims);
   }
-  std::sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
-  std::vector<SceneView> views(n);
-  std::vector<BatchItem> items(n);
-  uint64_t total = 0;
-  for (int k = 0; k < n; ++k) {
-    const int i = order[k];
-    views[k] = ctxs[i]->view;
-    views[k].env_lookup = params[i].env_sampler;
-    BatchItem& it = items[k];
-    it.start = total;
-    it.paths = (uint64_t)ctxs[i]->W * ctxs[i]->H * (uint64_t)params[i].spp;
-    it.seed = params[i].seed;
-    it.sample_base = (uint32_t)params[i].sample_base;
-    it.view = k;
-    it.max_bounces = params[i].max_bounces > 0 ? params[i].max_bounces : ctxs[i]->view.max_bounces;
-    it.jitter = params[i].jitter;
-    it.accum = ctxs[i]->accum.p;
-    total += it.paths;
-  }
-  SceneView* dv = nullptr;
-  BatchItem* di = nullptr;
   cudaStream_t st = c0->stream;
-  CK(cudaMallocAsync(&dv, sizeof(SceneView) * n, st));
-  CK(cudaMallocAsync(&di, sizeof(BatchItem) * n, st));
-  CK(cudaMemcpyAsync(dv, views.data(), sizeof(SceneView) * n, cudaMemcpyHostToDevice, st));
-  CK(cudaMemcpyAsync(di, items.data(), sizeof(BatchItem) * n, cudaMemcpyHostToDevice, st));
-  CK(cudaMemsetAsync(c0->status.p, 0, sizeof(int), st));
   // other contexts' streams may still be writing their accumulators
   for (int i = 0; i < n; ++i)
     if (ctxs[i]->stream != st) CK(cudaStreamSynchronize(ctxs[i]->stream));
-  CK(cudaEventRecord(c0->ev0, st));
-  int kind = 0;
+  for (int i = 0; i < n; ++i) CK(cudaMemsetAsync(ctxs[i]->status.p, 0, sizeof(int), st));
+  // megakernel scenes: one persistent launch per view type (the scenes of
+  // a launch share its kernel instantiation), longest first within it;
+  // device arrays written before anything is launched
+  struct Job { int kind; int scene; double cost; size_t m; uint64_t paths; };
+  std::vector<Job> jobs;
+  for (int kind = 0; kind < 3; ++kind) {
+    std::vector<int> order;
+    for (int i = 0; i < n; ++i) {
+      const SceneView& v = ctxs[i]->view;
+      const int k = v.has_textures ? 2 : (v.has_quadrics ? 1 : 0);
+      if (form[i] != MRT_FORM_WAVEFRONT && k == kind && params[i].spp > 0) order.push_back(i);
+    }
+    if (order.empty()) continue;
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+    const size_t m = order.size();
+    std::vector<SceneView> views(m);
+    std::vector<BatchItem> items(m);
+    uint64_t sub = 0;
+    double group_cost = 0;
+    for (size_t k = 0; k < m; ++k) {
+      const int i = order[k];
+      views[k] = ctxs[i]->view;
+      views[k].env_lookup = params[i].env_sampler;
+      BatchItem& it = items[k];
+      it.start = sub;
+      it.paths = (uint64_t)ctxs[i]->W * ctxs[i]->H * (uint64_t)params[i].spp;
+      it.seed = params[i].seed;
+      it.sample_base = (uint32_t)params[i].sample_base;
+      it.view = (int)k;
+      it.max_bounces = params[i].max_bounces > 0 ? params[i].max_bounces : ctxs[i]->view.max_bounces;
+      it.jitter = params[i].jitter;
+      it.accum = ctxs[i]->accum.p;
+      sub += it.paths;
+      group_cost += cost[i];
+    }
+    DevBuf<SceneView>& dv = c0->batch_views[kind];
+    DevBuf<BatchItem>& di = c0->batch_items[kind];
+    if (dv.n < m) CK(dv.alloc(m));
+    if (di.n < m) CK(di.alloc(m));
+    CK(cudaMemcpyAsync(dv.p, views.data(), sizeof(SceneView) * m, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(di.p, items.data(), sizeof(BatchItem) * m, cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    jobs.push_back({kind, -1, group_cost, m, sub});
+  }
   for (int i = 0; i < n; ++i)
-    kind = std::max(kind, ctxs[i]->view.has_textures ? 2 : (ctxs[i]->view.has_quadrics ? 1 : 0));
-  CK(launch_megakernel_batch(dv, di, n, total, c0->status.p, c0->counters.p + 7, params[0].block_size, kind,
-                             st));
+    if (form[i] == MRT_FORM_WAVEFRONT && params[i].spp > 0) jobs.push_back({-1, i, cost[i], 0, 0});
+  // jobs (megakernel groups, wavefront scenes) on kBatchStreams streams,
+  // longest first onto the least-loaded stream, forked from and joined back
+  // into the first context's stream
+  for (int k = 0; k < kBatchStreams; ++k) {
+    if (!c0->batch_stream[k]) CK(cudaStreamCreateWithFlags(&c0->batch_stream[k], cudaStreamNonBlocking));
+    if (!c0->batch_event[k]) CK(cudaEventCreateWithFlags(&c0->batch_event[k], cudaEventDisableTiming));
+  }
+  std::sort(jobs.begin(), jobs.end(), [](const Job& a, const Job& b) { return a.cost > b.cost; });
+  std::vector<double> load(kBatchStreams, 0.0);
+  unsigned launches = 0;
+  uint64_t total = 0;
+  CK(cudaEventRecord(c0->ev0, st));
+  for (int k = 0; k < kBatchStreams; ++k) CK(cudaStreamWaitEvent(c0->batch_stream[k], c0->ev0, 0));
+  for (const Job& j : jobs) {
+    const int k = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+    load[k] += j.cost;
+    cudaStream_t sk = c0->batch_stream[k];
+    if (j.kind >= 0) {
+      // each group its own work counter: groups may run at the same time
+      CK(launch_megakernel_batch(c0->batch_views[j.kind].p, c0->batch_items[j.kind].p, (int)j.m, j.paths,
+                                 c0->status.p, c0->counters.p + 5 + j.kind, params[0].block_size, j.kind, sk));
+      launches++;
+      total += j.paths;
+      continue;
+    }
+    mrt_ctx* c = ctxs[j.scene];
+    const mrt_render_params& p = params[j.scene];
+    const bool tuned = p.form == MRT_FORM_AUTO;
+    SceneView v = c->view;
+    v.env_lookup = p.env_sampler;
+    LaunchParams L{};
+    L.seed = p.seed;
+    L.max_bounces = p.max_bounces > 0 ? p.max_bounces : v.max_bounces;
+    L.jitter = p.jitter;
+    L.sample_base = (uint32_t)p.sample_base;
+    if (!c->wf) c->wf = wf_create();
+    const char* err = "";
+    unsigned nl = 0;
+    const int r2 = wf_render(c->wf, v, L, p.spp, p.queue_capacity ? p.queue_capacity : (tuned ? c->auto_capacity : 0),
+                             p.sort_threshold ? p.sort_threshold : (tuned ? c->auto_sort : 0), 1, c->accum.p,
+                             c->status.p, sk, &nl, &err);
+    if (r2) {
+      for (int q = 0; q < kBatchStreams; ++q) cudaStreamSynchronize(c0->batch_stream[q]);
+      return set_err(r2, "batch entry %d, wavefront: %s", j.scene, err);
+    }
+    launches += nl;
+    total += (uint64_t)c->W * c->H * (uint64_t)p.spp;
+  }
+  for (int k = 0; k < kBatchStreams; ++k) {
+    CK(cudaEventRecord(c0->batch_event[k], c0->batch_stream[k]));
+    CK(cudaStreamWaitEvent(st, c0->batch_event[k], 0));
+  }
   CK(cudaEventRecord(c0->ev1, st));
-  CK(cudaFreeAsync(dv, st));
-  CK(cudaFreeAsync(di, st));
   CK(cudaEventSynchronize(c0->ev1));
   int status = 0;
-  rc = read_status(c0, &status);
-  if (rc) return rc;
+  for (int i = 0; i < n; ++i) {
+    int s = 0;
+    rc = read_status(ctxs[i], &s);
+    if (rc) return rc;
+    status |= s;
+  }
   for (int i = 0; i < n; ++i) ctxs[i]->accum_spp += params[i].spp;
   if (stats) {
     float ms = 0;
@@ -1223,11 +1306,12 @@ extern "C" int mrt_render_batch(mrt_ctx** ctxs, const mrt_render_params* params,
     std::memset(stats, 0, sizeof(*stats));
     stats->ms = ms;
     stats->paths = total;
-    stats->kernel_launches = 1;
+    stats->kernel_launches = launches;
     stats->status = status;
   }
   if (status & ST_STACK) return set_err(MRT_ERR_STACK, "traversal stack overflow (status 0x%x)", status);
   if (status & ST_BUDGET) return set_err(MRT_ERR_BUDGET, "traversal budget exhausted (status 0x%x)", status);
+  if (status & ST_QUEUE) return set_err(MRT_ERR_QUEUE_OVERFLOW, "queue overflow (status 0x%x)", status);
   return MRT_OK;
 }
 
@@ -1242,8 +1326,7 @@ extern "C" int mrt_tune(mrt_ctx* c, int32_t spp, uint64_t seed, mrt_tune_result*
     if (out->n < MRT_TUNE_MAX) out->entry[out->n++] = mrt_tune_entry{form, block, cap, sort, 0.0};
   };
   for (int b : {64, 128, 256}) add(MRT_FORM_MEGAKERNEL, b, 0, 0);
-  if (!c->view.has_textures)   // the wavefront has no textured instantiation
-    for (int cap : {1 << 20, 1 << 21, 1 << 22})
+  for (int cap : {1 << 20, 1 << 21, 1 << 22})
       for (int sort : {1 << 30, 1 << 16}) add(MRT_FORM_WAVEFRONT, 0, cap, sort);
   int best = -1;
   for (int i = 0; i < out->n; ++i) {

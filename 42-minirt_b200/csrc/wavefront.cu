@@ -38,14 +38,18 @@ constexpr int kWfBlock = 128;
 // Traversal kernels are capped at 40 registers (12 blocks of 128 per SM):
 // measured 1.2 % faster on c1 than the 54-register build, despite a few
 // bytes of spills.
+// (The quadric and textured instantiations keep the compiler's choice: at
+// 40 registers they spill.)
 constexpr int kTravMinBlocks = 12;
+template <class V>
+constexpr int trav_min_blocks() { return V::kQuadrics ? 1 : kTravMinBlocks; }
 
 struct WfState {
   // path state, indexed by path slot
   float4* o;          // origin.xyz, pixel (int bits)
   float4* d;          // dir.xyz, remaining bounces (int bits)
   float4* pw;         // power.xyz, last material (int bits)
-  float4* acc;        // radiance.xyz, flags (int bits): bit0 default pending
+  float4* acc;        // radiance.xyz, ao of the last hit (the sky on a miss is scaled by it)
   uint64_t* rng;
   float4* hit;        // t, u, v, prim (int bits)
   float4* sp;         // surface point .xyz, material
@@ -60,7 +64,8 @@ struct WfState {
   int* q_kind;        // kKinds regions of capacity
   int* q_def;         // default-pending paths for finish
   float4* sh_o;       // shadow ray origin.xyz, tmax
-  float4* sh_d;       // shadow ray dir.xyz, (path << 4 | slot) bits
+  float4* sh_d;       // shadow ray dir.xyz, tag (see slot_bits)
+  uint64_t* sh_key;   // textured scenes: the path's random state at each shadow ray (alpha test)
   int* counters;      // see Cnt
   float4* frame;      // accumulator (W*H)
   int capacity;
@@ -150,7 +155,7 @@ __global__ void __launch_bounds__(kWfBlock) wf_generate(SceneView S, WfState W, 
 
 // --------------------------------------------------------------- extend
 template <int kBounceParity, class V>
-__global__ void __launch_bounds__(kWfBlock, kTravMinBlocks) wf_extend(V S, WfState W, int* status) {
+__global__ void __launch_bounds__(kWfBlock, trav_min_blocks<V>()) wf_extend(V S, WfState W, int* status) {
   const int n = W.counters[kBounceParity ? C_LIVE1 : C_LIVE0];
   const int* q = W.q_live[kBounceParity];
   const int lane = threadIdx.x & 31;
@@ -166,7 +171,10 @@ __global__ void __launch_bounds__(kWfBlock, kTravMinBlocks) wf_extend(V S, WfSta
       const float4 o = W.o[i], d = W.d[i];
       HitInfo h;
       int visits = 0;
-      bool hit = closest_hit_compact<false>(S, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), h, visits, status, stack);
+      // textured scenes: the alpha test draws from the path's random state
+      const uint64_t akey = V::kTextures ? W.rng[i] : 0;
+      bool hit = closest_hit_compact<false>(S, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), h, visits, status, stack,
+                                            akey);
       W.hit[i] = make_float4(h.t, h.u, h.v, __int_as_float(hit ? h.prim : kMiss));
     }
   }
@@ -206,7 +214,7 @@ __global__ void __launch_bounds__(kWfBlock) wf_classify(SceneView S, WfState W, 
         const float4 d = W.d[i], p = W.pw[i];
         float3 bg = background(S, f3(d.x, d.y, d.z), true);
         const int last = __float_as_int(p.w);
-        if (last >= 0) bg = bg * S.mats[last].ao;
+        if (last >= 0) bg = bg * W.acc[i].w;
         float4 a = W.acc[i];
         a.x += bg.x * p.x; a.y += bg.y * p.y; a.z += bg.z * p.z;
         W.acc[i] = a;
@@ -228,7 +236,7 @@ __global__ void __launch_bounds__(kWfBlock) wf_classify(SceneView S, WfState W, 
 // --------------------------------------------------------------- sample
 // Emits the shadow rays of a diffuse event and records what finish needs.
 __device__ __forceinline__ void emit_shadow(const WfState& W, int path, int slot, float3 o, float3 d,
-                                            float tmax, int* status) {
+                                            float tmax, int* status, uint64_t key) {
   const int s = atomicAdd(&W.counters[C_SH], 1);
   if (s >= W.sh_capacity) {
     atomicOr(status, ST_QUEUE);
@@ -236,6 +244,7 @@ __device__ __forceinline__ void emit_shadow(const WfState& W, int path, int slot
   }
   W.sh_o[s] = make_float4(o.x, o.y, o.z, tmax);
   W.sh_d[s] = make_float4(d.x, d.y, d.z, __int_as_float((path << W.slot_bits) | slot));
+  if (W.sh_key) W.sh_key[s] = key;
 }
 
 template <int kBounceParity, class V>
@@ -273,7 +282,7 @@ __global__ void __launch_bounds__(kWfBlock) wf_sample(V S, WfState W, const WfPa
       if (s.mat < 0) {
         diffuse = true;
       } else {
-        const MaterialD& M = S.mats[s.mat];
+        const MaterialD& M = surf_mat(S, s);
         if (M.emission_strength > 0.0f) ps.acc = ps.acc + (ld3(M.emission) * M.emission_strength) * ps.power;
         bool metal;
         if (M.metallic == 1.0f) metal = true;
@@ -310,16 +319,16 @@ __global__ void __launch_bounds__(kWfBlock) wf_sample(V S, WfState W, const WfPa
           if (L.type == 0) {
             if (L.radius == 0.0f || L.shadow_sample <= 1) {
               const float3 to = lp - s.p;
-              emit_shadow(W, i, l, s.p, unit(to), sqrtf(len2(to)), status);
+              emit_shadow(W, i, l, s.p, unit(to), sqrtf(len2(to)), status, ps.rng.s);
             } else {
               for (int t = 0; t < L.shadow_sample; ++t) {
                 const float3 tgt = lp + rnd_in_unit_sphere(ps.rng) * L.radius;
                 const float3 to = tgt - s.p;
-                emit_shadow(W, i, l, s.p, unit(to), sqrtf(len2(to)), status);
+                emit_shadow(W, i, l, s.p, unit(to), sqrtf(len2(to)), status, ps.rng.s);
               }
             }
           } else {
-            emit_shadow(W, i, l, s.p, unit(-lp), INFINITY, status);
+            emit_shadow(W, i, l, s.p, unit(-lp), INFINITY, status, ps.rng.s);
           }
         }
         for (int w = 0; w < W.vis_words; ++w) W.vis[(size_t)w * W.capacity + i] = 0u;
@@ -334,8 +343,8 @@ __global__ void __launch_bounds__(kWfBlock) wf_sample(V S, WfState W, const WfPa
           env_pdf = e.w;
           const float4 r = __ldg(S.env_rec1 + kk);
           env_rad = f3(r.x, r.y, r.z);
-          if (s.mat >= 0) env_rad = env_rad * S.mats[s.mat].ao;
-          emit_shadow(W, i, (1 << W.slot_bits) - 1, s.p, dir, INFINITY, status);
+          if (s.mat >= 0) env_rad = env_rad * surf_mat(S, s).ao;
+          emit_shadow(W, i, (1 << W.slot_bits) - 1, s.p, dir, INFINITY, status, ps.rng.s);
         }
         ps.d = cos_hemisphere(ps.rng, s.n);
         W.sp[i] = make_float4(s.p.x, s.p.y, s.p.z, __int_as_float(s.mat));
@@ -346,7 +355,8 @@ __global__ void __launch_bounds__(kWfBlock) wf_sample(V S, WfState W, const WfPa
       }
       p4 = make_float4(ps.power.x, ps.power.y, ps.power.z, __int_as_float(s.mat));
       W.pw[i] = p4;
-      W.acc[i] = make_float4(ps.acc.x, ps.acc.y, ps.acc.z, 0.f);
+      // the ao of this hit scales the sky if the next segment misses
+      W.acc[i] = make_float4(ps.acc.x, ps.acc.y, ps.acc.z, s.mat >= 0 ? surf_mat(S, s).ao : 1.0f);
       W.d[i] = make_float4(ps.d.x, ps.d.y, ps.d.z, __int_as_float(depth_left));
       W.o[i] = make_float4(ps.o.x, ps.o.y, ps.o.z, o.w);
       W.rng[i] = ps.rng.s;
@@ -365,7 +375,7 @@ __global__ void __launch_bounds__(kWfBlock) wf_sample(V S, WfState W, const WfPa
 
 // -------------------------------------------------------------- connect
 template <class V>
-__global__ void __launch_bounds__(kWfBlock, kTravMinBlocks) wf_connect(V S, WfState W, int* status) {
+__global__ void __launch_bounds__(kWfBlock, trav_min_blocks<V>()) wf_connect(V S, WfState W, int* status) {
   const int n = min(W.counters[C_SH], W.sh_capacity);
   const int lane = threadIdx.x & 31;
   LocalStack stack;
@@ -377,7 +387,8 @@ __global__ void __launch_bounds__(kWfBlock, kTravMinBlocks) wf_connect(V S, WfSt
     const int k = base + lane;
     if (k < n) {
       const float4 o = W.sh_o[k], d = W.sh_d[k];
-      const bool blocked = any_hit_compact(S, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), o.w, status, stack);
+      const uint64_t akey = V::kTextures ? W.sh_key[k] : 0;
+      const bool blocked = any_hit_compact(S, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), o.w, status, stack, akey);
       if (!blocked) {
         const int tag = __float_as_int(d.w);
         const int env_slot = (1 << W.slot_bits) - 1;
@@ -462,7 +473,7 @@ __global__ void __launch_bounds__(kWfBlock) wf_finish(SceneView S, WfState W) {
         acc = acc + rad;
         power = power * (1.0f - ev.w);
       }
-      W.acc[i] = make_float4(acc.x, acc.y, acc.z, 0.f);
+      W.acc[i] = make_float4(acc.x, acc.y, acc.z, a4.w);
       W.pw[i] = make_float4(power.x, power.y, power.z, pw4.w);
       const int depth_left = __float_as_int(W.d[i].w);
       const bool dead = power.x == 0.0f && power.y == 0.0f && power.z == 0.0f;
@@ -557,16 +568,25 @@ static cudaError_t wf_alloc(WfHost* H, int capacity, int n_lights, bool env) {
   return cudaMemset(s.counters, 0, sizeof(int) * C_COUNT);
 }
 
-static cudaError_t wf_shadow_alloc(WfHost* H, size_t sh_cap) {
-  if ((size_t)H->sh_capacity >= sh_cap) return cudaSuccess;
+// Shadow-ray queue of sh_cap rays; keys: the per-ray random state the alpha
+// test of textured scenes needs.
+static cudaError_t wf_shadow_alloc(WfHost* H, size_t sh_cap, bool keys) {
+  if ((size_t)H->sh_capacity >= sh_cap && (!keys || H->st.sh_key)) return cudaSuccess;
+  sh_cap = std::max(sh_cap, (size_t)H->sh_capacity);
   cudaError_t e;
   float4 *o = nullptr, *d = nullptr;
+  uint64_t* key = nullptr;
   if ((e = cudaMalloc(&o, sh_cap * 16)) != cudaSuccess) return e;
   H->allocs.push_back(o);
   if ((e = cudaMalloc(&d, sh_cap * 16)) != cudaSuccess) return e;
   H->allocs.push_back(d);
+  if (keys || H->st.sh_key) {
+    if ((e = cudaMalloc(&key, sh_cap * 8)) != cudaSuccess) return e;
+    H->allocs.push_back(key);
+  }
   H->st.sh_o = o;
   H->st.sh_d = d;
+  H->st.sh_key = key;
   H->st.sh_capacity = (int)sh_cap;
   H->sh_capacity = (int)sh_cap;
   if (H->graph) { cudaGraphExecDestroy(H->graph); H->graph = nullptr; }
@@ -612,9 +632,8 @@ static void wf_enqueue_wave_t(WfHost* H, const VT& v, const WfParams& P, int* st
 
 static void wf_enqueue_wave(WfHost* H, const SceneView& v, const WfParams& P, int* status,
                             cudaStream_t st, unsigned* launches) {
-  // textured scenes never reach the wavefront (mrt_render refuses them)
   with_view(v, [&](const auto& vt) {
-    if constexpr (!std::decay_t<decltype(vt)>::kTextures) wf_enqueue_wave_t(H, vt, P, status, st, launches);
+    wf_enqueue_wave_t(H, vt, P, status, st, launches);
     return 0;
   });
 }
@@ -659,7 +678,7 @@ int wf_render(WfHost* H, const SceneView& v, const LaunchParams& L, int spp, int
       per_path += k;
     }
   }
-  if ((e = wf_shadow_alloc(H, std::max<size_t>(per_path * capacity, 1024))) != cudaSuccess) {
+  if ((e = wf_shadow_alloc(H, std::max<size_t>(per_path * capacity, 1024), v.has_textures != 0)) != cudaSuccess) {
     *err = cudaGetErrorString(e);
     return MRT_ERR_OOM;
   }

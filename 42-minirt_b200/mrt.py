@@ -233,7 +233,10 @@ class MRTError(RuntimeError):
 
 
 def render_batch(ctxs: list, params: list[dict], block_size: int = 0) -> "RenderStats":
-    """One persistent launch over the scenes of several contexts (same device)."""
+    """One call over the scenes of several contexts (same device): megakernel
+    scenes in one persistent launch per view type, wavefront scenes each in
+    its own wavefront, all on concurrent streams. params[i]["form"] picks the
+    form per scene (FORM_AUTO: the scene's tuned choice)."""
     lib = load()
     n = len(ctxs)
     arr = (_P * n)(*[c.h for c in ctxs])
@@ -241,7 +244,8 @@ def render_batch(ctxs: list, params: list[dict], block_size: int = 0) -> "Render
     for i, p in enumerate(params):
         ps[i] = RenderParams(spp=p["spp"], sample_base=p.get("sample_base", 0), seed=p.get("seed", 1),
                              max_bounces=p.get("max_bounces", 0), jitter=p.get("jitter", 0),
-                             env_sampler=p.get("env_sampler", 0), block_size=block_size)
+                             env_sampler=p.get("env_sampler", 0), block_size=block_size,
+                             form=p.get("form", FORM_MEGAKERNEL))
     st = RenderStats()
     check(lib.mrt_render_batch(arr, ps, n, C.byref(st)), "mrt_render_batch")
     return st

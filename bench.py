@@ -303,7 +303,8 @@ def bench_c3(a) -> int:
     workload. Forms: one persistent launch over all scenes (mrt_render_batch,
     LPT-ordered), and per-scene launches of the plain megakernel, the
     regenerating megakernel, the wavefront and the per-scene autotuned
-    choice (mrt_tune). Device time (CUDA events) summed over the calls."""
+    choice (mrt_tune), and one batch call with every scene in its tuned
+    form. Device time (CUDA events) summed over the calls."""
     import mrt
     import scenes
     specs = scenes.make_c3_specs()
@@ -355,6 +356,18 @@ def bench_c3(a) -> int:
         picks[best["form"]] = picks.get(best["form"], 0) + 1
     ms, launches = per_scene(mrt.FORM_AUTO)
     forms["autotuned"] = {"ms_per_step": ms / a.steps, "launches": launches, "tuner_picks": picks}
+    # one batch call with each scene in its tuned form
+    for c in ctxs:
+        c.clear()
+    ms, launches = 0.0, 0
+    for s in range(a.warmup + a.steps):
+        params = [dict(spp=k, sample_base=s * k, seed=1, max_bounces=sc.max_bounces, form=mrt.FORM_AUTO)
+                  for sc, k in zip(scs, per_step)]
+        st = mrt.render_batch(ctxs, params)
+        if s >= a.warmup:
+            ms += st.ms
+            launches += st.kernel_launches
+    forms["batch_autotuned"] = {"ms_per_step": ms / a.steps, "launches": launches, "tuner_picks": picks}
     clk = clocks.stop()
     for f in forms.values():
         f["value"] = paths_step / (f["ms_per_step"] / 1000.0) / 1e6

@@ -368,12 +368,18 @@ MRT_API int			mrt_set_camera(mrt_ctx *ctx, const mrt_camera *camera,
 /* Render params->spp samples per pixel into the device accumulator. */
 MRT_API int			mrt_render(mrt_ctx *ctx, const mrt_render_params *params,
 				mrt_render_stats *stats);
-/* Multi-scene batch: renders params[i] on ctx[i] for all i in ONE persistent
- * launch (all contexts on the same device, each with a built scene). Paths of
- * all scenes share one work queue, scenes ordered longest-first by predicted
- * cost (paths x depth x log2 primitives). params[i].form / block_size apply
- * to the whole batch; offset must be NULL. stats (may be NULL) receives the
- * totals of the launch. */
+/* Multi-scene batch: renders params[i] on ctx[i] for all i in one call (all
+ * contexts on the same device, each with a built scene, no context twice).
+ * Each scene takes params[i].form (MRT_FORM_AUTO: its mrt_tune choice;
+ * textured scenes always a megakernel). Megakernel scenes share one
+ * persistent launch per view type (spheres / triangles, + quadrics,
+ * + textures), their paths in one work queue, longest scene first by
+ * predicted cost (paths x depth x log2 primitives); wavefront scenes each
+ * run their own wavefront. These jobs run on four streams forked from and
+ * joined back into ctx[0]'s stream, longest first onto the least-loaded
+ * stream, so small scenes overlap large ones. params[0].block_size applies
+ * to the megakernel launches; offset must be NULL. stats (may be NULL)
+ * receives the call's device time, paths and kernel launches. */
 MRT_API int			mrt_render_batch(mrt_ctx **ctx, const mrt_render_params *params,
 				int32_t n, mrt_render_stats *stats);
 

@@ -161,7 +161,7 @@ class RefOracle:
         return out
 
     def bvh(self):
-        n_prims = len(self.scene.spheres) + self.scene.n_triangles
+        n_prims = self.scene.n_prims_bvh()
         nn = max(1, 2 * n_prims)
         b = np.zeros((nn, 6))
         info = np.zeros((nn, 5), np.uint32)

@@ -213,10 +213,29 @@ def test_paths_match_oracle_stream(mrt, oracle, mg, name):
     assert abs(diff.mean()) <= 4 * se, (diff.mean(), se)
 
 
-@pytest.mark.parametrize("name", ["c0", "c1", "c2", "q0"])
-def test_wavefront_matches_megakernel(mrt, oracle, mg, name):
-    """Both forms run the same estimator on the same random streams."""
-    sc = mg.CASES[name]["make"]()
+def six_light_scene(scenes):
+    """c0 with six point lights, two of them soft (radius, shadow samples):
+    more lights than one visibility word of the wavefront holds."""
+    sc = scenes.make_c0(0, 32, 24, depth=6)
+    for k in range(6):
+        a = 2 * np.pi * k / 6
+        sc.lights.append(dict(position=(4 * np.cos(a), 4 + 0.3 * k, 4 * np.sin(a)), brightness=0.4,
+                              color=(255, 200 + 9 * k, 180), radius=0.3 if k % 3 == 0 else 0.0,
+                              shadow_sample=3 if k % 3 == 0 else 1))
+    return sc
+
+
+@pytest.mark.parametrize("name", ["c0", "c1", "c2", "q0", "t0", "t0_alpha", "lights6"])
+def test_wavefront_matches_megakernel(mrt, oracle, mg, scenes, name):
+    """Both forms run the same estimator on the same random streams
+    (textured scenes included: the alpha test draws from the same path state
+    in both)."""
+    if name == "lights6":
+        sc = six_light_scene(scenes)
+    elif name == "t0_alpha":
+        sc = scenes.make_textured(6, 32, 24, depth=6, partial_alpha=True)
+    else:
+        sc = mg.CASES[name]["make"]()
     ctx = gpu_ctx(mrt, oracle, sc)
     ctx.render(8, seed=5)
     a, _ = ctx.read_accum()
@@ -385,9 +404,10 @@ def test_batch_matches_individual_renders(mrt, oracle, scenes):
 
 
 def test_batch_with_quadrics_matches_individual_renders(mrt, oracle, scenes):
-    """A batch holding a scene with cylinders, cones and hyperboloids runs
-    the quadric instantiation of the batch kernel for every scene; each
-    accumulator still equals its own single-scene render."""
+    """A batch holding a scene with cylinders, cones and hyperboloids: the
+    quadric scene runs in the quadric instantiation of the batch kernel, the
+    others in the plain one (one launch per view type); each accumulator
+    equals its own single-scene render."""
     specs = [scenes.make_quadrics(5, 40, 30, depth=6), scenes.make_c0(0, 32, 24)]
     ctxs = []
     for sc in specs:
@@ -400,6 +420,33 @@ def test_batch_with_quadrics_matches_individual_renders(mrt, oracle, scenes):
     for i, c in enumerate(ctxs):
         c.clear()
         c.render(params[i]["spp"], seed=params[i]["seed"])
+        single, _ = c.read_accum()
+        np.testing.assert_allclose(batch[i][0], single, rtol=1e-4, atol=1e-5)
+
+
+def test_batch_with_mixed_forms_matches_individual_renders(mrt, oracle, scenes):
+    """Per-scene forms in one batch: megakernel scenes share a persistent
+    launch, wavefront scenes run their own wavefronts on concurrent streams,
+    and FORM_AUTO takes each scene's tuned choice; every accumulator equals
+    the single-scene render of the same form and streams."""
+    specs = [scenes.make_c0(0, 40, 30), scenes.make_c1(3, 32, 24, freq=6, sky=(32, 16)),
+             scenes.make_quadrics(5, 40, 30, depth=6), scenes.make_c1(4, 48, 36, freq=8, sky=(32, 16)),
+             scenes.make_c0(5, 16, 48)]
+    forms = [mrt.FORM_WAVEFRONT, mrt.FORM_MEGAKERNEL, mrt.FORM_WAVEFRONT, mrt.FORM_AUTO, mrt.FORM_MEGAKERNEL]
+    ctxs = []
+    for sc in specs:
+        c = mrt.Context(sc.width, sc.height)
+        c.build(oracle.canonical_scene(sc))
+        ctxs.append(c)
+    ctxs[3].tune(spp=1)
+    params = [dict(spp=3 + i, seed=31 + i, form=f) for i, f in enumerate(forms)]
+    st = mrt.render_batch(ctxs, params)
+    assert st.paths == sum(sc.width * sc.height * (3 + i) for i, sc in enumerate(specs))
+    batch = [c.read_accum() for c in ctxs]
+    for i, c in enumerate(ctxs):
+        assert batch[i][1] == params[i]["spp"]
+        c.clear()
+        c.render(params[i]["spp"], seed=params[i]["seed"], form=forms[i])
         single, _ = c.read_accum()
         np.testing.assert_allclose(batch[i][0], single, rtol=1e-4, atol=1e-5)
 
@@ -417,15 +464,14 @@ def test_quadric_scene_rejects_malformed_objects(mrt, scenes):
 
 
 def test_textured_scene_forms(mrt, oracle, scenes):
-    """Textured scenes render with the megakernel forms; an explicit
-    wavefront request is refused with a message, the autotuner and
-    FORM_AUTO pick a megakernel, and the plain and regenerating megakernels
-    agree per pixel on the same streams."""
+    """Textured scenes render in every form: the plain and regenerating
+    megakernels agree per pixel on the same streams, and the autotuner and
+    FORM_AUTO may pick any form (the wavefront's agreement is checked in
+    test_wavefront_matches_megakernel)."""
     sc = scenes.make_textured(6, 48, 36, depth=6)
     ctx = mrt.Context(48, 36)
     ctx.build(oracle.canonical_scene(sc))
-    with pytest.raises(mrt.MRTError, match="megakernel"):
-        ctx.render(2, seed=3, form=mrt.FORM_WAVEFRONT)
+    ctx.render(2, seed=3, form=mrt.FORM_WAVEFRONT)
     ctx.clear()
     ctx.render(8, seed=3, form=mrt.FORM_MEGAKERNEL)
     a, _ = ctx.read_accum()
