@@ -95,4 +95,12 @@ def compare(x: np.ndarray, var_x: np.ndarray, batch_means_x: np.ndarray, ref: di
     z = (x - r) / np.sqrt(var_x + var_r + floor ** 2)
     out["pixel_z_rms"] = float(np.sqrt(np.mean(z ** 2)))
     out["pixel_z_gt5"] = float(np.mean(np.abs(z) > 5))
+    # the bias relMSE over the pixels whose every channel is within 5
+    # standard errors (the outliers are bounded separately by pixel_z_gt5):
+    # a handful of firefly pixels, whose variance a few batch means cannot
+    # estimate, would otherwise decide it
+    keep = np.all(np.abs(z) <= 5, axis=-1) if z.ndim > 1 else np.abs(z) <= 5
+    tb = ((d2 - var_r - var_x) * w)[keep]
+    out["relmse_bias_inliers"] = float(np.mean(tb)) if tb.size else 0.0
+    out["relmse_bias_inliers_se"] = float(np.std(tb) / np.sqrt(max(tb.size, 1)))
     return out
