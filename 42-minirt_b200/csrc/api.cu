@@ -1326,7 +1326,7 @@ extern "C" int mrt_tune(mrt_ctx* c, int32_t spp, uint64_t seed, mrt_tune_result*
     if (out->n < MRT_TUNE_MAX) out->entry[out->n++] = mrt_tune_entry{form, block, cap, sort, 0.0};
   };
   for (int b : {64, 128, 256}) add(MRT_FORM_MEGAKERNEL, b, 0, 0);
-  for (int cap : {1 << 20, 1 << 21, 1 << 22})
+  for (int cap : {1 << 21, 1 << 23, 1 << 25})
       for (int sort : {1 << 30, 1 << 16}) add(MRT_FORM_WAVEFRONT, 0, cap, sort);
   int best = -1;
   for (int i = 0; i < out->n; ++i) {

@@ -24,6 +24,8 @@
 // A whole wave (generate + depth x stages) is captured once in a CUDA graph
 // and replayed; kernels read their queue lengths from device counters.
 #include <type_traits>
+#include <algorithm>
+#include <atomic>
 #include <vector>
 
 #include "../../include/mrt.h"
@@ -93,6 +95,7 @@ __host__ __device__ inline int slot_bits_for(int n_lights) {
 enum Cnt : int {
   C_LIVE0 = 0, C_LIVE1 = 1, C_KIND = 2,          // C_KIND..C_KIND+3
   C_DEF = 6, C_SH = 7, C_WORK = 8, C_WAVE = 9, C_GEN = 10, C_SEG = 11, C_SHADOW = 12,
+  C_WORK_SH = 13,      // work counter of connect (runs beside the next extend)
   C_COUNT = 16
 };
 
@@ -364,6 +367,10 @@ __global__ void __launch_bounds__(kWfBlock) wf_sample(V S, WfState W, const WfPa
         const bool dead = ps.power.x == 0.0f && ps.power.y == 0.0f && ps.power.z == 0.0f;
         cont = depth_left > 0 && !dead;
         if (!cont) retire(W, i);
+      } else {
+        // a diffuse path continues whatever its shadow rays find: its next
+        // segment is traced while connect and finish complete this bounce
+        cont = depth_left > 0;
       }
     }
     const int slot = warp_append(c_next, cont);
@@ -381,7 +388,7 @@ __global__ void __launch_bounds__(kWfBlock, trav_min_blocks<V>()) wf_connect(V S
   LocalStack stack;
   while (true) {
     int base = 0;
-    if (lane == 0) base = atomicAdd(&W.counters[C_WORK], 32);
+    if (lane == 0) base = atomicAdd(&W.counters[C_WORK_SH], 32);
     base = __shfl_sync(0xffffffffu, base, 0);
     if (base >= n) break;
     const int k = base + lane;
@@ -401,14 +408,10 @@ __global__ void __launch_bounds__(kWfBlock, trav_min_blocks<V>()) wf_connect(V S
 }
 
 // --------------------------------------------------------------- finish
-template <int kBounceParity>
 __global__ void __launch_bounds__(kWfBlock) wf_finish(SceneView S, WfState W) {
   const int n = W.counters[C_DEF];
-  int* q_next = W.q_live[kBounceParity ^ 1];
-  int* c_next = &W.counters[kBounceParity ? C_LIVE0 : C_LIVE1];
   for (int k0 = blockIdx.x * blockDim.x; k0 < n; k0 += gridDim.x * blockDim.x) {
     const int k = k0 + threadIdx.x;
-    bool cont = false;
     int i = -1;
     if (k < n) {
       i = W.q_def[k];
@@ -475,30 +478,31 @@ __global__ void __launch_bounds__(kWfBlock) wf_finish(SceneView S, WfState W) {
       }
       W.acc[i] = make_float4(acc.x, acc.y, acc.z, a4.w);
       W.pw[i] = make_float4(power.x, power.y, power.z, pw4.w);
-      const int depth_left = __float_as_int(W.d[i].w);
-      const bool dead = power.x == 0.0f && power.y == 0.0f && power.z == 0.0f;
-      cont = depth_left > 0 && !dead;
-      if (!cont) retire(W, i);
+      // the path continues (sample queued it) unless this was its last bounce
+      if (__float_as_int(W.d[i].w) <= 0) retire(W, i);
     }
-    const int slot = warp_append(c_next, cont);
-    if (cont) q_next[slot] = i;
   }
 }
 
-// Resets the per-bounce counters for the next bounce.
+// Resets the counters of bounce parity kBounceParity once its connect and
+// finish are done: its consumed live queue, the kind queues, the diffuse and
+// shadow-ray queues.
 template <int kBounceParity>
 __global__ void wf_reset(WfState W) {
   if (threadIdx.x == 0) {
-    W.counters[kBounceParity ? C_LIVE1 : C_LIVE0] = 0;   // the queue just consumed
+    W.counters[kBounceParity ? C_LIVE1 : C_LIVE0] = 0;   // the queue extend consumed
     for (int c = 0; c < kKinds; ++c) W.counters[C_KIND + c] = 0;
     W.counters[C_DEF] = 0;
     W.counters[C_SH] = 0;
-    W.counters[C_WORK] = 0;
   }
 }
 
 __global__ void wf_work_reset(WfState W) {
   if (threadIdx.x == 0) W.counters[C_WORK] = 0;
+}
+
+__global__ void wf_sh_work_reset(WfState W) {
+  if (threadIdx.x == 0) W.counters[C_WORK_SH] = 0;
 }
 
 __global__ void wf_wave_begin(WfState W) {
@@ -509,6 +513,7 @@ __global__ void wf_wave_begin(WfState W) {
     W.counters[C_DEF] = 0;
     W.counters[C_SH] = 0;
     W.counters[C_WORK] = 0;
+    W.counters[C_WORK_SH] = 0;
   }
 }
 
@@ -530,6 +535,10 @@ struct WfHost {
   WfParams* dparams = nullptr;
   std::vector<void*> allocs;
   cudaGraphExec_t graph = nullptr;
+  // the side stream of each bounce's connect and finish, which run beside
+  // the next bounce's extend; fork / join events
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int graph_bounces = -1;
   unsigned graph_launches = 0;   // kernels per replay of the graph
   uint64_t graph_key = 0;
@@ -593,37 +602,54 @@ static cudaError_t wf_shadow_alloc(WfHost* H, size_t sh_cap, bool keys) {
   return cudaSuccess;
 }
 
-// One bounce of the wave: extend, classify, sample, connect, finish, reset.
-// Returns the number of kernels launched.
-template <int kPar, class VT>
-static unsigned wf_enqueue_bounce(const WfHost* H, const VT& v, const WfState& s, const WfParams* dP,
-                                  int* status, cudaStream_t st) {
-  const int gen_blocks = std::max(1, std::min((H->capacity + kWfBlock - 1) / kWfBlock, H->sms * 16));
-  const int pers = H->sms * 12;
-  wf_extend<kPar, VT><<<pers, kWfBlock, 0, st>>>(v, s, status);
-  wf_classify<kPar><<<gen_blocks, kWfBlock, 0, st>>>(v, s, dP);
-  wf_sample<kPar, VT><<<gen_blocks, kWfBlock, 0, st>>>(v, s, dP, status);
-  wf_work_reset<<<1, 32, 0, st>>>(s);
-  wf_connect<VT><<<pers, kWfBlock, 0, st>>>(v, s, status);
-  wf_finish<kPar><<<gen_blocks, kWfBlock, 0, st>>>(v, s);
-  wf_reset<kPar><<<1, 32, 0, st>>>(s);
-  return 7;
-}
-
-// Enqueues one wave (generate + max_bounces x stages) on `st`; the
-// traversal and shading stages are the instantiation for the view's type.
+// One wave: generate, then per bounce classify and sample on the main
+// stream, connect and finish (the shadow rays of the bounce and the terms
+// they decide) on the side stream while the main stream traces the next
+// bounce's extension rays (extend), joined before the next classify, which
+// reads the power and radiance finish updates. The two branches touch
+// disjoint path state: extend writes the hit records, finish the power and
+// radiance, connect the visibility words.
 template <class VT>
 static void wf_enqueue_wave_t(WfHost* H, const VT& v, const WfParams& P, int* status,
                               cudaStream_t st, unsigned* launches) {
   const WfParams* dP = H->dparams;
   const int gen_blocks = std::max(1, std::min((H->capacity + kWfBlock - 1) / kWfBlock, H->sms * 16));
-  WfState s = H->st;
+  const int pers = H->sms * 12;
+  const WfState s = H->st;
+  cudaStream_t sd = H->side;
+  unsigned n = 0;
+  auto extend = [&](int par) {
+    wf_work_reset<<<1, 32, 0, st>>>(s);
+    if (par) wf_extend<1, VT><<<pers, kWfBlock, 0, st>>>(v, s, status);
+    else wf_extend<0, VT><<<pers, kWfBlock, 0, st>>>(v, s, status);
+    n += 2;
+  };
   wf_wave_begin<<<1, 32, 0, st>>>(s);
   wf_generate<<<gen_blocks, kWfBlock, 0, st>>>(v, s, dP);
-  unsigned n = 2;
-  for (int b = 0; b < P.max_bounces; ++b)
-    n += (b & 1) ? wf_enqueue_bounce<1>(H, v, s, dP, status, st)
-                 : wf_enqueue_bounce<0>(H, v, s, dP, status, st);
+  n += 2;
+  extend(0);
+  for (int b = 0; b < P.max_bounces; ++b) {
+    const int par = b & 1;
+    if (par) {
+      wf_classify<1><<<gen_blocks, kWfBlock, 0, st>>>(v, s, dP);
+      wf_sample<1, VT><<<gen_blocks, kWfBlock, 0, st>>>(v, s, dP, status);
+    } else {
+      wf_classify<0><<<gen_blocks, kWfBlock, 0, st>>>(v, s, dP);
+      wf_sample<0, VT><<<gen_blocks, kWfBlock, 0, st>>>(v, s, dP, status);
+    }
+    cudaEventRecord(H->ev_fork, st);
+    cudaStreamWaitEvent(sd, H->ev_fork, 0);
+    wf_sh_work_reset<<<1, 32, 0, sd>>>(s);
+    wf_connect<VT><<<pers, kWfBlock, 0, sd>>>(v, s, status);
+    wf_finish<<<gen_blocks, kWfBlock, 0, sd>>>(v, s);
+    cudaEventRecord(H->ev_join, sd);
+    n += 5;
+    if (b + 1 < P.max_bounces) extend(par ^ 1);
+    cudaStreamWaitEvent(st, H->ev_join, 0);
+    if (par) wf_reset<1><<<1, 32, 0, st>>>(s);
+    else wf_reset<0><<<1, 32, 0, st>>>(s);
+    n += 1;
+  }
   // paths still live after the last bounce retire with what they gathered
   wf_wave_end<<<1, 32, 0, st>>>(s);
   n += 1;
@@ -644,6 +670,14 @@ __global__ void wf_retire_remaining(WfState W, int parity_count_index, int parit
   for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) retire(W, q[k]);
 }
 
+size_t wf_device_bytes(const WfHost* H);
+
+// Device bytes of all wavefront states of the process (many contexts, as in a
+// batch of scenes, each keep theirs): their default capacities together stay
+// within kWfTotalBudget.
+static std::atomic<size_t> g_wf_bytes{0};
+constexpr size_t kWfTotalBudget = 48ull << 30;
+
 int wf_render(WfHost* H, const SceneView& v, const LaunchParams& L, int spp, int capacity,
               int sort_threshold, int use_graph, float4* frame, int* status, cudaStream_t st,
               unsigned* launches, const char** err) {
@@ -652,20 +686,18 @@ int wf_render(WfHost* H, const SceneView& v, const LaunchParams& L, int spp, int
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&H->sms, cudaDevAttrMultiProcessorCount, dev);
   }
+  if (!H->side) {
+    cudaError_t e0 = cudaStreamCreateWithFlags(&H->side, cudaStreamNonBlocking);
+    if (e0 == cudaSuccess) e0 = cudaEventCreateWithFlags(&H->ev_fork, cudaEventDisableTiming);
+    if (e0 == cudaSuccess) e0 = cudaEventCreateWithFlags(&H->ev_join, cudaEventDisableTiming);
+    if (e0 != cudaSuccess) { *err = cudaGetErrorString(e0); return MRT_ERR_CUDA; }
+  }
   const uint64_t npix = (uint64_t)v.width * v.height;
   const uint64_t total = npix * (uint64_t)spp;
   if (total == 0) return MRT_OK;
   if (v.n_lights > kMaxWfLights) {
     *err = "wavefront form supports up to 1023 lights (use the megakernel)";
     return MRT_ERR_INVALID;
-  }
-  if (capacity <= 0) capacity = 1 << 22;
-  const int slot_bits = slot_bits_for(v.n_lights);
-  capacity = std::min(capacity, 1 << (31 - slot_bits));
-  capacity = (int)std::min<uint64_t>((uint64_t)capacity, std::max<uint64_t>(total, 1024));
-  cudaError_t e;
-  if (H->capacity != capacity || H->vis_words != std::max(1, (v.n_lights + 3) / 4)) {
-    if ((e = wf_alloc(H, capacity, v.n_lights, v.env_nee)) != cudaSuccess) { *err = cudaGetErrorString(e); return MRT_ERR_OOM; }
   }
   // shadow rays per diffuse event: hard lights 1, soft lights shadow_sample, env 1
   size_t per_path = v.env_nee ? 1 : 0;
@@ -678,7 +710,33 @@ int wf_render(WfHost* H, const SceneView& v, const LaunchParams& L, int spp, int
       per_path += k;
     }
   }
-  if ((e = wf_shadow_alloc(H, std::max<size_t>(per_path * capacity, 1024), v.has_textures != 0)) != cudaSuccess) {
+  // Path slots: by default every path of the call at once, up to 2^25 and
+  // within min(16 GiB, a quarter of free memory) of path state and shadow
+  // queue. Fewer, larger waves mean fewer queue drains (the last bounces of
+  // a wave run with few live paths): on c1 (33 M paths per 16-spp step) one
+  // wave of 2^25 slots traced 511 Mpaths/s against 381 with 2^22.
+  const int slot_bits = slot_bits_for(v.n_lights);
+  if (capacity <= 0) {
+    const size_t per_slot = 16 * 10 + 8 + 4 * (4 + std::max(1, (v.n_lights + 3) / 4)) + 4 * kKinds +
+                            per_path * (32 + (v.has_textures ? 8 : 0));
+    size_t free_b = 0, total_b = 0;
+    cudaMemGetInfo(&free_b, &total_b);
+    const size_t have = wf_device_bytes(H);
+    const size_t others = g_wf_bytes.load() - std::min(g_wf_bytes.load(), have);
+    const size_t budget = std::min<size_t>({16ull << 30, (free_b + have) / 4,
+                                            kWfTotalBudget - std::min(kWfTotalBudget, others)});
+    capacity = (int)std::max<size_t>(1 << 20, std::min<size_t>(1 << 25, budget / per_slot));
+  }
+  capacity = std::min(capacity, 1 << (31 - slot_bits));
+  capacity = (int)std::min<uint64_t>((uint64_t)capacity, std::max<uint64_t>(total, 1024));
+  cudaError_t e = cudaSuccess;
+  const size_t before = wf_device_bytes(H);
+  if (H->capacity != capacity || H->vis_words != std::max(1, (v.n_lights + 3) / 4))
+    e = wf_alloc(H, capacity, v.n_lights, v.env_nee);
+  if (e == cudaSuccess) e = wf_shadow_alloc(H, std::max<size_t>(per_path * capacity, 1024), v.has_textures != 0);
+  g_wf_bytes += wf_device_bytes(H);
+  g_wf_bytes -= before;
+  if (e != cudaSuccess) {
     *err = cudaGetErrorString(e);
     return MRT_ERR_OOM;
   }
@@ -747,12 +805,16 @@ WfHost* wf_create() { return new WfHost(); }
 size_t wf_device_bytes(const WfHost* H) {
   if (!H) return 0;
   const size_t cap = (size_t)H->capacity, sh = (size_t)H->sh_capacity;
-  return cap * (16 * 10 + 8 + 4 * (4 + H->vis_words) + 4 * kKinds) + sh * 32;
+  return cap * (16 * 10 + 8 + 4 * (4 + H->vis_words) + 4 * kKinds) + sh * (H->st.sh_key ? 40 : 32);
 }
 
 void wf_destroy(WfHost* H) {
   if (!H) return;
+  g_wf_bytes -= wf_device_bytes(H);
   for (void* p : H->allocs) cudaFree(p);
   if (H->graph) cudaGraphExecDestroy(H->graph);
+  if (H->side) cudaStreamDestroy(H->side);
+  if (H->ev_fork) cudaEventDestroy(H->ev_fork);
+  if (H->ev_join) cudaEventDestroy(H->ev_join);
   delete H;
 }

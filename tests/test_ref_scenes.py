@@ -88,3 +88,34 @@ def test_drop_in_renders_the_shipped_scene_like_the_reference(mrt, oracle, monke
     assert_same_image(gpu, cpu_batches(cpu_ref, n, 16), scene)
     lib.clean_shaders(sd)
     lib.clean_scene(g)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("scene", SCENES)
+def test_first_hit_colours_of_the_shipped_scene(mrt, oracle, monkeypatch, scene):
+    """render_mode 2 (the first hit's colour, textures and normal maps
+    applied: path_trace_normal, path_trace.c:78-89) is deterministic for a
+    shared offset: the drop-in's calc_one_sample and the reference's give
+    the same image."""
+    if not oracle.REF_LIB.exists():
+        pytest.fail("oracle/_ref/liboracle_ref.so (the reference) is needed to parse .rt files")
+    monkeypatch.chdir(ROOT)
+    oracle.ref_lib()
+    lib = C.CDLL(str(mrt.MINIRT_LIB_PATH))
+
+    class V3(C.Structure):
+        _fields_ = [("x", C.c_double), ("y", C.c_double), ("z", C.c_double)]
+
+    lib.calc_one_sample.restype, lib.calc_one_sample.argtypes = None, [C.c_void_p, V3, C.c_int]
+    lib.clean_shaders.restype, lib.clean_shaders.argtypes = None, [C.c_void_p]
+    a = oracle.RefOracle.from_rt(scene, W, H, DEPTH)
+    b = oracle.RefOracle.from_rt(scene, W, H, DEPTH)
+    for r in (a, b):
+        r.lib.refh_set_render_mode(r.h, 2)
+    lib.calc_one_sample(a.lib.refh_minirt(a.h), V3(0.25, 0.75, 0.0), DEPTH)
+    b.lib.refh_calc_one_sample(b.h, 0.25, 0.75, DEPTH)
+    ga, gb = a.accum(), b.accum()
+    close = np.abs(ga - gb).max(axis=2) <= 1e-3 * np.maximum(1.0, np.abs(gb).max(axis=2))
+    print(scene, "first-hit colours equal on", close.mean(), "of pixels")
+    assert close.mean() >= 0.99, close.mean()
+    lib.clean_shaders(a.lib.refh_shader_data(a.h))
