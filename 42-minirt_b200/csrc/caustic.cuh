@@ -35,6 +35,88 @@ __device__ __forceinline__ float node_far2(const float4& lo, const float4& hi, f
   return dx * dx + dy * dy + dz * dz;
 }
 
+// The k nearest photons with k <= kKnnReg: the sorted list lives in
+// registers (every index compile-time: a new distance bubbles in through one
+// compare-and-swap per slot, equal distances keeping their visit order), so
+// none of it goes to local memory. Same photons, same order and the same
+// estimate as the general walk below.
+constexpr int kKnnReg = 16;
+
+__device__ __forceinline__ float3 knn_estimate_reg(const SceneView& S, float3 p, float r2max) {
+  const int n = S.n_photons, k = S.knn;
+  int stack[kPhotonStack];
+  int sp = 0;
+  int kids[2] = {n == 1 ? ~0 : 0, n == 1 ? ~0 : 0};
+  int n_kids = n == 1 ? 1 : 0;
+  if (n > 1) stack[sp++] = 0;
+  int guard = 2 * n + 8;
+  float bd[kKnnReg];
+  int bi[kKnnReg];
+#pragma unroll
+  for (int t = 0; t < kKnnReg; ++t) { bd[t] = INFINITY; bi[t] = 0; }
+  int cnt = 0;
+  float kth = INFINITY;                  // bd[k - 1]
+  while ((sp > 0 || n_kids > 0) && --guard > 0) {
+    const float bound = cnt == k ? fminf(r2max, kth) : r2max;
+    if (n_kids == 0) {
+      const int nd = stack[--sp];
+      const float4 lo = __ldg(S.photon_nodes + 4 * nd), hi = __ldg(S.photon_nodes + 4 * nd + 1);
+      if (node_dist2(lo, hi, p) > bound) continue;
+      const float4 ch = __ldg(S.photon_nodes + 4 * nd + 3);
+      const int c0 = __float_as_int(ch.x), c1 = __float_as_int(ch.y);
+      // internal children pushed farther first; photon children next
+      float d0 = INFINITY, d1 = INFINITY;
+      if (c0 >= 0) d0 = node_dist2(__ldg(S.photon_nodes + 4 * c0), __ldg(S.photon_nodes + 4 * c0 + 1), p);
+      if (c1 >= 0) d1 = node_dist2(__ldg(S.photon_nodes + 4 * c1), __ldg(S.photon_nodes + 4 * c1 + 1), p);
+      if (c0 >= 0 && c1 >= 0) {
+        const bool swap = d0 < d1;
+        const int fa = swap ? c1 : c0, ne = swap ? c0 : c1;
+        const float dfa = swap ? d1 : d0, dne = swap ? d0 : d1;
+        if (dfa <= bound && sp < kPhotonStack) stack[sp++] = fa;
+        if (dne <= bound && sp < kPhotonStack) stack[sp++] = ne;
+      } else if (c0 >= 0) {
+        if (d0 <= bound && sp < kPhotonStack) stack[sp++] = c0;
+      } else if (c1 >= 0) {
+        if (d1 <= bound && sp < kPhotonStack) stack[sp++] = c1;
+      }
+      n_kids = 0;
+      if (c0 < 0) kids[n_kids++] = c0;
+      if (c1 < 0) kids[n_kids++] = c1;
+      continue;
+    }
+    const int i = ~kids[--n_kids];
+    const float4 q = __ldg(S.photon_pos + i);
+    const float dx = q.x - p.x, dy = q.y - p.y, dz = q.z - p.z;
+    float d2 = dx * dx + dy * dy + dz * dz;
+    if (d2 > r2max) continue;
+    if (cnt == k && d2 >= kth) continue;
+    if (cnt < k) ++cnt;
+    int id = i;
+#pragma unroll
+    for (int t = 0; t < kKnnReg; ++t) {
+      if (d2 < bd[t]) {
+        const float td = bd[t]; bd[t] = d2; d2 = td;
+        const int ti = bi[t]; bi[t] = id; id = ti;
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < kKnnReg; ++t)
+      if (t == k - 1) kth = bd[t];
+  }
+  if (cnt < k) return f3(0.f, 0.f, 0.f);
+  const float area = 3.14159265358979f * kth;
+  if (area < 1e-9f) return f3(0.f, 0.f, 0.f);
+  float3 sum = f3(0.f, 0.f, 0.f);
+#pragma unroll
+  for (int t = 0; t < kKnnReg; ++t) {
+    if (t < k) {
+      const float4 w = __ldg(S.photon_pow + bi[t]);
+      sum = sum + f3(w.x, w.y, w.z);
+    }
+  }
+  return sum * (S.inv_norm / area);
+}
+
 // kNN mode: sum of the k nearest photon powers / (pi r_k^2) / norm when the
 // k-th distance^2 <= caustic_radius; fixed-radius mode: sum within the
 // pass radius / (pi r^2) / norm.
@@ -81,6 +163,7 @@ __device__ __forceinline__ float3 caustic_estimate(const SceneView& S, float3 p)
     const float area = 3.14159265358979f * r2max;
     return sum * (S.inv_norm / area);
   }
+  if (S.knn <= kKnnReg) return knn_estimate_reg(S, p, r2max);
   const int k = S.knn;
   float bd[kKnnMax];
   int bi[kKnnMax];

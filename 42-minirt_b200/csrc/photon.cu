@@ -24,7 +24,6 @@
 // every gather scanned thousands of photons. The hierarchy adapts: a kNN
 // gather prunes by its k-th distance, a fixed-radius gather adds whole nodes
 // that lie inside the sphere.
-#include <cub/device/device_radix_sort.cuh>
 
 #include "kernels.h"
 #include "path.cuh"
@@ -290,8 +289,96 @@ cudaError_t launch_photon_emit(const SceneView& S, const PhotonEmit& P, int* sta
   return cudaGetLastError();
 }
 
+
+// ------------------------------------------------------------ radix sort
+// Stable LSD radix sort of the photons' 64-bit Morton codes with their
+// indices, 8 bits per pass: per tile of kSortTile elements a 256-bin
+// histogram (stored bin-major, so one exclusive scan over all of them gives
+// every (bin, tile) its first output slot in stable order), the scan, then a
+// scatter that ranks equal digits within each 256-element chunk of a tile
+// with warp matching and running per-digit counters.
+constexpr int kSortThreads = 256;
+constexpr int kSortTile = 4096;
+
+__global__ void __launch_bounds__(kSortThreads) radix_hist_kernel(const uint64_t* key, int n, int shift,
+                                                                  unsigned* hist, int tiles) {
+  __shared__ unsigned h[256];
+  h[threadIdx.x] = 0;
+  __syncthreads();
+  const int t0 = blockIdx.x * kSortTile;
+  for (int i = t0 + threadIdx.x; i < min(n, t0 + kSortTile); i += kSortThreads)
+    atomicAdd(&h[(key[i] >> shift) & 255u], 1u);
+  __syncthreads();
+  hist[(size_t)threadIdx.x * tiles + blockIdx.x] = h[threadIdx.x];
+}
+
+// Exclusive scan of m counters in place, one block.
+__global__ void __launch_bounds__(1024) radix_scan_kernel(unsigned* c, int m) {
+  __shared__ unsigned part[1024];
+  const int per = (m + 1023) / 1024;
+  const int a = threadIdx.x * per, b = min(m, a + per);
+  unsigned sum = 0;
+  for (int i = a; i < b; ++i) sum += c[i];
+  part[threadIdx.x] = sum;
+  __syncthreads();
+  for (int off = 1; off < 1024; off <<= 1) {
+    const unsigned v = threadIdx.x >= off ? part[threadIdx.x - off] : 0u;
+    __syncthreads();
+    part[threadIdx.x] += v;
+    __syncthreads();
+  }
+  unsigned run = part[threadIdx.x] - sum;
+  for (int i = a; i < b; ++i) {
+    const unsigned x = c[i];
+    c[i] = run;
+    run += x;
+  }
+}
+
+__global__ void __launch_bounds__(kSortThreads) radix_scatter_kernel(const uint64_t* key, const uint32_t* val,
+                                                                     uint64_t* okey, uint32_t* oval, int n,
+                                                                     int shift, const unsigned* hist, int tiles) {
+  constexpr int kWarps = kSortThreads / 32;
+  __shared__ unsigned base[256];            // next output slot of each digit in this tile
+  __shared__ unsigned wcount[kWarps][256];  // digit counts per warp in the current chunk
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  base[threadIdx.x] = hist[(size_t)threadIdx.x * tiles + blockIdx.x];
+  const int t0 = blockIdx.x * kSortTile;
+  for (int c0 = t0; c0 < min(n, t0 + kSortTile); c0 += kSortThreads) {
+    for (int w = 0; w < kWarps; ++w) wcount[w][threadIdx.x] = 0;
+    __syncthreads();
+    const int i = c0 + threadIdx.x;
+    const bool ok = i < n && i < t0 + kSortTile;
+    uint64_t k = 0;
+    uint32_t v = 0;
+    unsigned d = 256;                        // no digit: beyond the tile
+    if (ok) {
+      k = key[i];
+      v = val[i];
+      d = (unsigned)((k >> shift) & 255u);
+    }
+    const unsigned peers = __match_any_sync(0xffffffffu, d);
+    const unsigned rank = __popc(peers & ((1u << lane) - 1u));
+    if (ok && lane == __ffs(peers) - 1) wcount[warp][d] = __popc(peers);
+    __syncthreads();
+    unsigned before = 0;                     // this digit in earlier warps of the chunk
+    if (ok)
+      for (int w = 0; w < warp; ++w) before += wcount[w][d];
+    if (ok) {
+      const unsigned dst = base[d] + before + rank;
+      okey[dst] = k;
+      oval[dst] = v;
+    }
+    __syncthreads();
+    unsigned tot = 0;
+    for (int w = 0; w < kWarps; ++w) tot += wcount[w][threadIdx.x];
+    base[threadIdx.x] += tot;
+    __syncthreads();
+  }
+}
+
 // Scratch: bounds (6 ints), code (n, 64-bit), idx (n), sorted code, sorted idx
-// (n), CUB temp; stream-ordered allocations released at the end.
+// (n), radix-sort histograms; stream-ordered allocations released at the end.
 cudaError_t launch_photon_tree(const PhotonTree& T, cudaStream_t st) {
   if (T.n == 0) return cudaSuccess;
   int* bounds = nullptr;
@@ -313,9 +400,30 @@ cudaError_t launch_photon_tree(const PhotonTree& T, cudaStream_t st) {
   const unsigned g = (T.n + b - 1) / b;
   photon_bounds_kernel<<<g, b, 0, st>>>(T, bounds);
   morton_kernel<<<g, b, 0, st>>>(T, bounds, code, idx);
-  cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, code, scode, idx, sidx, (int)T.n, 0, 63, st);
-  if ((e = cudaMallocAsync(&tmp, tmp_bytes, st)) != cudaSuccess) return e;
-  cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, code, scode, idx, sidx, (int)T.n, 0, 63, st);
+  {
+    // eight 8-bit passes over the 63-bit codes, ping-pong: the result lands
+    // back in (code, idx)
+    const int n = (int)T.n;
+    const int tiles = (n + kSortTile - 1) / kSortTile;
+    tmp_bytes = sizeof(unsigned) * 256 * (size_t)tiles;
+    if ((e = cudaMallocAsync(&tmp, tmp_bytes, st)) != cudaSuccess) return e;
+    unsigned* hist = static_cast<unsigned*>(tmp);
+    uint64_t* kin = code;
+    uint64_t* kout = scode;
+    uint32_t* vin = idx;
+    uint32_t* vout = sidx;
+    for (int pass = 0; pass < 8; ++pass) {
+      radix_hist_kernel<<<tiles, kSortThreads, 0, st>>>(kin, n, 8 * pass, hist, tiles);
+      radix_scan_kernel<<<1, 1024, 0, st>>>(hist, 256 * tiles);
+      radix_scatter_kernel<<<tiles, kSortThreads, 0, st>>>(kin, vin, kout, vout, n, 8 * pass, hist, tiles);
+      std::swap(kin, kout);
+      std::swap(vin, vout);
+    }
+    scode = kin;   // sorted codes and indices
+    sidx = vin;
+    code = kout;   // the other buffers, freed below like these
+    idx = vout;
+  }
   photon_gather_kernel<<<g, b, 0, st>>>(T, sidx);
   if (T.n > 1) {
     int *parent_node = nullptr, *parent_leaf = nullptr;
