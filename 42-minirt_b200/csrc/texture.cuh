@@ -35,6 +35,18 @@ __device__ __forceinline__ float3 solid_checker(float3 p, float scale, float3 c1
 }
 
 // Texture k (1-based): rgb and alpha / 255.
+// The texel the reference reads for (u, v): one linear index,
+// width * (int)(v * (h - 1)) + (int)(u * (w - 1)) (get_tex_color.c:37,
+// apply_map.c:45-47), so a u beyond [0, 1] runs on into the neighbouring
+// row rather than clamping to the edge. Where that index leaves the image
+// (the reference then reads outside its buffer) it is clamped to it.
+__device__ __forceinline__ uchar4 texel_at(const SceneView& S, const TexD& t, float u, float v) {
+  long long i = (long long)t.w * (int)(v * (float)(t.h - 1)) + (int)(u * (float)(t.w - 1));
+  const long long n = (long long)t.w * t.h;
+  i = i < 0 ? 0 : (i >= n ? n - 1 : i);
+  return __ldg(S.texels + t.offset + (size_t)i);
+}
+
 __device__ __forceinline__ float4 tex_lookup(const SceneView& S, int k, float u, float v, float3 p) {
   const TexD& t = S.texs[k - 1];
   if (t.type == 0) {   // IMAGE
@@ -42,9 +54,7 @@ __device__ __forceinline__ float4 tex_lookup(const SceneView& S, int k, float u,
       const float3 c = solid_checker(p, 2.0f, f3(0.f, 0.f, 0.f), f3(243.f / 255.f, 0.f, 243.f / 255.f));
       return make_float4(c.x, c.y, c.z, 1.f);
     }
-    const int x = min(max((int)(u * (float)(t.w - 1)), 0), t.w - 1);
-    const int y = min(max((int)(v * (float)(t.h - 1)), 0), t.h - 1);
-    const uchar4 q = __ldg(S.texels + t.offset + (size_t)y * t.w + x);
+    const uchar4 q = texel_at(S, t, u, v);
     const float s = 1.0f / 255.0f;
     return make_float4(q.x * s, q.y * s, q.z * s, q.w * s);
   }
@@ -192,9 +202,7 @@ __device__ __forceinline__ bool alpha_drops(const SceneView& S, int i, int type,
 __device__ __forceinline__ float3 normal_map(const SceneView& S, const MatTexD& mt, float u, float v, float3 n) {
   const TexD& t = S.texs[mt.tex[TS_NORMAL] - 1];
   if (t.w <= 0) return n;           // any type, as long as it has an image
-  const int x = min(max((int)(u * (float)(t.w - 1)), 0), t.w - 1);
-  const int y = min(max((int)(v * (float)(t.h - 1)), 0), t.h - 1);
-  const uchar4 q = __ldg(S.texels + t.offset + (size_t)y * t.w + x);
+  const uchar4 q = texel_at(S, t, u, v);
   const float3 mp = f3(q.x / 127.5f - 1.0f, q.y / 127.5f - 1.0f, q.z / 127.5f - 1.0f);
   float3 tg = cross(n, f3(0.f, -1.f, 0.f));
   if (len2(tg) == 0.0f) tg = cross(n, f3(0.f, 0.f, 1.f));

@@ -187,6 +187,7 @@ def convergence(ctx, sc, config: str, spp_step: int, forms: dict, fid: int, cap_
     forms (same estimator, same paths) it is that sample count at their
     measured rate. c = relMSE * N fitted over the run is reported beside it."""
     import convergence as cv
+    import mrt
     path = REPO / "tests" / "golden" / f"conv_{config}.npz"
     if not path.exists():
         return {"unavailable": f"no converged-radiance fixture for {config}"}
@@ -195,7 +196,8 @@ def convergence(ctx, sc, config: str, spp_step: int, forms: dict, fid: int, cap_
     ctx.clear()
     done, ms, trace, reached = 0, 0.0, [], None
     while done < cap_spp:
-        st = ctx.render(spp_step, seed=31, sample_base=done, form=fid)
+        st = ctx.render(spp_step, seed=31, sample_base=done, form=fid,
+                        use_graph=1 if fid == mrt.FORM_WAVEFRONT else 0)
         ms += st.ms
         done += spp_step
         img, n = ctx.read_accum()
@@ -501,7 +503,8 @@ def main() -> int:
         try:
             ctx.clear()
             for w in range(a.warmup):
-                ctx.render(spp, seed=99, sample_base=w * spp, form=fid)
+                ctx.render(spp, seed=99, sample_base=w * spp, form=fid,
+                           use_graph=1 if fid == mrt.FORM_WAVEFRONT else 0)
         except mrt.MRTError as e:
             forms[name] = {"error": str(e)[:200]}
             continue
@@ -511,7 +514,8 @@ def main() -> int:
         launches = 0
         base, _ = D.shard_samples(a.steps * spp * world, world, rank)
         for s in range(a.steps):
-            st = ctx.render(spp, seed=1, sample_base=base + s * spp, form=fid)
+            st = ctx.render(spp, seed=1, sample_base=base + s * spp, form=fid,
+                            use_graph=1 if fid == mrt.FORM_WAVEFRONT else 0)
             ms += st.ms
             launches += st.kernel_launches
         if dist:
@@ -547,7 +551,8 @@ def main() -> int:
     t0 = time.perf_counter()
     for s in range(a.steps):
         ctx.set_camera(cam, sc.ior_all, sc.ambient_ratio)
-        ctx.render(spp, seed=2, sample_base=rank * a.steps * spp + s * spp, form=fid)
+        ctx.render(spp, seed=2, sample_base=rank * a.steps * spp + s * spp, form=fid,
+                   use_graph=1 if fid == mrt.FORM_WAVEFRONT else 0)
         if dist:
             # every step's frame summed on rank 0 (mrt_reduce_frame), read
             # back there; the other ranks drop their consumed partial frame
