@@ -25,6 +25,17 @@
 #include <stdio.h>
 #include <string.h>
 
+/* gpu_bvh_sah(1): build this library's SAH tree instead of the
+ * reference's (faster on large meshes; exact-t ties may then resolve to
+ * another of the tied primitives). render_mode 1 always uses the
+ * reference's tree. */
+static int	g_sah_bvh = 0;
+
+void	gpu_bvh_sah(int on)
+{
+	g_sah_bvh = on != 0;
+}
+
 static void	err_line(const char *what)
 {
 	fprintf(stderr, "\033[0;31m[Error]\033[0m %s: %s\n", what, mrt_last_error());
@@ -363,8 +374,11 @@ static int	flatten(t_minirt *mrt, t_scene *s, t_flat *f)
  * triangles, as flatten lays them out), with the position its median split
  * sorts by (get_obj_position, bvh_utils.c:88: the object's position, or a
  * triangle's centre as its loader stored it). Selects the reference's own
- * tree for the next build, so that render_mode 1 reports hit_bvh's visit
- * counts (bvh_hit.c:16). */
+ * tree for the next build, traversed left child first: the first hit
+ * among primitives at exactly the same t is then the one hit_bvh keeps
+ * (bvh_hit.c:31-36, the left subtree wins a tie), e.g. the coincident
+ * wall faces of scenes/obj/cube.rt, and render_mode 1 reports hit_bvh's
+ * visit counts (bvh_hit.c:16). */
 static int	set_reference_bvh(t_minirt *mrt, t_scene *s, const t_flat *f)
 {
 	const int64_t	tb = f->d.n_spheres + f->d.n_cylinders + f->d.n_cones
@@ -446,7 +460,7 @@ int	convert_scene_build(t_minirt *minirt, t_scene *scene, t_viewport *vp,
 		free_flat(&f);
 		return (-1);
 	}
-	if (minirt->render_mode == 1)
+	if (!g_sah_bvh || minirt->render_mode == 1)
 	{
 		if (set_reference_bvh(minirt, scene, &f))
 		{

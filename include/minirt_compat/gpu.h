@@ -26,6 +26,11 @@ void	compute_frame_gpu(t_minirt *minirt);
 /* clean_shaders.c:69 / :32 */
 void	clean_shaders(t_shader_data *shader_data);
 void	clean_scene(t_gpu_structs *gpu_structs);
+/* Not in the reference: the BVH that convert_scene_build builds. By
+ * default the reference's own median-split tree (bvh_build.c:104), so that
+ * exact-t ties resolve as on the CPU; gpu_bvh_sah(1) selects this
+ * library's SAH tree (faster on large meshes). */
+void	gpu_bvh_sah(int on);
 /* send_uniforms.c:63, importance_sampling.c:69 — parameters now travel with
  * convert_scene / convert_scene_build, so these are kept as no-ops. */
 void	send_uniforms(t_minirt *minirt);
