@@ -147,6 +147,7 @@ struct mrt_ctx {
   bool has_scene = false;
   // scene
   DevBuf<Node> nodes;
+  DevBuf<WNode> wnodes;
   DevBuf<float4> geom, shade;
   DevBuf<int4> meta;
   DevBuf<PlaneD> planes;
@@ -396,7 +397,7 @@ void mrt_destroy(mrt_ctx* c) {
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
   c->accum.release(); c->depth.release(); c->status.release(); c->counters.release();
-  c->nodes.release(); c->geom.release(); c->shade.release(); c->meta.release();
+  c->nodes.release(); c->wnodes.release(); c->geom.release(); c->shade.release(); c->meta.release();
   c->planes.release(); c->mats.release(); c->lights.release(); c->point_lights.release();
   c->rgbe.release(); c->pdf_joint.release(); c->cdf_m.release(); c->cdf_c.release();
   c->alias.release(); c->env_rec0.release(); c->env_rec1.release();
@@ -676,6 +677,13 @@ extern "C" int mrt_scene_build(mrt_ctx* c, const mrt_scene_desc* d) {
   BvhResult bvh;
   std::string err;
   std::vector<double> dboxes;
+  // the wide traversal is compiled into the SceneView kernels only
+  bool has_quadrics_or_textures = (d->n_cylinders + d->n_cones + d->n_hyperboloids) > 0;
+  for (int i = 0; i < d->n_materials && !has_quadrics_or_textures; ++i) {
+    const mrt_material& m = d->materials[i];
+    has_quadrics_or_textures = m.color_tex || m.metallic_tex || m.roughness_tex || m.transmission_tex || m.ao_tex ||
+                               m.emission_strength_tex || m.emission_color_tex || m.normal_tex;
+  }
   if (ref_tree) {
     std::vector<uint32_t> list(n_prims);
     if (!c->bvh_list.empty()) {
@@ -701,7 +709,14 @@ extern "C" int mrt_scene_build(mrt_ctx* c, const mrt_scene_desc* d) {
     }
     if (!build_bvh_reference(refp, list, bvh, dboxes, err))
       return set_err(MRT_ERR_INVALID, "BVH: %s", err.c_str());
-  } else if (!build_bvh(boxes, bvh, err)) {
+  } else if (c->bvh_mode != MRT_BVH_WIDE || has_quadrics_or_textures) {
+    if (!build_bvh(boxes, bvh, err)) return set_err(MRT_ERR_INVALID, "BVH: %s", err.c_str());
+  } else if (!build_bvh_wide(boxes, bvh, err)) {
+    // a tree deeper than the wide stack, or a box beyond the quantisation
+    // range: the binary tree instead
+    err.clear();
+    if (!build_bvh(boxes, bvh, err)) return set_err(MRT_ERR_INVALID, "BVH: %s", err.c_str());
+  } else if (!check_bvh_wide(bvh, boxes, err)) {
     return set_err(MRT_ERR_INVALID, "BVH: %s", err.c_str());
   }
   c->bvh_depth = bvh.max_depth;
@@ -813,6 +828,7 @@ extern "C" int mrt_scene_build(mrt_ctx* c, const mrt_scene_desc* d) {
   }
 
   CK(c->nodes.upload(bvh.nodes.data(), bvh.nodes.size(), st));
+  CK(c->wnodes.upload(bvh.wnodes.data(), bvh.wnodes.size(), st));
   CK(c->geom.upload(geom.data(), geom.size(), st));
   CK(c->meta.upload(meta.data(), meta.size(), st));
   CK(c->shade.upload(shade.data(), shade.size(), st));
@@ -881,12 +897,16 @@ extern "C" int mrt_scene_build(mrt_ctx* c, const mrt_scene_desc* d) {
   v.mats = c->mats.p;
   v.lights = c->lights.p;
   v.n_nodes = (int)bvh.nodes.size();
+  v.wnodes = bvh.wnodes.empty() ? nullptr : c->wnodes.p;
+  v.n_wnodes = (int)bvh.wnodes.size();
   v.n_prims = (int)n_prims;
   v.n_planes = d->n_planes;
   v.n_mats = d->n_materials;
   v.n_lights = d->n_lights;
   v.has_bvh = n_prims > 0;
   v.has_quadrics = (d->n_cylinders + d->n_cones + d->n_hyperboloids) > 0;
+  if (v.wnodes && (v.has_quadrics || v.has_textures))   // only the SceneView kernels traverse it
+    return set_err(MRT_ERR_INVALID, "wide BVH built for a scene with quadrics or textures");
   v.root_leaf = bvh.root_leaf;
   v.left_first = ref_tree ? 1 : 0;
   v.ref_boxes = nullptr;
@@ -988,7 +1008,7 @@ extern "C" int mrt_scene_build(mrt_ctx* c, const mrt_scene_desc* d) {
     if (rc2) return rc2;
   }
   CK(cudaStreamSynchronize(st));
-  c->scene_bytes = c->nodes.bytes() + c->geom.bytes() + c->meta.bytes() + c->shade.bytes() +
+  c->scene_bytes = c->nodes.bytes() + c->wnodes.bytes() + c->geom.bytes() + c->meta.bytes() + c->shade.bytes() +
                    c->planes.bytes() + c->mats.bytes() + c->lights.bytes() + c->rgbe.bytes() +
                    c->pdf_joint.bytes() + c->cdf_m.bytes() + c->cdf_c.bytes() + c->alias.bytes() +
                    c->env_rec0.bytes() + c->env_rec1.bytes() + c->ph_pos.bytes() + c->ph_pow.bytes() + c->ph_nodes.bytes();
@@ -2006,11 +2026,43 @@ extern "C" void mrt_shard_samples(int64_t total, int32_t world, int32_t rank, in
 extern "C" int mrt_set_bvh_options(mrt_ctx* c, const mrt_bvh_options* o) {
   int rc = check_ctx(c);
   if (rc) return rc;
-  if (!o || (o->mode != MRT_BVH_SAH && o->mode != MRT_BVH_REFERENCE) || o->n_prims < 0)
+  if (!o || (o->mode != MRT_BVH_SAH && o->mode != MRT_BVH_REFERENCE && o->mode != MRT_BVH_WIDE) ||
+      o->n_prims < 0)
     return set_err(MRT_ERR_INVALID, "mrt_set_bvh_options: mode %d", o ? o->mode : -1);
   c->bvh_mode = o->mode;
   c->bvh_list.assign(o->order ? o->order : nullptr, o->order ? o->order + o->n_prims : nullptr);
   c->bvh_pos.assign(o->positions ? o->positions : nullptr, o->positions ? o->positions + 3 * o->n_prims : nullptr);
+  return MRT_OK;
+}
+
+// Host-only build of the binary SAH (default) or 8-wide tree over n boxes
+// (min xyz, max xyz per box, double) followed by the structural check of the
+// wide tree; stats[0..3] = nodes, depth, leaves, wide (1) or binary (0).
+extern "C" int mrt_bvh_build_check(const double* boxes, int64_t n, int32_t mode, int64_t* stats) {
+  if (!boxes || n <= 0 || n >= (int64_t)1 << 28 || (mode != MRT_BVH_SAH && mode != MRT_BVH_WIDE))
+    return set_err(MRT_ERR_INVALID, "mrt_bvh_build_check: bad arguments");
+  std::vector<PrimBox> prims((size_t)n);
+  for (int64_t i = 0; i < n; ++i) {
+    for (int k = 0; k < 6; ++k)
+      if (!std::isfinite(boxes[6 * i + k])) return set_err(MRT_ERR_INVALID, "mrt_bvh_build_check: box %lld", (long long)i);
+    prim_box_from_double(prims[(size_t)i], boxes + 6 * i, boxes + 6 * i + 3);
+  }
+  BvhResult bvh;
+  std::string err;
+  bool wide = false;
+  if (mode == MRT_BVH_WIDE && build_bvh_wide(prims, bvh, err)) {
+    wide = true;
+    if (!check_bvh_wide(bvh, prims, err)) return set_err(MRT_ERR_INVALID, "BVH: %s", err.c_str());
+  } else {
+    err.clear();
+    if (!build_bvh(prims, bvh, err)) return set_err(MRT_ERR_INVALID, "BVH: %s", err.c_str());
+  }
+  if (stats) {
+    stats[0] = wide ? (int64_t)bvh.wnodes.size() : (int64_t)bvh.nodes.size();
+    stats[1] = bvh.max_depth;
+    stats[2] = bvh.leaves;
+    stats[3] = wide ? 1 : 0;
+  }
   return MRT_OK;
 }
 

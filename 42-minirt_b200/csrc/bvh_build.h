@@ -15,6 +15,7 @@ struct PrimBox {
 
 struct BvhResult {
   std::vector<Node> nodes;        // device nodes, root at 0
+  std::vector<WNode> wnodes;      // 8-wide tree (build_bvh_wide), root at 0
   std::vector<uint32_t> order;    // leaf order -> input primitive index
   int root_leaf = 0;              // non-zero when the whole scene is one leaf
   int max_depth = 0;
@@ -23,6 +24,10 @@ struct BvhResult {
 
 void prim_box_from_double(PrimBox& p, const double* mn, const double* mx);
 bool build_bvh(const std::vector<PrimBox>& prims, BvhResult& out, std::string& err);
+// The 8-wide tree with quantised child boxes (WNode); out.nodes stays empty.
+bool build_bvh_wide(const std::vector<PrimBox>& prims, BvhResult& out, std::string& err);
+// Structural check of a wide tree against its primitives (host, O(n)).
+bool check_bvh_wide(const BvhResult& t, const std::vector<PrimBox>& prims, std::string& err);
 
 // A primitive of the reference-topology build: its bounds as the reference
 // computes them (compute_object_bounds, bvh_math.c:17) and the position its

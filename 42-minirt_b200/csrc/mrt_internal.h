@@ -7,6 +7,8 @@
 //             (float4 x-y of left, float4 x-y of right, float4 z of both,
 //             int4 child links). A negative link is a leaf:
 //             ~(first_prim << 3 | (count - 1)), up to 8 primitives.
+//   wnodes  : the MRT_BVH_WIDE option: 8-wide, 80 B per node (WNode
+//             below), leaves of up to 4 primitives, siblings contiguous.
 //   geom    : 48 B per primitive in leaf order. Triangle: (v0, type) (e1, -)
 //             (e2, -). Sphere: (centre, type) (radius, r^2, -, -) (-).
 //   meta    : int4 per primitive in leaf order: (flat id, material, type,
@@ -44,6 +46,30 @@ struct __align__(16) Node {
 __host__ __device__ inline int leaf_link(uint32_t first, uint32_t count) {
   return ~(int)((first << 3) | (count - 1));
 }
+
+// 8-wide BVH node with 8-bit quantised child boxes (the compressed wide BVH
+// of Ylitie, Karras and Laine, HPG 2017, in this library's own packing), 80 B:
+//   a: origin p.xyz, w = bits ex | ey << 8 | ez << 16 | imask << 24
+//      (child box along x: p.x + q * 2^(ex - 127), q in 0..255)
+//   b: (child_base, prim_base, meta of slots 0-3, meta of slots 4-7)
+//   c: (qlo.x slots 0-3, qlo.x 4-7, qlo.y 0-3, qlo.y 4-7)
+//   d: (qlo.z 0-3, qlo.z 4-7, qhi.x 0-3, qhi.x 4-7)
+//   e: (qhi.y 0-3, qhi.y 4-7, qhi.z 0-3, qhi.z 4-7)
+// A slot's meta byte is 0 when empty, else has bit 7 set. imask bit s marks
+// slot s as an internal child: node child_base + popc(imask below s). A
+// leaf slot holds ((meta >> 5) & 3) + 1 primitives from prim_base +
+// (meta & 31). Children sit in the slot whose octant they lie towards, so
+// visiting slots in the order of slot ^ (the ray's sign bits) is roughly
+// near to far.
+struct __align__(16) WNode {
+  float4 a;
+  int4 b;
+  int4 c;
+  int4 d;
+  int4 e;
+};
+constexpr int kWideLeafMax = 4;      // primitives per leaf slot
+constexpr int kWideStack = 32;       // node-group entries (2 ints each) in the 64-int stack
 
 struct MaterialD {
   float color[3];        // color_value / 255
@@ -126,6 +152,8 @@ struct SceneView {
   int has_textures;      // launch the SceneViewT instantiation
   int left_first;        // traverse the left child first (reference-topology tree), else the nearer
   const double* ref_boxes;  // reference-topology tree: double child boxes for its node-visit count
+  const WNode* wnodes;   // when set: the 8-wide tree, traversed instead of `nodes`
+  int n_wnodes;
   const MatTexD* mat_tex;    // per material
   const TexD* texs;
   const uchar4* texels;

@@ -1,4 +1,5 @@
-// traverse.cuh — closest-hit and any-hit queries over the BVH2 + planes.
+// traverse.cuh — closest-hit and any-hit queries over the BVH (the binary
+// tree, or the 8-wide tree in the SceneView instantiation) + planes.
 //
 // Semantics follow hit_register_all (hit_register.c:79-120): BVH primitives
 // (spheres, triangles, and in the SceneViewQ instantiation cylinders, cones
@@ -134,6 +135,191 @@ struct LocalStack {
   __device__ __forceinline__ int get(int i) const { return s[i]; }
 };
 
+// 8-wide tree (WNode). One node per iteration: its up-to-8 quantised child
+// boxes are tested against the ray clipped to [0, tbest]; hit leaves are
+// intersected at once, near to far; the nearest hit internal child is
+// visited next and the node's other hit internal children are pushed as
+// one group entry (child_base, remaining hit bits << 8 | imask), two ints
+// of the stack. Visit order is the ray's octant applied to the slots (key
+// = slot ^ sign bits, lowest key first). Slab test per child and axis:
+// t = q * (2^e / d) + (p - o) / d, one fma.
+struct WideHits {
+  uint32_t inner;    // hit internal children, bit = key
+  uint32_t leaf;     // hit leaves, bit = key
+};
+
+// Byte j of w as a float, exactly: the byte under the exponent of 2^23
+// (one byte permute) minus 2^23 (one add), instead of an integer-to-float
+// conversion, which issues at a fraction of the FP32 rate.
+__device__ __forceinline__ float qbyte(uint32_t w, int j) {
+  return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u + (uint32_t)j)) - 8388608.0f;
+}
+
+__device__ __forceinline__ WideHits wide_children(const WNode* nd, float3 o, float3 inv, uint32_t oct,
+                                                  float tmax, int4& b, uint32_t& imask) {
+  const float4 a = ldg4(&nd->a);
+  b = ldg4(&nd->b);
+  const int4 c = ldg4(&nd->c), d = ldg4(&nd->d), e = ldg4(&nd->e);
+  const uint32_t w = __float_as_uint(a.w);
+  imask = w >> 24;
+  const float ax = __uint_as_float((w & 0xffu) << 23) * inv.x;
+  const float ay = __uint_as_float(((w >> 8) & 0xffu) << 23) * inv.y;
+  const float az = __uint_as_float(((w >> 16) & 0xffu) << 23) * inv.z;
+  const float bx = (a.x - o.x) * inv.x, by = (a.y - o.y) * inv.y, bz = (a.z - o.z) * inv.z;
+  WideHits h{0u, 0u};
+  // near and far planes per axis: the low bytes for a non-negative direction
+  // component, the high bytes for a negative one (NaNs of zero components
+  // drop out of fminf / fmaxf, leaving the box conservative)
+  const bool fx = oct & 1u, fy = oct & 2u, fz = oct & 4u;
+#pragma unroll
+  for (int half = 0; half < 2; ++half) {
+    const uint32_t meta = (uint32_t)(half ? b.w : b.z);
+    const uint32_t lx = (uint32_t)(half ? c.y : c.x), ly = (uint32_t)(half ? c.w : c.z);
+    const uint32_t lz = (uint32_t)(half ? d.y : d.x), hx = (uint32_t)(half ? d.w : d.z);
+    const uint32_t hy = (uint32_t)(half ? e.y : e.x), hz = (uint32_t)(half ? e.w : e.z);
+    const uint32_t nx = fx ? hx : lx, ny = fy ? hy : ly, nz = fz ? hz : lz;
+    const uint32_t gx = fx ? lx : hx, gy = fy ? ly : hy, gz = fz ? lz : hz;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int sh = 8 * j;
+      const float tnx = fmaf(qbyte(nx, j), ax, bx), tfx = fmaf(qbyte(gx, j), ax, bx);
+      const float tny = fmaf(qbyte(ny, j), ay, by), tfy = fmaf(qbyte(gy, j), ay, by);
+      const float tnz = fmaf(qbyte(nz, j), az, bz), tfz = fmaf(qbyte(gz, j), az, bz);
+      const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));
+      const float tf = fminf(fminf(tfx, tfy), fminf(tfz, tmax));
+      const int slot = 4 * half + j;
+      if (((meta >> sh) & 0x80u) && tn <= tf) {
+        const uint32_t bit = 1u << ((uint32_t)slot ^ oct);
+        if ((imask >> slot) & 1u) h.inner |= bit;
+        else h.leaf |= bit;
+      }
+    }
+  }
+  return h;
+}
+
+__device__ __forceinline__ int wide_child(int base, uint32_t imask, uint32_t key, uint32_t oct) {
+  const uint32_t slot = key ^ oct;
+  return base + __popc(imask & ((1u << slot) - 1u));
+}
+
+// Leaf slot `key` of a node: its primitive range.
+__device__ __forceinline__ void wide_leaf(const int4& b, uint32_t key, uint32_t oct, int& first, int& count) {
+  const uint32_t slot = key ^ oct;
+  const uint32_t m = ((uint32_t)(slot < 4 ? b.z : b.w) >> (8 * (slot & 3))) & 0xffu;
+  first = b.y + (int)(m & 31u);
+  count = (int)((m >> 5) & 3u) + 1;
+}
+
+template <bool kCount, class V, class Stack>
+__device__ __forceinline__ void wide_closest(const V& S, float3 o, float3 d, float& tbest, int& best, float& bu,
+                                             float& bv, int& visits, int* status, Stack& stack, uint64_t akey) {
+  const float3 inv = f3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+  const uint32_t oct = (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u);
+  int sp = 0;
+  int cur = 0;
+  int budget = 2 * S.n_wnodes + S.n_prims + 64;
+  while (true) {
+    if (--budget < 0) {
+      if (status) atomicOr(status, ST_BUDGET);
+      return;
+    }
+    int4 b;
+    uint32_t imask;
+    if (kCount) visits++;
+    WideHits h = wide_children(S.wnodes + cur, o, inv, oct, tbest, b, imask);
+    while (h.leaf) {
+      const uint32_t key = (uint32_t)(__ffs(h.leaf) - 1);
+      h.leaf &= h.leaf - 1u;
+      int first, count;
+      wide_leaf(b, key, oct, first, count);
+      for (int i = first; i < first + count; ++i) {
+        float t, u = 0.f, v = 0.f;
+        if (prim_hit(S, i, o, d, tbest, t, u, v, akey)) { tbest = t; best = i; bu = u; bv = v; }
+      }
+    }
+    if (h.inner) {
+      const uint32_t key = (uint32_t)(__ffs(h.inner) - 1);
+      h.inner &= h.inner - 1u;
+      if (h.inner) {
+        if (sp < kWideStack) {
+          stack.put(2 * sp, b.x);
+          stack.put(2 * sp + 1, (int)((h.inner << 8) | imask));
+          ++sp;
+        } else if (status) {
+          atomicOr(status, ST_STACK);
+        }
+      }
+      cur = wide_child(b.x, imask, key, oct);
+      continue;
+    }
+    if (sp == 0) return;
+    const int base = stack.get(2 * sp - 2);
+    const uint32_t g = (uint32_t)stack.get(2 * sp - 1);
+    uint32_t rest = g >> 8;
+    const uint32_t im = g & 0xffu;
+    const uint32_t key = (uint32_t)(__ffs(rest) - 1);
+    rest &= rest - 1u;
+    if (rest) stack.put(2 * sp - 1, (int)((rest << 8) | im));
+    else --sp;
+    cur = wide_child(base, im, key, oct);
+  }
+}
+
+template <class V, class Stack>
+__device__ __forceinline__ bool wide_any(const V& S, float3 o, float3 d, float tlim, int* status, Stack& stack,
+                                         uint64_t akey) {
+  const float3 inv = f3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
+  const uint32_t oct = (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u);
+  int sp = 0;
+  int cur = 0;
+  int budget = 2 * S.n_wnodes + S.n_prims + 64;
+  while (true) {
+    if (--budget < 0) {
+      if (status) atomicOr(status, ST_BUDGET);
+      return false;
+    }
+    int4 b;
+    uint32_t imask;
+    WideHits h = wide_children(S.wnodes + cur, o, inv, oct, tlim, b, imask);
+    while (h.leaf) {
+      const uint32_t key = (uint32_t)(__ffs(h.leaf) - 1);
+      h.leaf &= h.leaf - 1u;
+      int first, count;
+      wide_leaf(b, key, oct, first, count);
+      for (int i = first; i < first + count; ++i) {
+        float t, u, v;
+        if (prim_hit(S, i, o, d, tlim, t, u, v, akey)) return true;
+      }
+    }
+    if (h.inner) {
+      const uint32_t key = (uint32_t)(__ffs(h.inner) - 1);
+      h.inner &= h.inner - 1u;
+      if (h.inner) {
+        if (sp < kWideStack) {
+          stack.put(2 * sp, b.x);
+          stack.put(2 * sp + 1, (int)((h.inner << 8) | imask));
+          ++sp;
+        } else if (status) {
+          atomicOr(status, ST_STACK);
+        }
+      }
+      cur = wide_child(b.x, imask, key, oct);
+      continue;
+    }
+    if (sp == 0) return false;
+    const int base = stack.get(2 * sp - 2);
+    const uint32_t g = (uint32_t)stack.get(2 * sp - 1);
+    uint32_t rest = g >> 8;
+    const uint32_t im = g & 0xffu;
+    const uint32_t key = (uint32_t)(__ffs(rest) - 1);
+    rest &= rest - 1u;
+    if (rest) stack.put(2 * sp - 1, (int)((rest << 8) | im));
+    else --sp;
+    cur = wide_child(base, im, key, oct);
+  }
+}
+
 // Closest hit. `visits` counts node fetches (heat-map / roofline counter).
 // Returns false on a miss. `status` receives ST_BUDGET if the bounded loop
 // ran out (a corrupted tree), never hangs.
@@ -143,14 +329,26 @@ struct LocalStack {
 // megakernels all use this loop: on B200 it measured 5 % faster in the
 // wavefront (c1) than the while-while loop with speculative leaf
 // postponement (Aila & Laine, HPG 2009) that the wavefront used first.
-template <bool kCount, class V, class Stack>
+// kTree: kTreeAny picks the tree at run time (S.wnodes); kTreeBinary and
+// kTreeWide compile one traversal only (the wavefront's extend and connect
+// kernels, launched per tree, so that neither carries the other's registers).
+enum TreeSel : int { kTreeAny = 0, kTreeBinary = 1, kTreeWide = 2 };
+
+template <bool kCount, int kTree = kTreeAny, class V, class Stack>
 __device__ __forceinline__ bool closest_hit_compact(const V& S, float3 o, float3 d, HitInfo& hit,
                                                     int& visits, int* status, Stack& stack,
                                                     uint64_t akey = 0) {
   float tbest = kTMax;
   int best = kMiss;
   float bu = 0.f, bv = 0.f;
-  if (S.has_bvh) {
+  bool wide = false;
+  if constexpr (!V::kQuadrics && kTree != kTreeBinary) {
+    if (S.has_bvh && (kTree == kTreeWide || S.wnodes)) {
+      wide_closest<kCount>(S, o, d, tbest, best, bu, bv, visits, status, stack, akey);
+      wide = true;
+    }
+  }
+  if (kTree != kTreeWide && S.has_bvh && !wide) {
     float3 inv = f3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
     float3 oi = o * inv;
     int sp = 0;
@@ -209,7 +407,7 @@ __device__ __forceinline__ bool closest_hit_compact(const V& S, float3 o, float3
 }
 
 // Any hit, compact loop.
-template <class V, class Stack>
+template <int kTree = kTreeAny, class V, class Stack>
 __device__ __forceinline__ bool any_hit_compact(const V& S, float3 o, float3 d, float tmax,
                                                 int* status, Stack& stack, uint64_t akey = 0) {
   for (int i = 0; i < S.n_planes; ++i) {
@@ -217,12 +415,15 @@ __device__ __forceinline__ bool any_hit_compact(const V& S, float3 o, float3 d, 
     if (plane_hit(S.planes[i], o, d, t) && t < tmax) return true;
   }
   if (!S.has_bvh) return false;
+  const float tlim = fminf(tmax, kTMax);
+  if constexpr (!V::kQuadrics && kTree != kTreeBinary) {
+    if (kTree == kTreeWide || S.wnodes) return wide_any(S, o, d, tlim, status, stack, akey);
+  }
   float3 inv = f3(1.0f / d.x, 1.0f / d.y, 1.0f / d.z);
   float3 oi = o * inv;
   int sp = 0;
   int cur = 0;
   int budget = 4 * S.n_nodes + 4 * S.n_prims + 64;
-  const float tlim = fminf(tmax, kTMax);
   while (true) {
     if (--budget < 0) {
       if (status) atomicOr(status, ST_BUDGET);

@@ -42,9 +42,14 @@ constexpr int kWfBlock = 128;
 // bytes of spills.
 // (The quadric and textured instantiations keep the compiler's choice: at
 // 40 registers they spill.)
-constexpr int kTravMinBlocks = 12;
-template <class V>
-constexpr int trav_min_blocks() { return V::kQuadrics ? 1 : kTravMinBlocks; }
+#ifndef MRT_TRAV_MIN_BLOCKS
+#define MRT_TRAV_MIN_BLOCKS 12
+#endif
+constexpr int kTravMinBlocks = MRT_TRAV_MIN_BLOCKS;
+// The 8-wide tree's traversal (MRT_BVH_WIDE) measured faster at 64
+// registers (8 blocks per SM) than at 40.
+template <class V, int kTree>
+constexpr int trav_min_blocks() { return V::kQuadrics ? 1 : (kTree == kTreeWide ? 8 : kTravMinBlocks); }
 
 struct WfState {
   // path state, indexed by path slot
@@ -157,8 +162,8 @@ __global__ void __launch_bounds__(kWfBlock) wf_generate(SceneView S, WfState W, 
 }
 
 // --------------------------------------------------------------- extend
-template <int kBounceParity, class V>
-__global__ void __launch_bounds__(kWfBlock, trav_min_blocks<V>()) wf_extend(V S, WfState W, int* status) {
+template <int kBounceParity, class V, int kTree>
+__global__ void __launch_bounds__(kWfBlock, trav_min_blocks<V, kTree>()) wf_extend(V S, WfState W, int* status) {
   const int n = W.counters[kBounceParity ? C_LIVE1 : C_LIVE0];
   const int* q = W.q_live[kBounceParity];
   const int lane = threadIdx.x & 31;
@@ -176,8 +181,8 @@ __global__ void __launch_bounds__(kWfBlock, trav_min_blocks<V>()) wf_extend(V S,
       int visits = 0;
       // textured scenes: the alpha test draws from the path's random state
       const uint64_t akey = V::kTextures ? W.rng[i] : 0;
-      bool hit = closest_hit_compact<false>(S, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), h, visits, status, stack,
-                                            akey);
+      bool hit = closest_hit_compact<false, kTree>(S, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), h, visits, status,
+                                                   stack, akey);
       W.hit[i] = make_float4(h.t, h.u, h.v, __int_as_float(hit ? h.prim : kMiss));
     }
   }
@@ -381,8 +386,8 @@ __global__ void __launch_bounds__(kWfBlock) wf_sample(V S, WfState W, const WfPa
 }
 
 // -------------------------------------------------------------- connect
-template <class V>
-__global__ void __launch_bounds__(kWfBlock, trav_min_blocks<V>()) wf_connect(V S, WfState W, int* status) {
+template <class V, int kTree>
+__global__ void __launch_bounds__(kWfBlock, trav_min_blocks<V, kTree>()) wf_connect(V S, WfState W, int* status) {
   const int n = min(W.counters[C_SH], W.sh_capacity);
   const int lane = threadIdx.x & 31;
   LocalStack stack;
@@ -395,7 +400,7 @@ __global__ void __launch_bounds__(kWfBlock, trav_min_blocks<V>()) wf_connect(V S
     if (k < n) {
       const float4 o = W.sh_o[k], d = W.sh_d[k];
       const uint64_t akey = V::kTextures ? W.sh_key[k] : 0;
-      const bool blocked = any_hit_compact(S, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), o.w, status, stack, akey);
+      const bool blocked = any_hit_compact<kTree>(S, f3(o.x, o.y, o.z), f3(d.x, d.y, d.z), o.w, status, stack, akey);
       if (!blocked) {
         const int tag = __float_as_int(d.w);
         const int env_slot = (1 << W.slot_bits) - 1;
@@ -614,15 +619,35 @@ static void wf_enqueue_wave_t(WfHost* H, const VT& v, const WfParams& P, int* st
                               cudaStream_t st, unsigned* launches) {
   const WfParams* dP = H->dparams;
   const int gen_blocks = std::max(1, std::min((H->capacity + kWfBlock - 1) / kWfBlock, H->sms * 16));
-  const int pers = H->sms * 12;
+  const int pers = H->sms * kTravMinBlocks, pers_wide = H->sms * 8;
   const WfState s = H->st;
   cudaStream_t sd = H->side;
   unsigned n = 0;
+  // the tree's own traversal kernels (the wide tree: SceneView only)
+  bool wide = false;
+  if constexpr (!VT::kQuadrics) wide = v.wnodes != nullptr;
   auto extend = [&](int par) {
     wf_work_reset<<<1, 32, 0, st>>>(s);
-    if (par) wf_extend<1, VT><<<pers, kWfBlock, 0, st>>>(v, s, status);
-    else wf_extend<0, VT><<<pers, kWfBlock, 0, st>>>(v, s, status);
+    if constexpr (!VT::kQuadrics) {
+      if (wide) {
+        if (par) wf_extend<1, VT, kTreeWide><<<pers_wide, kWfBlock, 0, st>>>(v, s, status);
+        else wf_extend<0, VT, kTreeWide><<<pers_wide, kWfBlock, 0, st>>>(v, s, status);
+        n += 2;
+        return;
+      }
+    }
+    if (par) wf_extend<1, VT, kTreeBinary><<<pers, kWfBlock, 0, st>>>(v, s, status);
+    else wf_extend<0, VT, kTreeBinary><<<pers, kWfBlock, 0, st>>>(v, s, status);
     n += 2;
+  };
+  auto connect = [&]() {
+    if constexpr (!VT::kQuadrics) {
+      if (wide) {
+        wf_connect<VT, kTreeWide><<<pers_wide, kWfBlock, 0, sd>>>(v, s, status);
+        return;
+      }
+    }
+    wf_connect<VT, kTreeBinary><<<pers, kWfBlock, 0, sd>>>(v, s, status);
   };
   wf_wave_begin<<<1, 32, 0, st>>>(s);
   wf_generate<<<gen_blocks, kWfBlock, 0, st>>>(v, s, dP);
@@ -640,7 +665,7 @@ static void wf_enqueue_wave_t(WfHost* H, const VT& v, const WfParams& P, int* st
     cudaEventRecord(H->ev_fork, st);
     cudaStreamWaitEvent(sd, H->ev_fork, 0);
     wf_sh_work_reset<<<1, 32, 0, sd>>>(s);
-    wf_connect<VT><<<pers, kWfBlock, 0, sd>>>(v, s, status);
+    connect();
     wf_finish<<<gen_blocks, kWfBlock, 0, sd>>>(v, s);
     cudaEventRecord(H->ev_join, sd);
     n += 5;

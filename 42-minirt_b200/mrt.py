@@ -167,7 +167,7 @@ class BvhOptions(C.Structure):
                 ("order", C.POINTER(C.c_int32)), ("positions", C.POINTER(C.c_double))]
 
 
-BVH_SAH, BVH_REFERENCE = 0, 1
+BVH_SAH, BVH_REFERENCE, BVH_WIDE = 0, 1, 2
 
 
 class Ray(C.Structure):
@@ -208,6 +208,7 @@ SIGNATURES = {
     "mrt_comm_unique_id": (C.c_int, [_P]),
     "mrt_set_bvh_options": (C.c_int, [_P, _P]),
     "mrt_read_bvh_leaves": (C.c_int64, [_P, _P, C.c_int64]),
+    "mrt_bvh_build_check": (C.c_int, [_P, C.c_int64, C.c_int32, _P]),
     "mrt_comm_init": (C.c_int, [_P, _P, C.c_int32, C.c_int32]),
     "mrt_reduce_frame": (C.c_int, [_P, C.c_int32]),
     "mrt_comm_destroy": (C.c_int, [_P]),
@@ -254,6 +255,15 @@ def render_batch(ctxs: list, params: list[dict], block_size: int = 0) -> "Render
 _lib = None
 
 COMM_ID_BYTES = 128
+
+
+def bvh_build_check(boxes, mode: int = BVH_WIDE) -> dict:
+    """mrt_bvh_build_check: build the BVH over (n, 6) boxes (min xyz, max
+    xyz) on the host and check the wide tree's structure."""
+    b = np.ascontiguousarray(boxes, np.float64).reshape(-1, 6)
+    st = np.zeros(4, np.int64)
+    check(load().mrt_bvh_build_check(_ptr(b), len(b), mode, _ptr(st)), "mrt_bvh_build_check")
+    return {"nodes": int(st[0]), "depth": int(st[1]), "leaves": int(st[2]), "wide": bool(st[3])}
 
 
 def comm_unique_id() -> bytes:
@@ -403,8 +413,10 @@ class Context:
         check(self.lib.mrt_comm_destroy(self.h), "mrt_comm_destroy")
 
     def set_bvh_options(self, mode: int, order=None, positions=None) -> None:
-        """BVH build for the next build(): BVH_SAH (default) or BVH_REFERENCE
-        (the reference's median-split tree, traversed left first, with the
+        """BVH build for the next build(): BVH_SAH (default, the binary SAH
+        tree), BVH_WIDE (the 8-wide tree, for scenes without quadrics or
+        textures) or BVH_REFERENCE (the
+        reference's median-split tree, traversed left first, with the
         reference's node-visit count in render_mode 1). order: flat ids in the
         reference's object-list order; positions: (n, 3) split positions."""
         o = BvhOptions(mode=mode)

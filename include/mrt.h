@@ -384,8 +384,14 @@ MRT_API int			mrt_render_batch(mrt_ctx **ctx, const mrt_render_params *params,
 				int32_t n, mrt_render_stats *stats);
 
 /* BVH build options, applied by the next mrt_scene_build.
- * MRT_BVH_SAH (default): this library's binned-SAH tree, up to 8 primitives
- * per leaf, traversed nearer child first. MRT_BVH_REFERENCE: the reference's
+ * MRT_BVH_SAH (default): this library's binned-SAH binary tree, up to 8
+ * primitives per leaf, traversed nearer child first. MRT_BVH_WIDE: the same
+ * SAH tree built with leaves of up to 4 primitives and collapsed to an
+ * 8-wide tree with 8-bit quantised child boxes (80-byte nodes, SAH-optimal
+ * slot distribution), children visited in the ray's octant order; for
+ * scenes of spheres, triangles and planes without textures (others get the
+ * binary tree), and the binary tree when a scene's wide tree would be too
+ * deep for its stack. MRT_BVH_REFERENCE: the reference's
  * own tree (bvh_build.c:16-127: one primitive per leaf, split at the median
  * of the object positions on the longest axis of the node bounds, in the
  * reference's sort order), traversed left child first, with the reference's
@@ -401,7 +407,8 @@ MRT_API int			mrt_render_batch(mrt_ctx **ctx, const mrt_render_params *params,
 typedef enum mrt_bvh_mode
 {
 	MRT_BVH_SAH = 0,
-	MRT_BVH_REFERENCE = 1
+	MRT_BVH_REFERENCE = 1,
+	MRT_BVH_WIDE = 2
 }	mrt_bvh_mode;
 
 typedef struct mrt_bvh_options
@@ -419,6 +426,13 @@ MRT_API int			mrt_set_bvh_options(mrt_ctx *ctx, const mrt_bvh_options *options);
  * With MRT_BVH_REFERENCE this is the reference's sorted prim_indices order
  * (one primitive per leaf). */
 MRT_API int64_t		mrt_read_bvh_leaves(mrt_ctx *ctx, int32_t *flat, int64_t cap);
+/* Host-only diagnostic (no device needed): builds the MRT_BVH_SAH (binary)
+ * or MRT_BVH_WIDE tree over n boxes (6 doubles each: min xyz, max xyz)
+ * and, for the wide tree, checks its structure: every node reached once,
+ * leaves inside the primitive array, each primitive in one leaf, and every
+ * quantised slot box containing the boxes below it. stats (may be NULL)
+ * receives 4 values: nodes, depth, leaves, 1 if the wide tree was built. */
+MRT_API int			mrt_bvh_build_check(const double *boxes, int64_t n, int32_t mode, int64_t *stats);
 
 /* Zero the device accumulator. */
 MRT_API int			mrt_clear(mrt_ctx *ctx);

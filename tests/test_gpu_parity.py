@@ -37,9 +37,11 @@ def require_device(mrt):
     assert lib.mrt_device_count() > 0, "gpu tests need a CUDA device"
 
 
-def gpu_ctx(mrt, oracle, scene):
+def gpu_ctx(mrt, oracle, scene, tree=0):
     cs = oracle.canonical_scene(scene)
     ctx = mrt.Context(scene.width, scene.height)
+    if tree:
+        ctx.set_bvh_options(tree)
     ctx.build(cs)
     return ctx
 
@@ -225,18 +227,19 @@ def six_light_scene(scenes):
     return sc
 
 
-@pytest.mark.parametrize("name", ["c0", "c1", "c2", "q0", "t0", "t0_alpha", "lights6"])
+@pytest.mark.parametrize("name", ["c0", "c1", "c2", "q0", "t0", "t0_alpha", "lights6", "c1_wide", "c2_wide"])
 def test_wavefront_matches_megakernel(mrt, oracle, mg, scenes, name):
     """Both forms run the same estimator on the same random streams
     (textured scenes included: the alpha test draws from the same path state
-    in both)."""
+    in both; *_wide: on the 8-wide tree, whose own extend and connect
+    kernels the wavefront launches)."""
     if name == "lights6":
         sc = six_light_scene(scenes)
     elif name == "t0_alpha":
         sc = scenes.make_textured(6, 32, 24, depth=6, partial_alpha=True)
     else:
-        sc = mg.CASES[name]["make"]()
-    ctx = gpu_ctx(mrt, oracle, sc)
+        sc = mg.CASES[name.replace("_wide", "")]["make"]()
+    ctx = gpu_ctx(mrt, oracle, sc, tree=mrt.BVH_WIDE if name.endswith("_wide") else mrt.BVH_SAH)
     ctx.render(8, seed=5)
     a, _ = ctx.read_accum()
     for graph in (0, 1):

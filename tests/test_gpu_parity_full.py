@@ -1,7 +1,8 @@
 """Parity of the CUDA path with the oracle at the benchmark configurations'
 own sizes (the other parity tests use miniature scenes):
 
-  * first hits on the full c1 mesh (1,310,720 triangles): 50,000 rays,
+  * first hits on the full c1 mesh (1,310,720 triangles), on the binary
+    SAH tree and on the 8-wide tree: 50,000 rays,
     rays from the camera aimed at the mesh and secondary rays leaving the
     surface; the primitive id must match the FP64 restatement (which walks
     the reference's own median-split BVH, bvh_build.c:104) on every ray
@@ -47,11 +48,15 @@ def cosine_dirs(rng, n_rm):
     return local[:, 0:1] * t + local[:, 1:2] * b + local[:, 2:3] * n_rm
 
 
-def test_first_hit_exact_on_full_c1_mesh(mrt, oracle, scenes):
+@pytest.mark.parametrize("tree", ["sah", "wide"])
+def test_first_hit_exact_on_full_c1_mesh(mrt, oracle, scenes, tree):
+    """On the default binary SAH tree and on the 8-wide tree
+    (MRT_BVH_WIDE, quantised child boxes): the same exact hits."""
     sc = scenes.make_c1()
     ro = oracle.Restatement(sc)
     tri_pos = ro.triangle_positions()
     ctx = mrt.Context(sc.width, sc.height)
+    ctx.set_bvh_options(mrt.BVH_WIDE if tree == "wide" else mrt.BVH_SAH)
     ctx.build(oracle.canonical_scene(sc))
     rng = np.random.default_rng(2024)
     # rays from the camera position
@@ -77,7 +82,7 @@ def test_first_hit_exact_on_full_c1_mesh(mrt, oracle, scenes):
     g = ctx.first_hit(o, d)
     r = ro.first_hit(o, d)
     exact, tie, boundary, other = hitcheck.classify(sc, tri_pos, o, d, g, r)
-    print(f"c1 full mesh: {len(o)} rays, exact {int(exact.sum())}, tie {int(tie.sum())}, "
+    print(f"c1 full mesh ({tree}): {len(o)} rays, exact {int(exact.sum())}, tie {int(tie.sum())}, "
           f"boundary {int(boundary.sum())}, other {int(other.sum())}; "
           f"hits gpu {int((g['prim'] >= 0).sum())} oracle {int((r['prim'] >= 0).sum())}")
     bad = np.nonzero(other)[0][:5]
