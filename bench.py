@@ -74,8 +74,10 @@ def parse():
     ap.add_argument("--spp-per-step", type=int, default=16)
     ap.add_argument("--forms", default="megakernel_plain,megakernel,wavefront")
     ap.add_argument("--no-relmse", action="store_true")
-    ap.add_argument("--relmse-cap-spp", type=int, default=4096,
-                    help="stop the time-to-relMSE render here if 1e-3 is not reached")
+    ap.add_argument("--relmse-cap-spp", type=int, default=None,
+                    help="most samples per pixel rendered while waiting for relMSE <= 1e-3 "
+                         "(default: 16384 for c0, whose emitter-lit frame converges slowly "
+                         "but renders in a fraction of a second, else 4096)")
     ap.add_argument("--cpu-seconds", type=float, default=8.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
@@ -218,6 +220,11 @@ def convergence(ctx, sc, config: str, spp_step: int, forms: dict, fid: int, cap_
                                 "relMSE against the converged image the reference estimates",
            "relmse_ref_noise": float(np.mean(var_r / (r ** 2 + 1e-2))),
            "c_fit": c, "trace": [[int(a), float(b)] for a, b in trace[:: max(1, len(trace) // 16)]]}
+    if config.startswith("c2"):
+        out["note"] = ("a kNN caustic image depends on its photon set: this render gathers the "
+                       "library's own photon map, the fixture the reference's, so relMSE levels "
+                       "off at their difference; the converged-radiance test gives the GPU the "
+                       "reference's photon map (mrt_set_photons) and meets the bar")
     if reached is None:
         out.update({"reached": False, "spp_rendered": done, "relmse_last": float(rs[-1])})
         return out
@@ -574,7 +581,8 @@ def main() -> int:
 
     relmse = None
     if not a.no_relmse and world == 1:
-        relmse = convergence(ctx, sc, a.config, spp, forms, form_ids[best], a.relmse_cap_spp)
+        cap = a.relmse_cap_spp or (16384 if a.config == "c0" else 4096)
+        relmse = convergence(ctx, sc, a.config, spp, forms, form_ids[best], cap)
     adjoint = None
     if not a.no_adjoint and world == 1:
         adjoint = adjoint_bench(local, a.adam_steps)
