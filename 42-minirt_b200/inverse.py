@@ -89,9 +89,20 @@ def perturb(theta0: np.ndarray, layout: dict, rel: float, seed: int) -> np.ndarr
     return t.astype(np.float32)
 
 
+def clip_quantile(g, q: float):
+    """g clipped to +-(the q-quantile of |g|), the quantile estimated on a
+    strided subsample of at most 2^16 entries."""
+    torch = _torch()
+    flat = g.abs().flatten()
+    step = max(1, flat.numel() // 65536)
+    t = torch.quantile(flat[::step].float(), q)
+    return g.clamp(-t, t)
+
+
 def fit(ctx: mrt.Context, theta_init, target, steps: int = 100, lr: float = 1e-2, spp: int = 64,
         seed: int = 1000, decorrelate: bool = True, mask=None, residual_spp: int | None = None,
-        lr_decay: bool = False, callback=None, sky_log: bool = False, sky_lr: float | None = None):
+        lr_decay: bool = False, callback=None, sky_log: bool = False, sky_lr: float | None = None,
+        grad_quantile: float | None = None):
     """Projected Adam on the mean squared error between render(theta) and
     target (an (H, W, 3) CUDA tensor); each step draws fresh samples. With
     decorrelate, the gradient replays samples independent of those of the
@@ -107,8 +118,16 @@ def fit(ctx: mrt.Context, theta_init, target, steps: int = 100, lr: float = 1e-2
     Adam's steps have a fixed size in the parameter, and sky radiance spans
     five orders of magnitude (0.2 to 5e4 at a sun), so equal steps in
     log-radiance are equal relative changes of every texel, and the texels
-    stay positive. sky_lr (default lr) is the rate of that group. Returns
-    (theta, losses)."""
+    stay positive. sky_lr (default lr) is the rate of that group.
+
+    grad_quantile clips the image gradient dL/dI of each step, per pixel and
+    channel, to that quantile of its magnitude (0.999: the largest 0.1 %).
+    A sky with a sun lobe makes single paths carry radiance four orders of
+    magnitude above the mean; their residuals dominate the L2 gradient of a
+    64-spp step, so the update is mostly noise. Clipping them trades a small
+    bias for most of that variance: on c4 (materials fitted under the target
+    sky, 100 steps, 3 seeds) the albedo error fell to 0.65-0.71 of its start
+    instead of 0.81-0.86. Returns (theta, losses)."""
     torch = _torch()
     layout = ctx.diff_layout()
     dev = target.device
@@ -143,6 +162,8 @@ def fit(ctx: mrt.Context, theta_init, target, steps: int = 100, lr: float = 1e-2
         base = step * stride
         theta = full()
         img = render(theta, ctx, rspp, seed, base, base + rspp if decorrelate else base, spp)
+        if grad_quantile is not None:
+            img.register_hook(lambda g: clip_quantile(g, grad_quantile))
         loss = torch.mean((img - target) ** 2)
         loss.backward()
         if keep is not None:
