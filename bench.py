@@ -285,8 +285,12 @@ def adjoint_bench(device: int, adam_steps: int, res: int = 512) -> dict:
         runs = []
         for fit_seed in (1000, 2000, 3000):
             t0 = time.perf_counter()
+            # the joint fit keeps the sky in log space and the full image
+            # gradient: in linear space one of three seeds diverged, and the
+            # clip below biased the sun texels' gradients, whose error the
+            # albedos then absorbed (material error 0.047-0.050 vs 0.040)
             fit, losses = inverse.fit(ctx, th, target, steps=adam_steps, lr=1e-2, spp=spp, seed=fit_seed,
-                                      residual_spp=128, lr_decay=True, sky_log=True, grad_quantile=0.999)
+                                      residual_spp=128, lr_decay=True, sky_log=True)
             torch.cuda.synchronize()
             wall = time.perf_counter() - t0
             fit = fit.cpu().numpy()
@@ -316,8 +320,9 @@ def adjoint_bench(device: int, adam_steps: int, res: int = 512) -> dict:
                     "seen_param_mae_start": float(np.abs(init[seen] - target_theta[seen]).mean()),
                     "seen_param_mae_end": float(np.abs(fit[seen] - target_theta[seen]).mean())}
         out["adam"] = {"steps": adam_steps, "lr": 1e-2, "spp": spp, "residual_spp": 128,
-                       "schedule": "cosine decay to 1% of lr; sky texels in log space; image gradient "
-                                   "clipped per pixel at its 99.9th percentile",
+                       "schedule": "cosine decay to 1% of lr; joint fit: sky texels in log space; "
+                                   "materials-only fit: image gradient clipped per pixel at its 99.9th "
+                                   "percentile",
                        "seen_material_entries": int(len(seen)), "of_material_entries": nm,
                        "median_of_3_seeds": med, "runs": runs, "materials_only_under_target_sky": mat_only}
     ctx.close()
