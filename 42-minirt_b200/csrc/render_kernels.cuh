@@ -81,9 +81,20 @@ __device__ __forceinline__ void add_path(const LaunchParams& L, float4* accum, u
 // by one bounce per loop iteration; lanes whose path ended take the next path
 // index (one atomic per warp for all idle lanes), so warps stay full until
 // the launch runs out of paths.
+// The regenerating and batch megakernels run at 44 registers per thread:
+// the whole path loop spills to local memory, which stays in L1, and the SM
+// keeps up to 46 warps of latency-bound traversal in flight instead of 16 at
+// the compiler's 128. Measured on B200 (regenerating megakernel, Mpaths/s,
+// 128 / 96 / 64 / 44 / 40 / 32 registers): c1 235 / 278 / 369 / 401 / 410 /
+// 384, c4 480 / 558 / 682 / 740 / 734 / 700, c0 4,288 / 4,608 / 5,742 /
+// 6,050 / 5,607 / 5,532, c2 81 / 90 / 97 / 98 / 103 / 65; the batch
+// megakernel on c3's 64 scenes 500 -> 703 (64 registers: 712). The plain
+// megakernel keeps the compiler's choice: it is the untuned baseline form.
+constexpr int kMegaRegs = 44;
+
 template <int kBlock, class V>
-__global__ void __launch_bounds__(kBlock) megakernel_regen(V S, LaunchParams L, float4* accum,
-                                                           int* status, unsigned long long* work) {
+__global__ void __maxnreg__(kMegaRegs) megakernel_regen(V S, LaunchParams L, float4* accum,
+                                                        int* status, unsigned long long* work) {
   const uint32_t npix = (uint32_t)S.width * (uint32_t)S.height;
   const int lane = threadIdx.x & 31;
   PathCounters C{0, 0, 0};
@@ -135,7 +146,7 @@ __global__ void __launch_bounds__(kBlock) megakernel_regen(V S, LaunchParams L, 
 // the scene whose [start, start + paths) range holds it (binary search over
 // <= a few hundred prefix sums). Otherwise the regenerating loop above.
 template <int kBlock, class V>
-__global__ void __launch_bounds__(kBlock) megakernel_batch(const SceneView* __restrict__ views,
+__global__ void __maxnreg__(kMegaRegs) megakernel_batch(const SceneView* __restrict__ views,
                                                            const BatchItem* __restrict__ items,
                                                            int n_items, uint64_t total,
                                                            int* status, unsigned long long* work) {
