@@ -525,11 +525,13 @@ def main() -> int:
         barrier()
         ms = 0.0
         launches = 0
+        step_ms = []
         base, _ = D.shard_samples(a.steps * spp * world, world, rank)
         for s in range(a.steps):
             st = ctx.render(spp, seed=1, sample_base=base + s * spp, form=fid,
                             use_graph=1 if fid == mrt.FORM_WAVEFRONT else 0)
             ms += st.ms
+            step_ms.append(round(st.ms, 3))
             launches += st.kernel_launches
         if dist:
             # the frame of the job: one sum-reduce of the accumulators onto rank 0
@@ -547,7 +549,7 @@ def main() -> int:
         mps = total_paths / (t_max / 1000.0) / 1e6
         per_launch_ms = ms / max(launches, 1)
         forms[name] = {"value": mps, "ms_per_step": t_max / a.steps, "launches": launches,
-                       "launch_ms": per_launch_ms}
+                       "launch_ms": per_launch_ms, "step_ms": step_ms}
         if best is None or mps > forms[best]["value"]:
             best = name
         launches_total = launches
