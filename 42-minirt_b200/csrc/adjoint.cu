@@ -494,8 +494,13 @@ __device__ __forceinline__ void finish_path(const SceneView& S, const AdjointArg
 // Replay: the paths of the forward again (persistent, lanes regenerate
 // paths as in the regenerating megakernel), writing one tape entry per
 // bounce to tape[k * n_paths + path].
+// The replay kernel traces like the regenerating megakernel and, like it,
+// runs faster at 44 registers than at the compiler's 128 (c4 512x512x64 spp
+// backward: 57.9 -> 46.8 ms; 64 registers: 49.7 ms). The per-level kernel
+// keeps its registers (its Dual<7> arithmetic needs them; 128: no change).
+constexpr int kReplayRegs = 44;
 template <int kBlock, class V>
-__global__ void __launch_bounds__(kBlock) adj_replay_kernel(V S, AdjointArgs A, TapeEntry* tape,
+__global__ void __maxnreg__(kReplayRegs) adj_replay_kernel(V S, AdjointArgs A, TapeEntry* tape,
                                                             float4* state, int* status,
                                                             unsigned long long* work) {
   const uint32_t npix = (uint32_t)S.width * (uint32_t)S.height;
