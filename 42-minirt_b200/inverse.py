@@ -102,7 +102,7 @@ def clip_quantile(g, q: float):
 def fit(ctx: mrt.Context, theta_init, target, steps: int = 100, lr: float = 1e-2, spp: int = 64,
         seed: int = 1000, decorrelate: bool = True, mask=None, residual_spp: int | None = None,
         lr_decay: bool = False, callback=None, sky_log: bool = False, sky_lr: float | None = None,
-        grad_quantile: float | None = None):
+        grad_quantile: float | None = None, betas: tuple = (0.9, 0.999)):
     """Projected Adam on the mean squared error between render(theta) and
     target (an (H, W, 3) CUDA tensor); each step draws fresh samples. With
     decorrelate, the gradient replays samples independent of those of the
@@ -127,7 +127,8 @@ def fit(ctx: mrt.Context, theta_init, target, steps: int = 100, lr: float = 1e-2
     64-spp step, so the update is mostly noise. Clipping them trades a small
     bias for most of that variance: on c4 (materials fitted under the target
     sky, 100 steps, 3 seeds) the albedo error fell to 0.65-0.71 of its start
-    instead of 0.81-0.86. Returns (theta, losses)."""
+    instead of 0.81-0.86. betas are Adam's moment decay rates. Returns
+    (theta, losses)."""
     torch = _torch()
     layout = ctx.diff_layout()
     dev = target.device
@@ -144,7 +145,7 @@ def fit(ctx: mrt.Context, theta_init, target, steps: int = 100, lr: float = 1e-2
         mat = th0.clone().requires_grad_(True)
         phi = None
         groups = [{"params": [mat], "lr": lr}]
-    opt = torch.optim.Adam(groups)
+    opt = torch.optim.Adam(groups, betas=betas)
     base_lrs = [g["lr"] for g in opt.param_groups]
 
     def full():
