@@ -104,3 +104,22 @@ def test_product_does_not_import_the_oracle():
     for f in (REPO / "42-minirt_b200").rglob("*.py"):
         txt = f.read_text()
         assert "import oracle" not in txt and "oracle/" not in txt.replace("# ", ""), f
+
+
+def test_drop_in_exports_every_gpu_h_entry_point(mrt):
+    """libmrt_minirt.so (the drop-in for miniRT's src/gpu) defines every
+    function include/minirt_compat/gpu.h declares, gpu_bvh_sah included
+    (read from the dynamic symbol table; nothing is loaded)."""
+    import re
+    import shutil
+    lib = Path(mrt.MINIRT_LIB_PATH)
+    if not lib.exists():
+        pytest.skip("libmrt_minirt.so is built only where the reference headers are present")
+    nm = shutil.which("nm")
+    assert nm, "binutils nm is needed"
+    decl = (REPO / "include" / "minirt_compat" / "gpu.h").read_text()
+    names = set(re.findall(r"^\w[\w\s\*]*?\b(\w+)\(", decl, re.M))
+    assert {"init_shader", "convert_scene_build", "compute_frame_gpu", "gpu_bvh_sah"} <= names
+    out = subprocess.run([nm, "-D", "--defined-only", str(lib)], capture_output=True, text=True, check=True).stdout
+    defined = {line.split()[-1] for line in out.splitlines() if line.strip()}
+    assert names <= defined, sorted(names - defined)
